@@ -1,0 +1,622 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200-native warpcore hot path.
+
+Default workload (one step): SingleValueHashTable<uint64,uint64>, CG 8, at
+load factor 0.9 (reference capacity 149,963,432 slots): init the table,
+insert 2^27 unique uniform keys with uniform values, retrieve 2^27 queries
+(50 % hits) in uniform random order.  Metric: Gops/s = keys processed
+(inserts + queries) per second, whole job.  Inputs (1 GiB per array) are
+larger than L2, so no flush is needed between iterations.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload svht64|svht32|hashset64|counting32|bloom64]
+                  [--log2n L] [--load F]
+
+--impl reference times the reference algorithm's CPU port (the oracle's
+multi-threaded open-addressing table: same MurmurHash, DoubleHashing and
+lane order) on the host cores; it is the one other place this script runs
+oracle code besides the cpu_baseline leg.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+MASK64 = (1 << 64) - 1
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "of measured"
+    except Exception:
+        return 6650.0, "of fallback"
+
+
+def profile_traffic(name):
+    """dram bytes per launch recorded by the ncu capture summarised under
+    profiles/ (line 'dram_bytes_per_launch <kernel-tag> <bytes>')."""
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        f = line.split()
+        if len(f) == 3 and f[0] == "dram_bytes_per_launch" and f[1] == name:
+            return float(f[2])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region"""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# synthetic data on the device (torch int64 holds the uint64 bits)
+# ---------------------------------------------------------------------------
+
+def _srl(x, s):
+    import torch
+    return torch.bitwise_and(torch.bitwise_right_shift(x, s), (1 << (64 - s)) - 1)
+
+
+def fmix64_t(x):
+    """MurmurHash3 fmix64 on int64 tensors (two's complement wrap)"""
+    import torch
+    c1 = 0xFF51AFD7ED558CCD - (1 << 64)
+    c2 = 0xC4CEB9FE1A85EC53 - (1 << 64)
+    x = torch.bitwise_xor(x, _srl(x, 33))
+    x = x * c1
+    x = torch.bitwise_xor(x, _srl(x, 33))
+    x = x * c2
+    x = torch.bitwise_xor(x, _srl(x, 33))
+    return x
+
+
+def unique_keys64(start, n, seed, device):
+    """n distinct uint64 keys: fmix64 is a bijection of the 64-bit index;
+    the two sentinels (0, ~0) are dropped"""
+    import torch
+    off = (seed * 0x9E3779B97F4A7C15) & MASK64
+    off = off - (1 << 64) if off >= (1 << 63) else off  # as a signed int64
+    idx = torch.arange(start, start + n + 4, dtype=torch.int64, device=device) + off
+    k = fmix64_t(idx)
+    k = k[(k != 0) & (k != -1)]
+    return k[:n].contiguous()
+
+
+def unique_keys32(start, n, seed, device):
+    """n distinct uint32 keys (stored in int32): a 32-bit mix of the index"""
+    import torch
+    idx = torch.arange(start, start + n + 4, dtype=torch.int64, device=device)
+    x = (idx + seed * 0x9E3779B9) & 0xFFFFFFFF
+    x = x ^ (x >> 16)
+    x = (x * 0x85EBCA6B) & 0xFFFFFFFF
+    x = x ^ (x >> 13)
+    x = (x * 0xC2B2AE35) & 0xFFFFFFFF
+    x = x ^ (x >> 16)
+    x = x[(x != 0) & (x != 0xFFFFFFFF)][:n]
+    return (x - ((x >= (1 << 31)).to(torch.int64) << 32)).to(torch.int32).contiguous()
+
+
+def uniform_values(n, nbytes, gen, device):
+    import torch
+    if nbytes == 8:
+        return torch.randint(-(1 << 63), (1 << 63) - 1, (n,), dtype=torch.int64,
+                             device=device, generator=gen)
+    return torch.randint(-(1 << 31), (1 << 31) - 1, (n,), dtype=torch.int32,
+                         device=device, generator=gen)
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+
+class Workload:
+    """one step = init + insert(n) + retrieve(q) on resident inputs"""
+
+    def __init__(self, kind, log2n, load, rank, device):
+        import torch
+        import warpcore_b200 as wc
+        self.kind = kind
+        self.n = 1 << log2n
+        self.q = 1 << log2n
+        self.load = load
+        self.device = device
+        gen = torch.Generator(device=device)
+        gen.manual_seed(1000 + rank)
+        seed = 17 + 101 * rank
+        kb = 4 if kind in ("svht32", "counting32") else 8
+        self.kb = kb
+        n, q = self.n, self.q
+        if kind in ("svht32", "svht64", "hashset64"):
+            mk = unique_keys32 if kb == 4 else unique_keys64
+            keys = mk(0, n + q // 2, seed, device)
+            self.keys = keys[:n].contiguous()
+            absent = keys[n:n + q // 2]
+            self.values = uniform_values(n, kb, gen, device)
+            hit_idx = torch.randperm(n, device=device, generator=gen)[: q - q // 2]
+            queries = torch.cat([self.keys[hit_idx], absent])
+            exp = torch.cat([self.values[hit_idx],
+                             torch.zeros(q // 2, dtype=self.values.dtype, device=device)])
+            hit = torch.cat([torch.ones(q - q // 2, dtype=torch.bool, device=device),
+                             torch.zeros(q // 2, dtype=torch.bool, device=device)])
+            perm = torch.randperm(q, device=device, generator=gen)
+            self.queries = queries[perm].contiguous()
+            self.expected = exp[perm].contiguous()
+            self.hit = hit[perm].contiguous()
+            if kind == "hashset64":
+                self.table = wc.HashSet(int(n / load), key_bytes=8)
+                self.out = torch.empty(q, dtype=torch.uint8, device=device)
+                self.bytes_insert, self.bytes_retrieve = 8 + 32 + 32, 8 + 1 + 32
+            else:
+                self.table = wc.SingleValueHashTable(int(n / load), key_bytes=kb)
+                self.out = torch.empty(q, dtype=self.values.dtype, device=device)
+                self.bytes_insert = kb + kb + 32 + 32
+                self.bytes_retrieve = kb + kb + 1 + 32
+        elif kind == "counting32":
+            distinct = n >> 4
+            self.distinct = distinct
+            keys = unique_keys32(0, distinct + (distinct >> 2), seed, device)
+            self.dkeys = keys[:distinct]
+            ranks = zipf_ranks_t(distinct, 1.1, n, gen, device)
+            self.keys = self.dkeys[ranks].contiguous()
+            self.values = None
+            self.queries = keys.contiguous()
+            self.q = self.queries.numel()
+            self.hist = torch.bincount(ranks, minlength=distinct)
+            self.table = wc.CountingHashTable(int(distinct / load), key_bytes=4)
+            self.out = torch.empty(self.q, dtype=torch.int32, device=device)
+            self.bytes_insert, self.bytes_retrieve = 4 + 32 + 32, 4 + 4 + 1 + 32
+        elif kind == "bloom64":
+            keys = unique_keys64(0, 2 * n, seed, device)
+            self.keys = keys[:n].contiguous()
+            self.queries = torch.cat([keys[n:], keys[:n]]).contiguous()
+            self.q = 2 * n
+            self.values = None
+            # 16 bits per key, 512-bit blocks, 8 bits per key
+            self.table = wc.BloomFilter(16 * n, 8, key_bytes=8, slot_bytes=8, cg_size=8)
+            self.out = torch.empty(self.q, dtype=torch.uint8, device=device)
+            self.bytes_insert, self.bytes_retrieve = 8 + 64 + 64, 8 + 1 + 64
+        else:
+            raise ValueError(kind)
+        torch.cuda.synchronize()
+
+    # -- one step's operations --
+    def init(self, stream):
+        self.table.init(stream=stream)
+
+    def insert(self, stream):
+        if self.kind in ("svht32", "svht64"):
+            self.table.insert(self.keys, self.values, stream=stream)
+        else:
+            self.table.insert(self.keys, stream=stream)
+
+    def retrieve(self, stream):
+        self.table.retrieve(self.queries, self.out, stream=stream)
+
+    def verify(self):
+        """size-independent properties of one fresh step"""
+        import torch
+        s = torch.cuda.current_stream()
+        self.init(s)
+        self.insert(s)
+        if self.kind in ("svht32", "svht64"):
+            self.out.fill_(-1)
+            self.retrieve(s)
+            torch.cuda.synchronize()
+            ok_hits = bool(torch.equal(self.out[self.hit], self.expected[self.hit]))
+            ok_miss = bool((self.out[~self.hit] == -1).all())
+            ok_size = self.table.size() == self.n
+            return ok_hits and ok_miss and ok_size
+        if self.kind == "hashset64":
+            self.out.fill_(7)
+            self.retrieve(s)
+            torch.cuda.synchronize()
+            return bool((self.out == self.hit.to(torch.uint8)).all()) and self.table.size() == self.n
+        if self.kind == "counting32":
+            self.out.fill_(0)
+            self.retrieve(s)
+            torch.cuda.synchronize()
+            got = self.out[: self.distinct].to(torch.int64)
+            present = self.hist > 0
+            ok = bool(torch.equal(got[present], self.hist[present]))
+            return ok and bool((self.out[self.distinct:] == 0).all())
+        if self.kind == "bloom64":
+            self.retrieve(s)
+            torch.cuda.synchronize()
+            return bool(self.out[self.n:].all())
+        return False
+
+
+def zipf_ranks_t(n_in, s, n_out, gen, device):
+    """Zipf(s) ranks in [0, n_in) on the device by rejection sampling
+    (the published method random_distributions.cuh:285-310 follows)"""
+    import torch
+    t = (float(n_in) ** (1.0 - s) - s) / (1.0 - s)
+    out = torch.empty(n_out, dtype=torch.int64, device=device)
+    filled = 0
+    while filled < n_out:
+        m = int((n_out - filled) * 1.3) + 1024
+        p = torch.rand(m, dtype=torch.float64, device=device, generator=gen)
+        y = torch.rand(m, dtype=torch.float64, device=device, generator=gen)
+        pt = p * t
+        inv_b = torch.where(pt <= 1.0, pt, torch.pow(pt * (1.0 - s) + s, 1.0 / (1.0 - s)))
+        k = torch.floor(inv_b + 1.0)
+        b = torch.where(k <= 1.0, torch.full_like(inv_b, 1.0 / t), torch.pow(inv_b, -s) / t)
+        rat = torch.pow(k, -s) / (b * t)
+        acc = k[y < rat].clamp(max=n_in).to(torch.int64) - 1
+        take = min(acc.numel(), n_out - filled)
+        out[filled:filled + take] = acc[:take]
+        filled += take
+    return out
+
+
+WORKLOAD_NAMES = {
+    "svht64": "SingleValueHashTable<u64,u64> CG8 LF0.9: insert 2^{L} + retrieve 2^{L} (50% hit)",
+    "svht32": "SingleValueHashTable<u32,u32> CG8: insert 2^{L} + retrieve 2^{L} (50% hit)",
+    "hashset64": "HashSet<u64> CG16 LF0.9: insert 2^{L} + contains 2^{L} (50% hit)",
+    "counting32": "CountingHashTable<u32,u32> CG4 LF0.85: insert 2^{L} Zipf(1.1) + retrieve distinct+absent",
+    "bloom64": "BloomFilter<u64,Murmur64,u64,CG8> 16 bits/key k=8: insert 2^{L} + query 2^{L+1}",
+}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.gpus != world and world > 1:
+        log("warning: --gpus %d but WORLD_SIZE %d" % (args.gpus, world))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=device)
+
+    import warpcore_b200  # noqa: F401
+    warpcore_b200.lib()
+
+    wl = Workload(args.workload, args.log2n, args.load, rank, device)
+    stream = torch.cuda.Stream(device=device)
+    torch.cuda.synchronize()
+    verified = wl.verify()
+
+    # warm-up
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            wl.init(stream)
+            wl.insert(stream)
+            wl.retrieve(stream)
+    torch.cuda.synchronize()
+
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    wall0 = time.perf_counter()
+    t0.record(stream)
+    for k in range(args.steps):
+        ev[k][0].record(stream)
+        wl.init(stream)
+        ev[k][1].record(stream)
+        wl.insert(stream)
+        ev[k][2].record(stream)
+        wl.retrieve(stream)
+        ev[k][3].record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    total_ms = t0.elapsed_time(t1)
+    init_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    ins_ms = [e[1].elapsed_time(e[2]) for e in ev]
+    ret_ms = [e[2].elapsed_time(e[3]) for e in ev]
+    if world > 1:
+        tt = torch.tensor([total_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    ops_step = wl.n + wl.q
+    value = world * ops_step * args.steps / (total_ms * 1e-3) / 1e9
+
+    # end to end through the public API with host buffers
+    e2e = run_e2e(wl, stream, args, world) if not args.no_e2e else None
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        peak, peak_src = measured_peak()
+        ins_avg = statistics.mean(ins_ms)
+        ret_avg = statistics.mean(ret_ms)
+        if ins_avg >= ret_avg:
+            dom, dom_ms, dom_bytes, dom_ops = "insert", ins_avg, wl.bytes_insert, wl.n
+        else:
+            dom, dom_ms, dom_bytes, dom_ops = "retrieve", ret_avg, wl.bytes_retrieve, wl.q
+        achieved = dom_bytes * dom_ops / (dom_ms * 1e-3) / 1e9
+        tag = "%s_%s_2p%d" % (args.workload, dom, args.log2n)
+        traffic = profile_traffic(tag)
+        cpu = cpu_baseline(args) if not args.no_cpu else None
+        line = {
+            "metric": "insert+retrieve Gops/s (keys processed per second, whole job)",
+            "value": round(value, 4),
+            "unit": "Gops/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(total_ms / args.steps, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "u64" if wl.kb == 8 else "u32",
+            "data": "synthetic (seeded uniform unique keys, uniform values; inputs resident in HBM)",
+            "config": {
+                "workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n),
+                "capacity": int(wl.table.capacity) if hasattr(wl.table, "capacity") else None,
+                "ops_per_step": ops_step,
+                "l2": "inputs larger than L2 (no flush)" if args.log2n >= 24 else "inputs may be L2-resident",
+                "parallelism": "independent table per GPU" if world > 1 else "single GPU",
+            },
+            "insert_gops": round(wl.n / (statistics.mean(ins_ms) * 1e-3) / 1e9, 4),
+            "retrieve_gops": round(wl.q / (statistics.mean(ret_ms) * 1e-3) / 1e9, 4),
+            "init_ms": round(statistics.mean(init_ms), 4),
+            "insert_ms": round(statistics.mean(ins_ms), 4),
+            "retrieve_ms": round(statistics.mean(ret_ms), 4),
+            "verified": verified,
+            "roofline": {
+                "bound": "hbm",
+                "kernel": dom,
+                "achieved": round(achieved, 2),
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": round(achieved / peak, 4),
+                "peak_source": peak_src,
+                "algorithmic_bytes_per_op": dom_bytes,
+                "traffic": traffic,
+            },
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": 3 * args.steps,
+            "clocks": clocks,
+            "wall_s": round(wall, 3),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_e2e(wl, stream, args, world):
+    """Same workload through the public API with pinned host buffers: every
+    step copies its inputs host->device, runs init + insert + retrieve and
+    copies the results back."""
+    import torch
+    hk = wl.keys.cpu().pin_memory()
+    hv = wl.values.cpu().pin_memory() if wl.values is not None else None
+    hq = wl.queries.cpu().pin_memory()
+    ho = torch.empty(wl.out.shape, dtype=wl.out.dtype).pin_memory()
+    dk = torch.empty_like(wl.keys)
+    dv = torch.empty_like(wl.values) if wl.values is not None else None
+    dq = torch.empty_like(wl.queries)
+    h2d = hk.numel() * hk.element_size() + hq.numel() * hq.element_size()
+    if hv is not None:
+        h2d += hv.numel() * hv.element_size()
+    d2h = ho.numel() * ho.element_size()
+    keys0, vals0, q0 = wl.keys, wl.values, wl.queries
+    steps = max(1, min(args.steps, 3))
+
+    def step():
+        dk.copy_(hk, non_blocking=True)
+        if dv is not None:
+            dv.copy_(hv, non_blocking=True)
+        dq.copy_(hq, non_blocking=True)
+        wl.keys, wl.values, wl.queries = dk, dv, dq
+        wl.init(stream)
+        wl.insert(stream)
+        wl.retrieve(stream)
+        ho.copy_(wl.out, non_blocking=True)
+
+    with torch.cuda.stream(stream):
+        step()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            step()
+        b.record(stream)
+        torch.cuda.synchronize()
+    wl.keys, wl.values, wl.queries = keys0, vals0, q0
+    ms = a.elapsed_time(b)
+    ops = (wl.n + wl.q) * steps * world
+    return {"value": round(ops / (ms * 1e-3) / 1e9, 4), "unit": "Gops/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "steps": steps, "api": "warpcore_b200 Python binding over the C ABI"}
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (oracle port of the reference algorithm)
+# ---------------------------------------------------------------------------
+
+def cpu_sample(args, threads, reps):
+    """bounded sample of the workload on the host cores: insert + retrieve
+    2^log2s keys through the oracle's multi-threaded port"""
+    import numpy as np
+    from oracle import oracle as o
+    kb = 4 if args.workload in ("svht32", "counting32") else 8
+    log2s = args.cpu_log2n
+    n = 1 << log2s
+    keys = o.gen_unique_keys(kb, n + n // 2, 31)
+    ins = keys[:n]
+    vals = o.gen_uniform(kb, n, 32)
+    rng = np.random.default_rng(5)
+    q = np.concatenate([ins[rng.permutation(n)[: n - n // 2]], keys[n:]])
+    q = q[rng.permutation(n)]
+    cap = o.valid_capacity(int(n / args.load), 8)
+    t = o.MTTable(kb, cap, 8)
+    out = np.zeros(n, dtype=keys.dtype)
+    found = np.zeros(n, dtype=np.uint8)
+    best = None
+    for _ in range(reps):
+        t.clear(threads)
+        ti = t.insert(ins, vals, threads)
+        tr = t.retrieve(q, out, found, threads)
+        best = ti + tr if best is None else min(best, ti + tr)
+    ok = int(found.sum()) == n - n // 2
+    return 2 * n / best / 1e9, n, ok
+
+
+def cpu_baseline(args):
+    threads = os.cpu_count() or 1
+    v, n, ok = cpu_sample(args, threads, 3)
+    return {"value": round(v, 5), "unit": "Gops/s", "cores": threads, "kind": "port",
+            "sample": "insert 2^%d + retrieve 2^%d (50%% hit) at load %.2f, CG 8, min of 3"
+                      % (args.cpu_log2n, args.cpu_log2n, args.load),
+            "verified": ok}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    vals = []
+    for _ in range(args.warmup):
+        cpu_sample(args, threads, 1)
+    for _ in range(args.steps):
+        v, n, ok = cpu_sample(args, threads, 1)
+        vals.append(v)
+    value = statistics.mean(vals)
+    line = {
+        "impl": "reference",
+        "metric": "insert+retrieve Gops/s (keys processed per second, whole job)",
+        "value": round(value, 5),
+        "unit": "Gops/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(2 * (1 << args.cpu_log2n) / (value * 1e9) * 1e3, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u64" if args.workload not in ("svht32", "counting32") else "u32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n),
+                   "sample": "2^%d keys per step on the host" % args.cpu_log2n},
+        "cpu_baseline": {"value": round(value, 5), "unit": "Gops/s", "cores": threads,
+                         "kind": "port",
+                         "sample": "insert 2^%d + retrieve 2^%d per step, CG 8 windows, "
+                                   "reference lane order" % (args.cpu_log2n, args.cpu_log2n)},
+        "e2e": {"value": round(value, 5), "unit": "Gops/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "wall_s": round(time.perf_counter() - t0, 2),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="svht64", choices=sorted(WORKLOAD_NAMES))
+    ap.add_argument("--log2n", type=int, default=27)
+    ap.add_argument("--load", type=float, default=0.9)
+    ap.add_argument("--cpu-log2n", type=int, default=24)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("warm-up raised to 3 steps")
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

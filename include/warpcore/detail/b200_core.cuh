@@ -1,0 +1,439 @@
+/*
+ * b200_core.cuh -- device-side core of the B200-native warpcore library.
+ *
+ * Shared by the bulk kernels compiled into libwarpcore_b200.so and by the
+ * C++ drop-in headers' device-side per-key API, so that both agree on the
+ * table layout and probe order.
+ *
+ * Layout in HBM
+ *   The slot array is the reference's AoS store (storage.cuh:165-187,
+ *   438-645): {Key key; Value value;} per slot, a bare Key for hash sets.
+ *   u32/u32 slots are one 64-bit word (key in the low half), u64/u64 slots
+ *   one 16-byte word, so a slot is claimed with ONE compare-and-swap that
+ *   publishes key and value together (64-bit atomicCAS, 128-bit atom.cas).
+ *
+ * Probing
+ *   The reference probes cg_size consecutive, unaligned slots per step
+ *   (probing_schemes.cuh:79-100).  Here the table is split into buckets of
+ *   cg_size slots that start on a bucket boundary, so a probe window is one
+ *   aligned, sector-multiple block read with 16-byte vector loads.  The
+ *   number of buckets is capacity / cg_size, which under the reference's
+ *   capacity rule (base.cuh:27-34) is a prime, and the probing schemes are
+ *   restated over buckets:
+ *     double hashing  b0 = h1(key+seed) % nb,
+ *                     step = h2(key+seed+1) % (nb-1) + 1, b = (b+step) % nb
+ *     linear          b = (b+1) % nb
+ *     quadratic       b = (b+1) % nb, (b+2) % nb, ... (step grows by one)
+ *   With nb prime, double hashing and linear probing visit every bucket in
+ *   nb windows (cycle-free like the reference's), so probing stops after at
+ *   most nb windows and reports probing_length_exceeded instead of spinning.
+ *   Slot placement therefore differs from the reference; results (values,
+ *   flags, counts, statuses, table contents as a multiset) do not.
+ */
+#ifndef WARPCORE_B200_CORE_CUH
+#define WARPCORE_B200_CORE_CUH
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace warpcore {
+namespace b200 {
+
+/* Status bits (status.cuh:44-68) */
+enum : uint32_t {
+    kStNone = 0u,
+    kStUnknownError = 1u << 0,
+    kStProbingLengthExceeded = 1u << 1,
+    kStInvalidConfiguration = 1u << 2,
+    kStInvalidKey = 1u << 3,
+    kStDuplicateKey = 1u << 4,
+    kStKeyNotFound = 1u << 5,
+    kStIndexOverflow = 1u << 6,
+    kStOutOfMemory = 1u << 7,
+    kStNotInitialized = 1u << 8,
+};
+
+enum : uint32_t {
+    kHashMurmur = 0,
+    kHashNvidia = 1,
+    kHashMueller = 2,
+    kHashIdentity32 = 3,
+    kHashIdentity64 = 4,
+};
+
+enum : uint32_t { kProbeDouble = 0, kProbeLinear = 1, kProbeQuadratic = 2 };
+
+enum : int { kHandlerNothing = 0, kHandlerStatus = 1, kHandlerBoolean = 2 };
+
+/* ------------------------------------------------------------------ */
+/* hashers (hashers.cuh:34-44, 70-77, 116-139, 147-175)                */
+/* ------------------------------------------------------------------ */
+
+__host__ __device__ __forceinline__ uint32_t fmix32(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x85ebca6bu;
+    x ^= x >> 13;
+    x *= 0xc2b2ae35u;
+    x ^= x >> 16;
+    return x;
+}
+
+__host__ __device__ __forceinline__ uint64_t fmix64(uint64_t x)
+{
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
+}
+
+__host__ __device__ __forceinline__ uint32_t nvidia_hash32(uint32_t x)
+{
+    x = (x + 0x7ed55d16u) + (x << 12);
+    x = (x ^ 0xc761c23cu) ^ (x >> 19);
+    x = (x + 0x165667b1u) + (x << 5);
+    x = (x + 0xd3a2646cu) ^ (x << 9);
+    x = (x + 0xfd7046c5u) + (x << 3);
+    x = (x ^ 0xb55a4f09u) ^ (x >> 16);
+    return x;
+}
+
+__host__ __device__ __forceinline__ uint32_t mueller_hash32(uint32_t x)
+{
+    x = ((x >> 16) ^ x) * 0x45d9f3bu;
+    x = ((x >> 16) ^ x) * 0x45d9f3bu;
+    x = ((x >> 16) ^ x);
+    return x;
+}
+
+template <class K>
+__host__ __device__ __forceinline__ uint64_t hash_key(uint32_t hasher, K x)
+{
+    switch (hasher) {
+    case kHashMurmur:
+        return sizeof(K) == 4 ? uint64_t(fmix32(uint32_t(x)))
+                              : fmix64(uint64_t(x));
+    case kHashNvidia: return nvidia_hash32(uint32_t(x));
+    case kHashMueller: return mueller_hash32(uint32_t(x));
+    case kHashIdentity32: return uint32_t(x);
+    default: return uint64_t(x);
+    }
+}
+
+/* x % m, with the cheaper 32-bit path when both fit */
+__host__ __device__ __forceinline__ uint64_t mod_u64(uint64_t x, uint64_t m)
+{
+    if (((x | m) >> 32) == 0) return uint32_t(x) % uint32_t(m);
+    return x % m;
+}
+
+/* ------------------------------------------------------------------ */
+/* table view and bucket probing                                        */
+/* ------------------------------------------------------------------ */
+
+struct TableView {
+    void *slots;
+    uint32_t *status;
+    uint64_t num_buckets; /* capacity / cg_size; prime under the capacity rule */
+    uint64_t seed;
+    uint64_t empty_key;
+    uint64_t tombstone_key;
+    uint64_t max_count;
+    uint32_t probing, hasher1, hasher2, cg_size;
+};
+
+template <class K>
+__host__ __device__ __forceinline__ uint64_t probe_begin(const TableView &t, K key)
+{
+    const K k = K(key + K(t.seed));
+    return mod_u64(hash_key<K>(t.hasher1, k), t.num_buckets);
+}
+
+template <class K>
+__host__ __device__ __forceinline__ uint64_t probe_step(const TableView &t, K key)
+{
+    if (t.probing != kProbeDouble || t.num_buckets < 2) return 1;
+    const K k = K(key + K(t.seed) + K(1));
+    return mod_u64(hash_key<K>(t.hasher2, k), t.num_buckets - 1) + 1;
+}
+
+/* advance to the next bucket; `step` grows by one per window for
+ * quadratic probing */
+__host__ __device__ __forceinline__ uint64_t probe_next(const TableView &t,
+                                                        uint64_t b,
+                                                        uint64_t &step)
+{
+    uint64_t s = step;
+    if (s >= t.num_buckets) s = mod_u64(s, t.num_buckets);
+    b += s;
+    if (b >= t.num_buckets) b -= t.num_buckets;
+    if (t.probing == kProbeQuadratic) step++;
+    return b;
+}
+
+/* windows the reference visits for a probing length: SDIV(pl, cg) windows
+ * (probing_schemes.cuh:61, same unsigned wrap), at least one; capped at the
+ * number of buckets */
+__host__ __device__ __forceinline__ uint64_t max_windows(uint64_t probing_length,
+                                                         uint64_t cg,
+                                                         uint64_t num_buckets)
+{
+    uint64_t w = (probing_length + cg - 1) / cg;
+    if (w == 0) w = 1;
+    return w < num_buckets ? w : num_buckets;
+}
+
+/* ------------------------------------------------------------------ */
+/* slot layouts                                                          */
+/* ------------------------------------------------------------------ */
+
+/* u32 key, u32 value: one 64-bit word, key in the low half */
+struct LayoutKV32 {
+    using key_t = uint32_t;
+    using val_t = uint32_t;
+    static constexpr int kSlotBytes = 8;
+    static constexpr bool kHasValue = true;
+};
+/* u64 key, u64 value: one 16-byte word */
+struct LayoutKV64 {
+    using key_t = uint64_t;
+    using val_t = uint64_t;
+    static constexpr int kSlotBytes = 16;
+    static constexpr bool kHasValue = true;
+};
+/* hash set of u32 / u64 keys */
+struct LayoutSet32 {
+    using key_t = uint32_t;
+    using val_t = uint32_t;
+    static constexpr int kSlotBytes = 4;
+    static constexpr bool kHasValue = false;
+};
+struct LayoutSet64 {
+    using key_t = uint64_t;
+    using val_t = uint64_t;
+    static constexpr int kSlotBytes = 8;
+    static constexpr bool kHasValue = false;
+};
+
+/* up to 16 bytes of a probe window held by one lane */
+struct LaneWords {
+    uint32_t w[4];
+};
+
+template <int kBytes>
+__device__ __forceinline__ LaneWords load_lane(const void *p)
+{
+    LaneWords r;
+    if constexpr (kBytes == 16) {
+        const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(p));
+        r.w[0] = v.x; r.w[1] = v.y; r.w[2] = v.z; r.w[3] = v.w;
+    } else if constexpr (kBytes == 8) {
+        const uint2 v = __ldcg(reinterpret_cast<const uint2 *>(p));
+        r.w[0] = v.x; r.w[1] = v.y; r.w[2] = 0; r.w[3] = 0;
+    } else {
+        r.w[0] = __ldcg(reinterpret_cast<const unsigned int *>(p));
+        r.w[1] = 0; r.w[2] = 0; r.w[3] = 0;
+    }
+    return r;
+}
+
+template <class L>
+__device__ __forceinline__ typename L::key_t slot_key(const LaneWords &lw, int s)
+{
+    if constexpr (L::kSlotBytes == 4) return lw.w[s];
+    else if constexpr (L::kSlotBytes == 8 && !L::kHasValue)
+        return uint64_t(lw.w[2 * s]) | (uint64_t(lw.w[2 * s + 1]) << 32);
+    else if constexpr (L::kSlotBytes == 8) return lw.w[2 * s];
+    else return uint64_t(lw.w[0]) | (uint64_t(lw.w[1]) << 32);
+}
+
+template <class L>
+__device__ __forceinline__ typename L::val_t slot_val(const LaneWords &lw, int s)
+{
+    if constexpr (L::kSlotBytes == 8 && L::kHasValue) return lw.w[2 * s + 1];
+    else if constexpr (L::kSlotBytes == 16)
+        return uint64_t(lw.w[2]) | (uint64_t(lw.w[3]) << 32);
+    else return 0;
+}
+
+/* 128-bit compare-and-swap (atom.cas.b128, sm_90 and newer) */
+__device__ __forceinline__ void cas128(void *addr, uint64_t cmp_lo,
+                                       uint64_t cmp_hi, uint64_t new_lo,
+                                       uint64_t new_hi, uint64_t &old_lo,
+                                       uint64_t &old_hi)
+{
+    asm volatile(
+        "{\n\t"
+        ".reg .b128 cmp, nv, old;\n\t"
+        "mov.b128 cmp, {%2, %3};\n\t"
+        "mov.b128 nv, {%4, %5};\n\t"
+        "atom.global.cas.b128 old, [%6], cmp, nv;\n\t"
+        "mov.b128 {%0, %1}, old;\n\t"
+        "}"
+        : "=l"(old_lo), "=l"(old_hi)
+        : "l"(cmp_lo), "l"(cmp_hi), "l"(new_lo), "l"(new_hi), "l"(addr)
+        : "memory");
+}
+
+/* Claim an empty slot for key with payload v (value or initial count).
+ * Empty slots hold the empty key and a zero payload (the init kernels write
+ * whole slots).  Returns true on success; otherwise old_key is the key now
+ * in the slot. */
+template <class L>
+__device__ __forceinline__ bool claim_slot(void *sp, typename L::key_t empty,
+                                           typename L::key_t key,
+                                           typename L::val_t v,
+                                           typename L::key_t &old_key)
+{
+    if constexpr (L::kSlotBytes == 4) {
+        old_key = atomicCAS(reinterpret_cast<unsigned int *>(sp), empty, key);
+        return old_key == empty;
+    } else if constexpr (L::kSlotBytes == 8 && !L::kHasValue) {
+        old_key = atomicCAS(reinterpret_cast<unsigned long long *>(sp),
+                            (unsigned long long)empty, (unsigned long long)key);
+        return old_key == empty;
+    } else if constexpr (L::kSlotBytes == 8) {
+        unsigned long long expect = (unsigned long long)empty;
+        const unsigned long long nw =
+            (unsigned long long)key | ((unsigned long long)v << 32);
+        for (int tries = 0; tries < 4; ++tries) {
+            const unsigned long long old =
+                atomicCAS(reinterpret_cast<unsigned long long *>(sp), expect, nw);
+            if (old == expect) return true;
+            old_key = uint32_t(old);
+            if (old_key != empty) return false;
+            expect = old; /* empty key with a stale payload: retry on it */
+        }
+        return false;
+    } else {
+        uint64_t exp_lo = empty, exp_hi = 0;
+        for (int tries = 0; tries < 4; ++tries) {
+            uint64_t olo, ohi;
+            cas128(sp, exp_lo, exp_hi, key, v, olo, ohi);
+            if (olo == exp_lo && ohi == exp_hi) return true;
+            old_key = olo;
+            if (old_key != empty) return false;
+            exp_hi = ohi;
+        }
+        return false;
+    }
+}
+
+template <class L>
+__device__ __forceinline__ typename L::val_t *slot_value_ptr(void *sp)
+{
+    if constexpr (L::kSlotBytes == 8)
+        return reinterpret_cast<uint32_t *>(sp) + 1;
+    else
+        return reinterpret_cast<typename L::val_t *>(reinterpret_cast<uint64_t *>(sp) + 1);
+}
+
+template <class L>
+__device__ __forceinline__ void store_value(void *sp, typename L::val_t v)
+{
+    if constexpr (L::kHasValue) {
+        volatile typename L::val_t *p = slot_value_ptr<L>(sp);
+        *p = v;
+    }
+}
+
+template <class L>
+__device__ __forceinline__ void store_key(void *sp, typename L::key_t k)
+{
+    volatile typename L::key_t *p = reinterpret_cast<typename L::key_t *>(sp);
+    *p = k;
+}
+
+/* width-generic wrappers: uint64_t is unsigned long on LP64, while the CUDA
+ * intrinsics are declared for unsigned long long */
+template <class T>
+__device__ __forceinline__ T atomic_add_any(T *p, T v)
+{
+    if constexpr (sizeof(T) == 8)
+        return T(atomicAdd(reinterpret_cast<unsigned long long *>(p), (unsigned long long)v));
+    else
+        return T(atomicAdd(reinterpret_cast<unsigned int *>(p), (unsigned int)v));
+}
+
+template <class T>
+__device__ __forceinline__ T atomic_exch_any(T *p, T v)
+{
+    if constexpr (sizeof(T) == 8)
+        return T(atomicExch(reinterpret_cast<unsigned long long *>(p), (unsigned long long)v));
+    else
+        return T(atomicExch(reinterpret_cast<unsigned int *>(p), (unsigned int)v));
+}
+
+template <class T>
+__device__ __forceinline__ T ld_stream(const T *p)
+{
+    if constexpr (sizeof(T) == 8)
+        return T(__ldcs(reinterpret_cast<const unsigned long long *>(p)));
+    else if constexpr (sizeof(T) == 4)
+        return T(__ldcs(reinterpret_cast<const unsigned int *>(p)));
+    else
+        return *p;
+}
+
+template <class T>
+__device__ __forceinline__ void st_stream(T *p, T v)
+{
+    if constexpr (sizeof(T) == 8)
+        __stcs(reinterpret_cast<unsigned long long *>(p), (unsigned long long)v);
+    else if constexpr (sizeof(T) == 4)
+        __stcs(reinterpret_cast<unsigned int *>(p), (unsigned int)v);
+    else
+        *p = v;
+}
+
+/* counting increment with the reference's wrap guard
+ * (counting_hash_table.cuh:152-169), c occurrences at once */
+template <class L>
+__device__ __forceinline__ void count_add(void *sp, uint32_t c, uint64_t max_count,
+                                          uint32_t &st, uint32_t &join)
+{
+    using V = typename L::val_t;
+    V *vp = slot_value_ptr<L>(sp);
+    const V old = atomic_add_any(vp, V(c));
+    if (V(old + V(c)) < old) {
+        st |= kStIndexOverflow;
+        join |= kStIndexOverflow;
+        atomic_exch_any(vp, V(max_count));
+    }
+}
+
+/* window bit of (lane-in-group qq, slot s) is qq * SPL + s */
+template <int TPK, int SPL>
+__device__ __forceinline__ uint32_t spread_bits(uint32_t group_bits, int s)
+{
+    if constexpr (SPL == 1) {
+        return group_bits;
+    } else {
+        uint32_t r = 0;
+#pragma unroll
+        for (int qq = 0; qq < TPK; ++qq)
+            r |= ((group_bits >> qq) & 1u) << (qq * SPL + s);
+        return r;
+    }
+}
+
+__device__ __forceinline__ int nth_set_bit(uint32_t mask, int n)
+{
+    return int(__fns(mask, 0, n + 1));
+}
+
+__device__ __forceinline__ void join_status(uint32_t *status, uint32_t bits)
+{
+    /* Status::atomic_join (status.cuh:187-193) */
+    if (bits) {
+        const uint32_t cur = *reinterpret_cast<volatile uint32_t *>(status);
+        if ((cur & bits) != bits) atomicOr(status, bits);
+    }
+}
+
+} // namespace b200
+} // namespace warpcore
+
+#endif /* WARPCORE_B200_CORE_CUH */

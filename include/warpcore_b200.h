@@ -1,0 +1,271 @@
+/*
+ * warpcore_b200.h -- C ABI of the B200-native warpcore library.
+ *
+ * The reference (sleeepyjack/warpcore) is a header-only C++ template library
+ * with no C ABI; its host "bulk" methods are the boundary this library
+ * replaces.  Each entry point below names the reference method it stands in
+ * for (paths relative to the warpcore project).  The C++ drop-in headers in
+ * include/warpcore/ call these functions; foreign callers (ctypes, cgo, JNI)
+ * bind them directly.
+ *
+ * Conventions
+ *  - Every function returns an int error code (WC_OK == 0) and never throws.
+ *    A short message for the last failure on the calling thread is in
+ *    wc_last_error().
+ *  - Key, value, status and flag buffers are DEVICE pointers owned by the
+ *    caller, exactly like the reference's bulk methods.
+ *  - Bulk operations are asynchronous on the given stream (NULL = legacy
+ *    default stream).  size, retrieve_all, peek_status, pop_status,
+ *    *_create and *_init synchronise that stream, as the reference does.
+ *  - probing_length is the reference's maximum number of probed slots per
+ *    key; the library probes at most ceil(probing_length / cg_size) windows
+ *    and never more windows than the table has, so a full table reports
+ *    WC_STATUS_PROBING_LENGTH_EXCEEDED instead of spinning.
+ *  - Per-key status output (status_out, may be NULL) follows the reference's
+ *    status handlers: WC_HANDLER_NOTHING (ReturnNothing), WC_HANDLER_STATUS
+ *    (ReturnStatus: one uint32 Status per key) and WC_HANDLER_BOOLEAN
+ *    (ReturnBoolean<ignore>: one byte per key, computed with the reference's
+ *    own Status algebra, status.cuh:142-146 and :316-330).
+ */
+#ifndef WARPCORE_B200_H
+#define WARPCORE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* cudaStream_t without pulling in the CUDA headers */
+typedef struct CUstream_st *wc_stream_t;
+
+/* ---- error codes ---- */
+#define WC_OK 0
+#define WC_ERR_INVALID_ARGUMENT (-1)
+#define WC_ERR_CUDA (-2)
+#define WC_ERR_OUT_OF_MEMORY (-3)
+#define WC_ERR_NOT_INITIALIZED (-4)
+#define WC_ERR_UNSUPPORTED (-5)
+
+/* ---- Status bits: identical to warpcore::Status (status.cuh:44-68) ---- */
+#define WC_STATUS_NONE 0u
+#define WC_STATUS_UNKNOWN_ERROR (1u << 0)
+#define WC_STATUS_PROBING_LENGTH_EXCEEDED (1u << 1)
+#define WC_STATUS_INVALID_CONFIGURATION (1u << 2)
+#define WC_STATUS_INVALID_KEY (1u << 3)
+#define WC_STATUS_DUPLICATE_KEY (1u << 4)
+#define WC_STATUS_KEY_NOT_FOUND (1u << 5)
+#define WC_STATUS_INDEX_OVERFLOW (1u << 6)
+#define WC_STATUS_OUT_OF_MEMORY (1u << 7)
+#define WC_STATUS_NOT_INITIALIZED (1u << 8)
+#define WC_STATUS_DRY_RUN (1u << 9)
+#define WC_STATUS_INVALID_PHASE_OVERLAP (1u << 10)
+#define WC_STATUS_MAX_VALUES_FOR_KEY_REACHED (1u << 11)
+#define WC_STATUS_INVALID_VALUE (1u << 12)
+
+/* ---- per-key status handlers (status.cuh:278-333) ---- */
+#define WC_HANDLER_NOTHING 0
+#define WC_HANDLER_STATUS 1
+#define WC_HANDLER_BOOLEAN 2
+
+/* ---- hashers (hashers.cuh:14-175) ---- */
+#define WC_HASH_MURMUR 0     /* MurmurHash<Key> */
+#define WC_HASH_NVIDIA 1     /* NvidiaHash (32-bit keys) */
+#define WC_HASH_MUELLER 2    /* MuellerHash (32-bit keys) */
+#define WC_HASH_IDENTITY32 3 /* IdentityMap<Key, uint32_t> */
+#define WC_HASH_IDENTITY64 4 /* IdentityMap<Key, uint64_t> */
+
+/* ---- probing schemes (probing_schemes.cuh:22-305) ---- */
+#define WC_PROBING_DOUBLE 0    /* DoubleHashing<H1, H2, CG> */
+#define WC_PROBING_LINEAR 1    /* LinearProbing<H, CG> */
+#define WC_PROBING_QUADRATIC 2 /* QuadraticProbing<H, CG> */
+
+/* Template knobs of SingleValueHashTable / HashSet / CountingHashTable
+ * (single_value_hash_table.cuh:29-37, hash_set.cuh:16-22,
+ * counting_hash_table.cuh:18-26) as run-time values. */
+typedef struct wc_table_config {
+    uint32_t key_bytes;     /* 4 or 8 */
+    uint32_t value_bytes;   /* 4 or 8, equal to key_bytes; 0 for a hash set */
+    uint64_t empty_key;     /* EmptyKey, default 0 */
+    uint64_t tombstone_key; /* TombstoneKey, default ~0 */
+    uint32_t probing;       /* WC_PROBING_* */
+    uint32_t hasher1;       /* WC_HASH_*, probing hash */
+    uint32_t hasher2;       /* WC_HASH_*, step hash (double hashing) */
+    uint32_t cg_size;       /* cooperative group size = probe window width
+                               in slots: 1, 2, 4, 8, 16 or 32 */
+} wc_table_config;
+
+/* Read-only description of a table, for the device-side per-key API. */
+typedef struct wc_table_info {
+    uint32_t kind;          /* 0 single-value, 1 hash set, 2 counting */
+    uint32_t key_bytes, value_bytes, slot_bytes, cg_size;
+    uint32_t probing, hasher1, hasher2;
+    uint64_t capacity;      /* slots, reference capacity rule */
+    uint64_t num_buckets;   /* capacity / cg_size */
+    uint64_t seed, empty_key, tombstone_key, max_count;
+    uint64_t bytes_total;
+    void *slots;            /* device pointer to the slot array */
+    uint32_t *status;       /* device pointer to the table's Status word */
+    int is_initialized;
+} wc_table_info;
+
+typedef struct wc_table wc_table;
+
+/* last error message of the calling thread ("" if none) */
+const char *wc_last_error(void);
+/* library version string */
+const char *wc_version(void);
+
+/* Default knobs of each table kind: MurmurHash, DoubleHashing, sentinels
+ * 0 / ~0 and CG 8 (single-value), 16 (hash set), 4 (counting)
+ * (defaults.cuh:11-42). */
+void wc_svht_default_config(wc_table_config *cfg, uint32_t key_bytes,
+                            uint32_t value_bytes);
+void wc_hashset_default_config(wc_table_config *cfg, uint32_t key_bytes);
+void wc_counting_default_config(wc_table_config *cfg, uint32_t key_bytes,
+                                uint32_t value_bytes);
+
+/* Capacity rule of the reference: detail::get_valid_capacity
+ * (base.cuh:27-34 with primes.hpp). 0 if min_capacity is beyond the table. */
+uint64_t wc_valid_capacity(uint64_t min_capacity, uint64_t cg_size);
+
+/* ------------------------------------------------------------------ */
+/* SingleValueHashTable<Key, Value, ...>                               */
+/* ------------------------------------------------------------------ */
+
+/* SingleValueHashTable(min_capacity, seed, no_init)
+ * (single_value_hash_table.cuh:112-128) */
+int wc_svht_create(const wc_table_config *cfg, uint64_t min_capacity,
+                   uint64_t seed, int no_init, wc_table **out);
+/* ~SingleValueHashTable (single_value_hash_table.cuh:162-169); also destroys
+ * hash sets and counting tables */
+int wc_table_destroy(wc_table *t);
+/* init(seed, stream) (single_value_hash_table.cuh:176-192); hash sets and
+ * counting tables too (hash_set.cuh:161-175, counting_hash_table.cuh:114-124) */
+int wc_table_init(wc_table *t, uint64_t seed, wc_stream_t stream);
+/* insert(keys_in, values_in, num_in, stream, probing_length, status_out)
+ * (single_value_hash_table.cuh:241-258) */
+int wc_svht_insert(wc_table *t, const void *keys_in, const void *values_in,
+                   uint64_t num_in, wc_stream_t stream,
+                   uint64_t probing_length, void *status_out,
+                   int status_handler, uint32_t ignore);
+/* retrieve(keys_in, num_in, values_out, stream, probing_length, status_out)
+ * (single_value_hash_table.cuh:320-337); values_out is written on hits only */
+int wc_svht_retrieve(wc_table *t, const void *keys_in, uint64_t num_in,
+                     void *values_out, wc_stream_t stream,
+                     uint64_t probing_length, void *status_out,
+                     int status_handler, uint32_t ignore);
+/* erase(keys_in, num_in, stream, probing_length, status_out)
+ * (single_value_hash_table.cuh:480-496) */
+int wc_svht_erase(wc_table *t, const void *keys_in, uint64_t num_in,
+                  wc_stream_t stream, uint64_t probing_length,
+                  void *status_out, int status_handler, uint32_t ignore);
+/* size(stream) (single_value_hash_table.cuh:535-592); blocking */
+int wc_table_size(wc_table *t, wc_stream_t stream, uint64_t *size_out);
+/* retrieve_all(keys_out, values_out, num_out, stream)
+ * (single_value_hash_table.cuh:391-417, hash_set.cuh:367-384); blocking;
+ * values_out may be NULL and is ignored for hash sets */
+int wc_table_retrieve_all(wc_table *t, void *keys_out, void *values_out,
+                          uint64_t *num_out, wc_stream_t stream);
+/* peek_status(stream) / pop_status(stream)
+ * (single_value_hash_table.cuh:646-687); blocking */
+int wc_table_peek_status(wc_table *t, wc_stream_t stream, uint32_t *out);
+int wc_table_pop_status(wc_table *t, wc_stream_t stream, uint32_t *out);
+/* capacity(), bytes_total(), seed(), is_initialized() and the device view */
+int wc_table_get_info(const wc_table *t, wc_table_info *info);
+
+/* ------------------------------------------------------------------ */
+/* HashSet<Key, ...>                                                   */
+/* ------------------------------------------------------------------ */
+
+/* HashSet(min_capacity, seed) (hash_set.cuh:81-110) */
+int wc_hashset_create(const wc_table_config *cfg, uint64_t min_capacity,
+                      uint64_t seed, wc_table **out);
+/* insert(keys_in, num_in, stream, probing_length, status_out)
+ * (hash_set.cuh:266-282) */
+int wc_hashset_insert(wc_table *t, const void *keys_in, uint64_t num_in,
+                      wc_stream_t stream, uint64_t probing_length,
+                      void *status_out, int status_handler, uint32_t ignore);
+/* retrieve(keys_in, num_in, flags_out, stream, probing_length, status_out)
+ * (hash_set.cuh:342-359 host form; the device form :292-329 it launches);
+ * flags_out is one byte per key (C++ bool), written when the key's status
+ * is none */
+int wc_hashset_retrieve(wc_table *t, const void *keys_in, uint64_t num_in,
+                        uint8_t *flags_out, wc_stream_t stream,
+                        uint64_t probing_length, void *status_out,
+                        int status_handler, uint32_t ignore);
+/* erase(keys_in, num_in, stream, probing_length, status_out)
+ * (hash_set.cuh:450-462) */
+int wc_hashset_erase(wc_table *t, const void *keys_in, uint64_t num_in,
+                     wc_stream_t stream, uint64_t probing_length,
+                     void *status_out, int status_handler, uint32_t ignore);
+
+/* ------------------------------------------------------------------ */
+/* CountingHashTable<Key, Value, ...>                                  */
+/* ------------------------------------------------------------------ */
+
+/* CountingHashTable(min_capacity, seed, max_count, no_init)
+ * (counting_hash_table.cuh:75-85) */
+int wc_counting_create(const wc_table_config *cfg, uint64_t min_capacity,
+                       uint64_t seed, uint64_t max_count, int no_init,
+                       wc_table **out);
+/* insert(keys_in, num_in, stream, probing_length, status_out)
+ * (counting_hash_table.cuh:184-194) */
+int wc_counting_insert(wc_table *t, const void *keys_in, uint64_t num_in,
+                       wc_stream_t stream, uint64_t probing_length,
+                       void *status_out, int status_handler, uint32_t ignore);
+/* retrieve(keys_in, num_in, values_out, stream, probing_length, status_out)
+ * (counting_hash_table.cuh:238-249); counts clamped to max_count, written
+ * on hits only */
+int wc_counting_retrieve(wc_table *t, const void *keys_in, uint64_t num_in,
+                         void *values_out, wc_stream_t stream,
+                         uint64_t probing_length, void *status_out,
+                         int status_handler, uint32_t ignore);
+/* erase (counting_hash_table.cuh:292-301, with the stream passed through) */
+int wc_counting_erase(wc_table *t, const void *keys_in, uint64_t num_in,
+                      wc_stream_t stream, uint64_t probing_length,
+                      void *status_out, int status_handler, uint32_t ignore);
+
+/* ------------------------------------------------------------------ */
+/* BloomFilter<Key, Hasher, Slot, CGSize>                               */
+/* ------------------------------------------------------------------ */
+
+typedef struct wc_bloom_config {
+    uint32_t key_bytes;  /* 4 or 8 */
+    uint32_t slot_bytes; /* 4 or 8 */
+    uint32_t cg_size;    /* slots per block: 1, 2, 4, 8, 16 or 32 */
+    uint32_t hasher;     /* WC_HASH_* */
+} wc_bloom_config;
+
+typedef struct wc_bloom_info {
+    uint32_t key_bytes, slot_bytes, cg_size, hasher;
+    uint64_t num_bits, num_slots, num_blocks, k, seed;
+    void *words; /* device pointer to the bit vector */
+} wc_bloom_info;
+
+typedef struct wc_bloom wc_bloom;
+
+/* BloomFilter(num_bits, k, seed) (bloom_filter.cuh:78-93) */
+int wc_bloom_create(const wc_bloom_config *cfg, uint64_t num_bits, uint64_t k,
+                    uint64_t seed, wc_bloom **out);
+/* ~BloomFilter (bloom_filter.cuh:130-138) */
+int wc_bloom_destroy(wc_bloom *b);
+/* init(seed, stream) (bloom_filter.cuh:143-152) */
+int wc_bloom_init(wc_bloom *b, uint64_t seed, wc_stream_t stream);
+/* insert(keys_in, num_in, stream) (bloom_filter.cuh:200-208) */
+int wc_bloom_insert(wc_bloom *b, const void *keys_in, uint64_t num_in,
+                    wc_stream_t stream);
+/* retrieve(keys_in, num_in, flags_out, stream) (bloom_filter.cuh:246-255) */
+int wc_bloom_retrieve(wc_bloom *b, const void *keys_in, uint64_t num_in,
+                      uint8_t *flags_out, wc_stream_t stream);
+/* num_bits(), num_slots(), num_blocks(), k() and the device view */
+int wc_bloom_get_info(const wc_bloom *b, wc_bloom_info *info);
+/* fpr(n) (bloom_filter.cuh:342-354), the reference's own formula */
+int wc_bloom_fpr(const wc_bloom *b, uint64_t n, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WARPCORE_B200_H */

@@ -1,0 +1,911 @@
+/*
+ * wc_oracle.c -- TEST INFRASTRUCTURE ONLY: CPU restatement of warpcore's hot
+ * path, used as the checker for the CUDA library.  Every function cites the
+ * reference file:line it follows (paths relative to the warpcore project).
+ * See wc_oracle.h for the parity pin.
+ */
+#define _GNU_SOURCE
+#include "wc_oracle.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+/* ------------------------------------------------------------------------ */
+/* hashers (hashers.cuh:34-44 NvidiaHash, :70-77 MuellerHash,
+ *          :116-124 fmix32, :131-139 fmix64, :147-175 IdentityMap)          */
+/* ------------------------------------------------------------------------ */
+
+static uint32_t fmix32(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x85ebca6bu;
+    x ^= x >> 13;
+    x *= 0xc2b2ae35u;
+    x ^= x >> 16;
+    return x;
+}
+
+static uint64_t fmix64(uint64_t x)
+{
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
+}
+
+static uint32_t nvidia32(uint32_t x)
+{
+    x = (x + 0x7ed55d16u) + (x << 12);
+    x = (x ^ 0xc761c23cu) ^ (x >> 19);
+    x = (x + 0x165667b1u) + (x << 5);
+    x = (x + 0xd3a2646cu) ^ (x << 9);
+    x = (x + 0xfd7046c5u) + (x << 3);
+    x = (x ^ 0xb55a4f09u) ^ (x >> 16);
+    return x;
+}
+
+static uint32_t mueller32(uint32_t x)
+{
+    x = ((x >> 16) ^ x) * 0x45d9f3bu;
+    x = ((x >> 16) ^ x) * 0x45d9f3bu;
+    x = ((x >> 16) ^ x);
+    return x;
+}
+
+static uint64_t kmask(int key_bytes)
+{
+    return key_bytes == 4 ? 0xffffffffull : ~0ull;
+}
+
+int wco_hash_bits(int hasher, int key_bytes)
+{
+    switch (hasher) {
+    case WCO_HASH_MURMUR: return key_bytes * 8;
+    case WCO_HASH_NVIDIA:
+    case WCO_HASH_MUELLER:
+    case WCO_HASH_IDENTITY32: return 32;
+    default: return 64;
+    }
+}
+
+uint64_t wco_hash(int hasher, int key_bytes, uint64_t x)
+{
+    x &= kmask(key_bytes);
+    switch (hasher) {
+    case WCO_HASH_MURMUR:
+        return key_bytes == 4 ? (uint64_t)fmix32((uint32_t)x) : fmix64(x);
+    case WCO_HASH_NVIDIA: return nvidia32((uint32_t)x);
+    case WCO_HASH_MUELLER: return mueller32((uint32_t)x);
+    case WCO_HASH_IDENTITY32: return (uint32_t)x;
+    default: return x;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* prime chain (utils/generate_primes_hpp.py:20-43, defaults :70-73):
+ * p0 = first prime >= 131072, p[i+1] = first prime >= p[i] + 131072,
+ * up to 17177772037.  Computed here with a deterministic Miller-Rabin.     */
+/* ------------------------------------------------------------------------ */
+
+static uint64_t mulmod(uint64_t a, uint64_t b, uint64_t m)
+{
+    return (uint64_t)((unsigned __int128)a * b % m);
+}
+
+static uint64_t powmod(uint64_t a, uint64_t e, uint64_t m)
+{
+    uint64_t r = 1;
+    a %= m;
+    while (e) {
+        if (e & 1) r = mulmod(r, a, m);
+        a = mulmod(a, a, m);
+        e >>= 1;
+    }
+    return r;
+}
+
+static int is_prime_u64(uint64_t n)
+{
+    static const uint64_t small[] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+    if (n < 2) return 0;
+    for (int i = 0; i < 12; i++) {
+        if (n == small[i]) return 1;
+        if (n % small[i] == 0) return 0;
+    }
+    uint64_t d = n - 1;
+    int s = 0;
+    while ((d & 1) == 0) { d >>= 1; s++; }
+    for (int i = 0; i < 12; i++) {
+        uint64_t x = powmod(small[i], d, n);
+        if (x == 1 || x == n - 1) continue;
+        int comp = 1;
+        for (int r = 1; r < s; r++) {
+            x = mulmod(x, x, n);
+            if (x == n - 1) { comp = 0; break; }
+        }
+        if (comp) return 0;
+    }
+    return 1;
+}
+
+#define PRIME_STEP 131072ull
+#define PRIME_MAX 17177772037ull
+
+static uint64_t *g_primes = NULL;
+static uint64_t g_num_primes = 0;
+static pthread_once_t g_primes_once = PTHREAD_ONCE_INIT;
+
+static void build_primes(void)
+{
+    uint64_t cap = 140000;
+    uint64_t *p = (uint64_t *)malloc(cap * sizeof(uint64_t));
+    uint64_t n = 0;
+    uint64_t x = PRIME_STEP;
+    for (;;) {
+        while (!is_prime_u64(x)) x++;
+        if (x > PRIME_MAX) break;
+        p[n++] = x;
+        x += PRIME_STEP;
+    }
+    g_primes = p;
+    g_num_primes = n;
+}
+
+uint64_t wco_num_primes(void)
+{
+    pthread_once(&g_primes_once, build_primes);
+    return g_num_primes;
+}
+
+void wco_primes(uint64_t *out)
+{
+    pthread_once(&g_primes_once, build_primes);
+    memcpy(out, g_primes, g_num_primes * sizeof(uint64_t));
+}
+
+/* base.cuh:27-34: smallest table prime >= ceil(min/cg), times cg; 0 if none */
+uint64_t wco_valid_capacity(uint64_t min_capacity, uint64_t cg_size)
+{
+    pthread_once(&g_primes_once, build_primes);
+    uint64_t x = (min_capacity + cg_size - 1) / cg_size;
+    uint64_t lo = 0, hi = g_num_primes;
+    while (lo < hi) {
+        uint64_t mid = (lo + hi) / 2;
+        if (g_primes[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    return lo == g_num_primes ? 0 : g_primes[lo] * cg_size;
+}
+
+/* ------------------------------------------------------------------------ */
+/* probing iterators (probing_schemes.cuh:79-100 DoubleHashing,
+ * LinearProbing begin/next, QuadraticProbing begin/next).
+ * All lanes of a cooperative group advance together; lane r's slot is
+ * pos[r].  The hash plus lane rank wraps in the hasher's output width,
+ * because thread_block_tile::thread_rank() is an unsigned int.             */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    int scheme, h1, h2, key_bytes;
+    uint64_t cg, capacity, windows_left, base, step;
+    uint64_t pos[32];
+} probe_t;
+
+static uint64_t wrap_add(uint64_t h, uint64_t r, int bits)
+{
+    uint64_t s = h + r;
+    return bits == 32 ? (s & 0xffffffffull) : s;
+}
+
+/* number of windows the reference visits for a probing length:
+ * SDIV(pl, cg) * cg slots per lane (probing_schemes.cuh:61), computed with
+ * the same unsigned wrap; the first window is always visited. */
+static uint64_t windows_for(uint64_t probing_length, uint64_t cg)
+{
+    uint64_t pl = (probing_length + cg - 1) / cg;
+    return pl == 0 ? 1 : pl;
+}
+
+static void probe_begin(probe_t *p, int scheme, int h1, int h2, int key_bytes,
+                        uint64_t cg, uint64_t capacity, uint64_t key,
+                        uint64_t seed, uint64_t probing_length)
+{
+    const uint64_t km = kmask(key_bytes);
+    p->scheme = scheme; p->h1 = h1; p->h2 = h2; p->key_bytes = key_bytes;
+    p->cg = cg; p->capacity = capacity;
+    p->windows_left = windows_for(probing_length, cg);
+    const uint64_t h = wco_hash(h1, key_bytes, (key + seed) & km);
+    const int hb = wco_hash_bits(h1, key_bytes);
+    for (uint64_t r = 0; r < cg; r++) p->pos[r] = wrap_add(h, r, hb) % capacity;
+    p->step = 1;
+    p->base = 0;
+    if (scheme == WCO_PROBE_DOUBLE) {
+        const uint64_t h2v = wco_hash(h2, key_bytes, (key + seed + 1) & km);
+        p->base = (h2v % (capacity / cg - 1) + 1) * cg;
+    }
+}
+
+/* returns 0 when the sequence has ended */
+static int probe_next(probe_t *p)
+{
+    if (p->windows_left <= 1) return 0;
+    p->windows_left--;
+    for (uint64_t r = 0; r < p->cg; r++) {
+        if (p->scheme == WCO_PROBE_DOUBLE)
+            p->pos[r] = (p->pos[r] + p->base) % p->capacity;
+        else if (p->scheme == WCO_PROBE_LINEAR)
+            p->pos[r] = (p->pos[r] + p->cg) % p->capacity;
+        else
+            p->pos[r] = (p->pos[r] + p->step) % p->capacity;
+    }
+    if (p->scheme == WCO_PROBE_QUADRATIC) p->step++;
+    return 1;
+}
+
+uint64_t wco_probe_sequence(int scheme, int h1, int h2, int key_bytes,
+                            uint64_t cg, uint64_t capacity, uint64_t key,
+                            uint64_t seed, uint64_t probing_length,
+                            uint64_t max_windows, uint64_t *out)
+{
+    probe_t p;
+    probe_begin(&p, scheme, h1, h2, key_bytes, cg, capacity, key, seed,
+                probing_length);
+    uint64_t w = 0;
+    do {
+        if (w >= max_windows) break;
+        for (uint64_t r = 0; r < cg; r++) out[w * cg + r] = p.pos[r];
+        w++;
+    } while (probe_next(&p));
+    return w;
+}
+
+/* status.cuh:142-146 (operator~) and :316-330 (ReturnBoolean::handle):
+ * ~Status(x) is (~x) ^ 0xFFF, so the flag is set for bits of the status
+ * that are in Ignore's low twelve bits or at bit 12 and above. */
+uint8_t wco_status_to_bool(uint32_t status, uint32_t ignore)
+{
+    const uint32_t m = (~ignore) ^ 0xFFFu;
+    return (status & m) != 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* tables: single_value_hash_table.cuh, hash_set.cuh, counting_hash_table.cuh */
+/* ------------------------------------------------------------------------ */
+
+struct wco_table {
+    int kind, key_bytes, value_bytes, scheme, h1, h2;
+    uint64_t capacity, cg, seed, empty, tomb, max_count;
+    uint64_t *keys;
+    uint64_t *values;
+    uint32_t status;
+};
+
+wco_table *wco_table_create(int kind, int key_bytes, int value_bytes,
+                            uint64_t min_capacity, uint64_t seed, uint64_t cg,
+                            int scheme, int h1, int h2, uint64_t empty_key,
+                            uint64_t tombstone_key, uint64_t max_count)
+{
+    wco_table *t = (wco_table *)calloc(1, sizeof(wco_table));
+    t->kind = kind;
+    t->key_bytes = key_bytes;
+    t->value_bytes = kind == WCO_HASHSET ? 0 : value_bytes;
+    t->scheme = scheme; t->h1 = h1; t->h2 = h2;
+    t->cg = cg;
+    t->capacity = wco_valid_capacity(min_capacity, cg);
+    t->empty = empty_key & kmask(key_bytes);
+    t->tomb = tombstone_key & kmask(key_bytes);
+    t->max_count = max_count;
+    t->keys = (uint64_t *)malloc((t->capacity ? t->capacity : 1) * 8);
+    t->values = (uint64_t *)calloc(t->capacity ? t->capacity : 1, 8);
+    wco_table_init(t, seed);
+    return t;
+}
+
+void wco_table_destroy(wco_table *t)
+{
+    if (!t) return;
+    free(t->keys);
+    free(t->values);
+    free(t);
+}
+
+uint64_t wco_table_capacity(const wco_table *t) { return t->capacity; }
+
+/* init(): keys := empty (storage.cuh:523-539); counting also zeroes the
+ * values (counting_hash_table.cuh:114-124).  Values of a plain SVHT are
+ * left as they were, like the reference. */
+void wco_table_init(wco_table *t, uint64_t seed)
+{
+    t->seed = seed & kmask(t->key_bytes);
+    for (uint64_t i = 0; i < t->capacity; i++) t->keys[i] = t->empty;
+    if (t->kind == WCO_COUNTING)
+        memset(t->values, 0, t->capacity * 8);
+    t->status = 0;
+}
+
+static uint64_t load_elem(const void *p, int bytes, uint64_t i)
+{
+    return bytes == 4 ? ((const uint32_t *)p)[i] : ((const uint64_t *)p)[i];
+}
+
+static void store_elem(void *p, int bytes, uint64_t i, uint64_t v)
+{
+    if (bytes == 4) ((uint32_t *)p)[i] = (uint32_t)v;
+    else ((uint64_t *)p)[i] = v;
+}
+
+static int valid_key(const wco_table *t, uint64_t k)
+{
+    return k != t->empty && k != t->tomb;
+}
+
+/* Status::atomic_join (status.cuh:187-193) */
+static void join(wco_table *t, uint32_t s) { t->status |= s; }
+
+/* insert_impl (single_value_hash_table.cuh:743-823; hash_set.cuh:193-254):
+ * returns the slot index that holds the key afterwards, or -1. */
+static int64_t insert_impl(wco_table *t, uint64_t key, uint64_t pl,
+                           uint32_t *st)
+{
+    if (!valid_key(t, key)) {
+        join(t, WCO_ST_INVALID_KEY);
+        *st = WCO_ST_INVALID_KEY;
+        return -1;
+    }
+    probe_t p;
+    probe_begin(&p, t->scheme, t->h1, t->h2, t->key_bytes, t->cg, t->capacity,
+                key, t->seed, pl);
+    /* a cycle-free sequence has seen every slot after capacity/cg windows;
+     * stop there instead of spinning like the unbounded reference loop */
+    uint64_t guard = t->capacity / t->cg + 1;
+    do {
+        for (uint64_t r = 0; r < t->cg; r++) {
+            if (t->keys[p.pos[r]] == key) {
+                join(t, WCO_ST_DUPLICATE_KEY);
+                *st = WCO_ST_DUPLICATE_KEY;
+                return (int64_t)p.pos[r];
+            }
+        }
+        for (uint64_t r = 0; r < t->cg; r++) {
+            if (t->keys[p.pos[r]] == t->empty) {
+                t->keys[p.pos[r]] = key;
+                *st = WCO_ST_NONE;
+                return (int64_t)p.pos[r];
+            }
+        }
+    } while (--guard && probe_next(&p));
+    join(t, WCO_ST_PROBING_LENGTH_EXCEEDED);
+    *st = WCO_ST_PROBING_LENGTH_EXCEEDED;
+    return -1;
+}
+
+void wco_insert(wco_table *t, const void *keys, const void *values, uint64_t n,
+                uint64_t probing_length, uint32_t *status_out)
+{
+    const uint64_t vmask = t->value_bytes == 4 ? 0xffffffffull : ~0ull;
+    for (uint64_t i = 0; i < n; i++) {
+        uint32_t st = WCO_ST_UNKNOWN_ERROR;
+        const uint64_t key = load_elem(keys, t->key_bytes, i);
+        const int64_t slot = insert_impl(t, key, probing_length, &st);
+        if (slot >= 0) {
+            if (t->kind == WCO_SVHT) {
+                /* single_value_hash_table.cuh:222-225 */
+                t->values[slot] = load_elem(values, t->value_bytes, i);
+            } else if (t->kind == WCO_COUNTING) {
+                /* counting_hash_table.cuh:152-169 */
+                uint64_t *v = &t->values[slot];
+                if (*v < t->max_count) {
+                    const uint64_t old = *v;
+                    *v = (*v + 1) & vmask;
+                    if (old > *v) {
+                        st |= WCO_ST_INDEX_OVERFLOW;
+                        join(t, WCO_ST_INDEX_OVERFLOW);
+                        *v = t->max_count;
+                    }
+                }
+            }
+        }
+        if (status_out) status_out[i] = st;
+    }
+}
+
+/* SVHT::retrieve (single_value_hash_table.cuh:268-307), HashSet::retrieve
+ * (hash_set.cuh:292-329), CountingHashTable::retrieve (:204-225), and the
+ * kernel's hit-only write (gpu_engine.cuh:252-257). */
+void wco_retrieve(wco_table *t, const void *keys, uint64_t n, void *values_out,
+                  uint64_t probing_length, uint32_t *status_out)
+{
+    for (uint64_t i = 0; i < n; i++) {
+        const uint64_t key = load_elem(keys, t->key_bytes, i);
+        uint32_t st;
+        uint64_t val = 0;
+        int flag = 0;
+        if (!valid_key(t, key)) {
+            join(t, WCO_ST_INVALID_KEY);
+            st = WCO_ST_INVALID_KEY;
+        } else {
+            probe_t p;
+            probe_begin(&p, t->scheme, t->h1, t->h2, t->key_bytes, t->cg,
+                        t->capacity, key, t->seed, probing_length);
+            uint64_t guard = t->capacity / t->cg + 1;
+            st = WCO_ST_PROBING_LENGTH_EXCEEDED;
+            int done = 0;
+            do {
+                for (uint64_t r = 0; r < t->cg && !done; r++) {
+                    if (t->keys[p.pos[r]] == key) {
+                        val = t->values[p.pos[r]];
+                        flag = 1;
+                        st = WCO_ST_NONE;
+                        done = 1;
+                    }
+                }
+                if (done) break;
+                for (uint64_t r = 0; r < t->cg && !done; r++) {
+                    if (t->keys[p.pos[r]] == t->empty) {
+                        done = 1;
+                        flag = 0;
+                        if (t->kind == WCO_HASHSET) {
+                            st = WCO_ST_NONE;
+                        } else {
+                            st = WCO_ST_KEY_NOT_FOUND;
+                            join(t, WCO_ST_KEY_NOT_FOUND);
+                        }
+                    }
+                }
+                if (done) break;
+            } while (--guard && probe_next(&p));
+            if (!done) join(t, WCO_ST_PROBING_LENGTH_EXCEEDED);
+        }
+        if (st == WCO_ST_NONE) {
+            if (t->kind == WCO_HASHSET) {
+                ((uint8_t *)values_out)[i] = (uint8_t)flag;
+            } else {
+                if (t->kind == WCO_COUNTING && val > t->max_count)
+                    val = t->max_count;
+                store_elem(values_out, t->value_bytes, i, val);
+            }
+        }
+        if (status_out) status_out[i] = st;
+    }
+}
+
+/* SVHT::erase (single_value_hash_table.cuh:426-468) and HashSet::erase
+ * (hash_set.cuh:396-438, which always reports none). */
+void wco_erase(wco_table *t, const void *keys, uint64_t n,
+               uint64_t probing_length, uint32_t *status_out)
+{
+    for (uint64_t i = 0; i < n; i++) {
+        const uint64_t key = load_elem(keys, t->key_bytes, i);
+        uint32_t st;
+        if (!valid_key(t, key)) {
+            join(t, WCO_ST_INVALID_KEY);
+            st = WCO_ST_INVALID_KEY;
+        } else {
+            probe_t p;
+            probe_begin(&p, t->scheme, t->h1, t->h2, t->key_bytes, t->cg,
+                        t->capacity, key, t->seed, probing_length);
+            uint64_t guard = t->capacity / t->cg + 1;
+            st = WCO_ST_PROBING_LENGTH_EXCEEDED;
+            int done = 0;
+            do {
+                for (uint64_t r = 0; r < t->cg && !done; r++) {
+                    if (t->keys[p.pos[r]] == key) {
+                        t->keys[p.pos[r]] = t->tomb;
+                        st = WCO_ST_NONE;
+                        done = 1;
+                    }
+                }
+                if (done) break;
+                for (uint64_t r = 0; r < t->cg && !done; r++) {
+                    if (t->keys[p.pos[r]] == t->empty) {
+                        st = WCO_ST_KEY_NOT_FOUND;
+                        done = 1;
+                    }
+                }
+                if (done) break;
+            } while (--guard && probe_next(&p));
+            if (t->kind == WCO_HASHSET) st = WCO_ST_NONE;
+        }
+        if (status_out) status_out[i] = st;
+    }
+}
+
+/* size() (single_value_hash_table.cuh:535-592, hash_set.cuh:500-557) */
+uint64_t wco_size(const wco_table *t)
+{
+    uint64_t n = 0;
+    for (uint64_t i = 0; i < t->capacity; i++) n += valid_key(t, t->keys[i]);
+    return n;
+}
+
+/* retrieve_all (single_value_hash_table.cuh:391-417), in slot order */
+uint64_t wco_retrieve_all(const wco_table *t, void *keys_out, void *values_out)
+{
+    uint64_t n = 0;
+    for (uint64_t i = 0; i < t->capacity; i++) {
+        if (!valid_key(t, t->keys[i])) continue;
+        if (keys_out) store_elem(keys_out, t->key_bytes, n, t->keys[i]);
+        if (values_out && t->value_bytes)
+            store_elem(values_out, t->value_bytes, n, t->values[i]);
+        n++;
+    }
+    return n;
+}
+
+uint32_t wco_peek_status(const wco_table *t) { return t->status; }
+
+uint32_t wco_pop_status(wco_table *t)
+{
+    uint32_t s = t->status;
+    t->status = 0;
+    return s;
+}
+
+void wco_table_slots(const wco_table *t, uint64_t *keys_out,
+                     uint64_t *values_out)
+{
+    if (keys_out) memcpy(keys_out, t->keys, t->capacity * 8);
+    if (values_out) memcpy(values_out, t->values, t->capacity * 8);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Bloom filter (bloom_filter.cuh:78-93 sizes, :168-192 insert,
+ * :216-237 retrieve, :342-408 fpr)                                          */
+/* ------------------------------------------------------------------------ */
+
+struct wco_bloom {
+    int key_bytes, slot_bytes, hasher;
+    uint64_t cg, num_bits, num_slots, num_blocks, k, seed;
+    uint64_t *words;
+};
+
+wco_bloom *wco_bloom_create(int key_bytes, int slot_bytes, uint64_t cg,
+                            int hasher, uint64_t num_bits, uint64_t k,
+                            uint64_t seed)
+{
+    wco_bloom *b = (wco_bloom *)calloc(1, sizeof(wco_bloom));
+    b->key_bytes = key_bytes;
+    b->slot_bytes = slot_bytes;
+    b->hasher = hasher;
+    b->cg = cg;
+    b->num_bits = num_bits;
+    b->num_slots = (num_bits + slot_bytes * 8 - 1) / (slot_bytes * 8);
+    b->num_blocks = (b->num_slots + cg - 1) / cg;
+    b->k = k;
+    b->seed = seed & kmask(key_bytes);
+    b->words = (uint64_t *)calloc(b->num_slots ? b->num_slots : 1, 8);
+    return b;
+}
+
+void wco_bloom_destroy(wco_bloom *b)
+{
+    if (!b) return;
+    free(b->words);
+    free(b);
+}
+
+/* per-lane slot index and bit pattern of one key */
+static void bloom_pattern(const wco_bloom *b, uint64_t key, uint64_t *idx,
+                          uint64_t *mask)
+{
+    const uint64_t km = kmask(b->key_bytes);
+    const uint64_t slot_bits = (uint64_t)b->slot_bytes * 8;
+    const uint64_t block_bits = slot_bits * b->cg;
+    const uint64_t blk = wco_hash(b->hasher, b->key_bytes, (key + b->seed) & km)
+                         % b->num_blocks;
+    for (uint64_t r = 0; r < b->cg; r++) {
+        idx[r] = (blk * b->cg + r) % b->num_slots;
+        mask[r] = 0;
+    }
+    for (uint64_t i = 0; i < b->k; i++) {
+        const uint64_t h =
+            wco_hash(b->hasher, b->key_bytes, (key + b->seed + i) & km) %
+            block_bits;
+        mask[h / slot_bits] |= 1ull << (h % slot_bits);
+    }
+}
+
+void wco_bloom_insert(wco_bloom *b, const void *keys, uint64_t n)
+{
+    uint64_t idx[32], mask[32];
+    for (uint64_t i = 0; i < n; i++) {
+        bloom_pattern(b, load_elem(keys, b->key_bytes, i), idx, mask);
+        for (uint64_t r = 0; r < b->cg; r++) b->words[idx[r]] |= mask[r];
+    }
+}
+
+void wco_bloom_retrieve(const wco_bloom *b, const void *keys, uint64_t n,
+                        uint8_t *flags_out)
+{
+    uint64_t idx[32], mask[32];
+    for (uint64_t i = 0; i < n; i++) {
+        bloom_pattern(b, load_elem(keys, b->key_bytes, i), idx, mask);
+        int all = 1;
+        for (uint64_t r = 0; r < b->cg; r++)
+            all &= (b->words[idx[r]] & mask[r]) == mask[r];
+        flags_out[i] = (uint8_t)all;
+    }
+}
+
+uint64_t wco_bloom_num_slots(const wco_bloom *b) { return b->num_slots; }
+uint64_t wco_bloom_num_blocks(const wco_bloom *b) { return b->num_blocks; }
+
+void wco_bloom_words(const wco_bloom *b, uint64_t *out)
+{
+    memcpy(out, b->words, b->num_slots * 8);
+}
+
+/* bloom_filter.cuh:371-408 binom / fpr_base, :342-354 fpr */
+static double bloom_binom(uint64_t n, uint64_t k, double p)
+{
+    double res = 1.0;
+    for (uint64_t i = n - k + 1; i <= n; ++i) res = res * (double)i;
+    for (uint64_t i = 1; i <= k; ++i) res = res / (double)i;
+    return res * pow(p, (double)k) * pow(1.0 - p, (double)(n - k));
+}
+
+static double bloom_fpr_base(uint64_t m, uint64_t n, uint64_t k)
+{
+    return pow(1.0 - pow(1.0 - 1.0 / (double)m, (double)(n * k)), (double)k);
+}
+
+double wco_bloom_fpr(const wco_bloom *b, uint64_t n)
+{
+    const uint64_t block_bits = (uint64_t)b->slot_bytes * 8 * b->cg;
+    const double bl = (double)(b->num_bits / block_bits);
+    double res = 0.0;
+    const uint64_t upper = 5 * n / (b->num_bits / block_bits);
+    for (uint64_t i = 0; i < upper; ++i)
+        res += bloom_binom(n, i, 1.0 / bl) *
+               bloom_fpr_base((uint64_t)((double)b->num_bits / bl), i, b->k);
+    return res;
+}
+
+/* ------------------------------------------------------------------------ */
+/* synthetic data                                                            */
+/* ------------------------------------------------------------------------ */
+
+uint64_t wco_splitmix64(uint64_t *state)
+{
+    uint64_t z = (*state += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+/* distinct keys: a bijective mix of the index (fmix is invertible), skipping
+ * the two sentinels; for 32-bit keys the index is taken mod 2^32 */
+void wco_gen_unique_keys(int key_bytes, uint64_t n, uint64_t seed, void *out)
+{
+    const uint64_t km = kmask(key_bytes);
+    uint64_t j = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t k;
+        do {
+            const uint64_t x = (j++ + seed * 0x9e3779b97f4a7c15ull) & km;
+            k = key_bytes == 4 ? (uint64_t)fmix32((uint32_t)x) : fmix64(x);
+        } while (k == 0 || k == km);
+        store_elem(out, key_bytes, i, k);
+    }
+}
+
+void wco_gen_uniform(int bytes, uint64_t n, uint64_t seed, void *out)
+{
+    uint64_t s = seed;
+    for (uint64_t i = 0; i < n; i++) store_elem(out, bytes, i, wco_splitmix64(&s));
+}
+
+static double u01(uint64_t *s)
+{
+    return (double)(wco_splitmix64(s) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+/* rejection sampler of random_distributions.cuh:285-310 */
+void wco_gen_zipf_ranks(uint64_t n_in, double s, uint64_t n_out, uint64_t seed,
+                        uint64_t *ranks_out)
+{
+    uint64_t st = seed;
+    const double t = (pow((double)n_in, 1.0 - s) - s) / (1.0 - s);
+    for (uint64_t i = 0; i < n_out; i++) {
+        uint64_t k;
+        double y, rat;
+        do {
+            const double p = u01(&st);
+            const double inv_b = (p * t <= 1.0)
+                ? p * t
+                : pow((p * t) * (1.0 - s) + s, 1.0 / (1.0 - s));
+            k = (uint64_t)(inv_b + 1.0);
+            y = u01(&st);
+            const double bnd = (k <= 1) ? 1.0 / t : pow(inv_b, -s) / t;
+            rat = pow((double)k, -s) / (bnd * t);
+        } while (y >= rat);
+        if (k > n_in) k = n_in;
+        ranks_out[i] = k; /* 1-based rank; key index is k-1 */
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* multi-threaded CPU port of the reference insert/retrieve                  */
+/* ------------------------------------------------------------------------ */
+
+struct wco_mt_table {
+    int key_bytes, value_bytes;
+    uint64_t capacity, cg, seed;
+    void *slots; /* AoS {K key; V value;} like storage.cuh:165-187 */
+};
+
+wco_mt_table *wco_mt_create(int key_bytes, int value_bytes, uint64_t capacity,
+                            uint64_t cg, uint64_t seed)
+{
+    wco_mt_table *t = (wco_mt_table *)calloc(1, sizeof(wco_mt_table));
+    t->key_bytes = key_bytes;
+    t->value_bytes = value_bytes;
+    t->capacity = capacity;
+    t->cg = cg;
+    t->seed = seed & kmask(key_bytes);
+    t->slots = aligned_alloc(64, ((capacity * 2 * key_bytes + 63) / 64) * 64);
+    return t;
+}
+
+void wco_mt_destroy(wco_mt_table *t)
+{
+    if (!t) return;
+    free(t->slots);
+    free(t);
+}
+
+typedef struct {
+    wco_mt_table *t;
+    const void *keys;
+    const void *values;
+    void *values_out;
+    uint8_t *found_out;
+    uint64_t begin, end;
+} mt_job;
+
+static double now_s(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + ts.tv_nsec * 1e-9;
+}
+
+static void *mt_clear_worker(void *arg)
+{
+    mt_job *j = (mt_job *)arg;
+    const size_t sb = 2 * (size_t)j->t->key_bytes;
+    memset((char *)j->t->slots + j->begin * sb, 0, (j->end - j->begin) * sb);
+    return NULL;
+}
+
+/* the reference's insert_impl with the key CAS and the value store after it
+ * (single_value_hash_table.cuh:743-823, :222-225), one key per thread step */
+#define MT_WORKERS(K, SUFFIX)                                                  \
+    typedef struct { K key; K value; } mt_pair_##SUFFIX;                       \
+    static void *mt_insert_##SUFFIX(void *arg)                                 \
+    {                                                                          \
+        mt_job *j = (mt_job *)arg;                                             \
+        wco_mt_table *t = j->t;                                                \
+        mt_pair_##SUFFIX *s = (mt_pair_##SUFFIX *)t->slots;                    \
+        const K *keys = (const K *)j->keys;                                    \
+        const K *vals = (const K *)j->values;                                  \
+        const uint64_t cap = t->capacity, cg = t->cg;                          \
+        const uint64_t base_mod = cap / cg - 1;                                \
+        for (uint64_t i = j->begin; i < j->end; i++) {                         \
+            const K key = keys[i];                                             \
+            const uint64_t h = (K)(MT_HASH(K, (K)(key + (K)t->seed)));         \
+            uint64_t pos0 = (K)(h);                                            \
+            const uint64_t step =                                              \
+                ((uint64_t)MT_HASH(K, (K)(key + (K)t->seed + 1)) % base_mod + 1) \
+                * cg;                                                          \
+            uint64_t w = 0;                                                    \
+            for (; w <= cap / cg; w++) {                                       \
+                int done = 0;                                                  \
+                for (uint64_t r = 0; r < cg && !done; r++) {                   \
+                    const uint64_t p =                                         \
+                        ((uint64_t)(K)(pos0 + r) % cap + w * step) % cap;      \
+                    if (__atomic_load_n(&s[p].key, __ATOMIC_RELAXED) == key) { \
+                        s[p].value = vals[i];                                  \
+                        done = 1;                                              \
+                    }                                                          \
+                }                                                              \
+                for (uint64_t r = 0; r < cg && !done; r++) {                   \
+                    const uint64_t p =                                         \
+                        ((uint64_t)(K)(pos0 + r) % cap + w * step) % cap;      \
+                    K expect = 0;                                              \
+                    if (__atomic_load_n(&s[p].key, __ATOMIC_RELAXED) != 0)     \
+                        continue;                                              \
+                    if (__atomic_compare_exchange_n(&s[p].key, &expect, key,   \
+                            0, __ATOMIC_RELAXED, __ATOMIC_RELAXED) ||          \
+                        expect == key) {                                       \
+                        s[p].value = vals[i];                                  \
+                        done = 1;                                              \
+                    }                                                          \
+                }                                                              \
+                if (done) break;                                               \
+            }                                                                  \
+        }                                                                      \
+        return NULL;                                                           \
+    }                                                                          \
+    static void *mt_retrieve_##SUFFIX(void *arg)                               \
+    {                                                                          \
+        mt_job *j = (mt_job *)arg;                                             \
+        wco_mt_table *t = j->t;                                                \
+        const mt_pair_##SUFFIX *s = (const mt_pair_##SUFFIX *)t->slots;        \
+        const K *keys = (const K *)j->keys;                                    \
+        K *out = (K *)j->values_out;                                           \
+        const uint64_t cap = t->capacity, cg = t->cg;                          \
+        const uint64_t base_mod = cap / cg - 1;                                \
+        for (uint64_t i = j->begin; i < j->end; i++) {                         \
+            const K key = keys[i];                                             \
+            const uint64_t pos0 = (K)(MT_HASH(K, (K)(key + (K)t->seed)));     \
+            const uint64_t step =                                              \
+                ((uint64_t)MT_HASH(K, (K)(key + (K)t->seed + 1)) % base_mod + 1) \
+                * cg;                                                          \
+            uint8_t found = 0;                                                 \
+            for (uint64_t w = 0; w <= cap / cg; w++) {                         \
+                int hit = -1, empty = 0;                                       \
+                uint64_t p = 0;                                                \
+                for (uint64_t r = 0; r < cg; r++) {                            \
+                    p = ((uint64_t)(K)(pos0 + r) % cap + w * step) % cap;      \
+                    if (s[p].key == key) { hit = (int)r; break; }              \
+                    empty |= s[p].key == 0;                                    \
+                }                                                              \
+                if (hit >= 0) { out[i] = s[p].value; found = 1; break; }       \
+                if (empty) break;                                              \
+            }                                                                  \
+            if (j->found_out) j->found_out[i] = found;                         \
+        }                                                                      \
+        return NULL;                                                           \
+    }
+
+#define MT_HASH(K, x) (sizeof(K) == 4 ? (uint64_t)fmix32((uint32_t)(x)) : fmix64((uint64_t)(x)))
+MT_WORKERS(uint32_t, u32)
+MT_WORKERS(uint64_t, u64)
+#undef MT_HASH
+
+static double mt_run(void *(*fn)(void *), wco_mt_table *t, const void *keys,
+                     const void *values, void *values_out, uint8_t *found_out,
+                     uint64_t n, int threads)
+{
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    pthread_t th[256];
+    mt_job jobs[256];
+    const double t0 = now_s();
+    for (int i = 0; i < threads; i++) {
+        jobs[i].t = t;
+        jobs[i].keys = keys;
+        jobs[i].values = values;
+        jobs[i].values_out = values_out;
+        jobs[i].found_out = found_out;
+        jobs[i].begin = n * (uint64_t)i / threads;
+        jobs[i].end = n * (uint64_t)(i + 1) / threads;
+        pthread_create(&th[i], NULL, fn, &jobs[i]);
+    }
+    for (int i = 0; i < threads; i++) pthread_join(th[i], NULL);
+    return now_s() - t0;
+}
+
+void wco_mt_clear(wco_mt_table *t, int threads)
+{
+    mt_run(mt_clear_worker, t, NULL, NULL, NULL, NULL, t->capacity, threads);
+}
+
+double wco_mt_insert(wco_mt_table *t, const void *keys, const void *values,
+                     uint64_t n, int threads)
+{
+    return mt_run(t->key_bytes == 4 ? mt_insert_u32 : mt_insert_u64, t, keys,
+                  values, NULL, NULL, n, threads);
+}
+
+double wco_mt_retrieve(wco_mt_table *t, const void *keys, uint64_t n,
+                       void *values_out, uint8_t *found_out, int threads)
+{
+    return mt_run(t->key_bytes == 4 ? mt_retrieve_u32 : mt_retrieve_u64, t,
+                  keys, NULL, values_out, found_out, n, threads);
+}

@@ -1,0 +1,505 @@
+"""warpcore_b200 -- B200-native GPU hash tables and Bloom filter.
+
+Python binding of the C ABI in ``include/warpcore_b200.h`` (ctypes).  The
+classes mirror the reference's C++ class templates (warpcore's
+``SingleValueHashTable``, ``HashSet``, ``CountingHashTable`` and
+``BloomFilter``): same constructor arguments, same bulk methods on device
+buffers, same ``Status`` flags.  Buffers are CUDA tensors (any 4- or 8-byte
+dtype; bits are read as unsigned integers); ``stream`` is a
+``torch.cuda.Stream`` or a raw ``cudaStream_t`` integer and defaults to the
+current torch stream.
+
+There is no CPU fallback: importing works without a GPU, but every table
+operation needs the compiled ``libwarpcore_b200.so`` and a CUDA device, and
+raises otherwise.
+"""
+import ctypes
+import os
+
+from ._status import Status  # noqa: F401
+
+__all__ = [
+    "Status", "SingleValueHashTable", "HashSet", "CountingHashTable",
+    "BloomFilter", "lib", "valid_capacity", "WarpcoreError",
+    "HASH_MURMUR", "HASH_NVIDIA", "HASH_MUELLER", "HASH_IDENTITY32",
+    "HASH_IDENTITY64", "PROBING_DOUBLE", "PROBING_LINEAR",
+    "PROBING_QUADRATIC", "HANDLER_NOTHING", "HANDLER_STATUS",
+    "HANDLER_BOOLEAN", "DEFAULT_SEED", "DEFAULT_PROBING_LENGTH",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libwarpcore_b200.so")
+
+HASH_MURMUR, HASH_NVIDIA, HASH_MUELLER, HASH_IDENTITY32, HASH_IDENTITY64 = range(5)
+PROBING_DOUBLE, PROBING_LINEAR, PROBING_QUADRATIC = range(3)
+HANDLER_NOTHING, HANDLER_STATUS, HANDLER_BOOLEAN = range(3)
+
+# defaults.cuh:21 (seed) and :27 (probing length)
+DEFAULT_SEED = 0x5AD0DED
+DEFAULT_PROBING_LENGTH = (2**64 - 1) - 1024
+
+
+class WarpcoreError(RuntimeError):
+    pass
+
+
+class TableConfig(ctypes.Structure):
+    _fields_ = [
+        ("key_bytes", ctypes.c_uint32),
+        ("value_bytes", ctypes.c_uint32),
+        ("empty_key", ctypes.c_uint64),
+        ("tombstone_key", ctypes.c_uint64),
+        ("probing", ctypes.c_uint32),
+        ("hasher1", ctypes.c_uint32),
+        ("hasher2", ctypes.c_uint32),
+        ("cg_size", ctypes.c_uint32),
+    ]
+
+
+class TableInfo(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_uint32),
+        ("key_bytes", ctypes.c_uint32),
+        ("value_bytes", ctypes.c_uint32),
+        ("slot_bytes", ctypes.c_uint32),
+        ("cg_size", ctypes.c_uint32),
+        ("probing", ctypes.c_uint32),
+        ("hasher1", ctypes.c_uint32),
+        ("hasher2", ctypes.c_uint32),
+        ("capacity", ctypes.c_uint64),
+        ("num_buckets", ctypes.c_uint64),
+        ("seed", ctypes.c_uint64),
+        ("empty_key", ctypes.c_uint64),
+        ("tombstone_key", ctypes.c_uint64),
+        ("max_count", ctypes.c_uint64),
+        ("bytes_total", ctypes.c_uint64),
+        ("slots", ctypes.c_void_p),
+        ("status", ctypes.c_void_p),
+        ("is_initialized", ctypes.c_int),
+    ]
+
+
+class BloomConfig(ctypes.Structure):
+    _fields_ = [
+        ("key_bytes", ctypes.c_uint32),
+        ("slot_bytes", ctypes.c_uint32),
+        ("cg_size", ctypes.c_uint32),
+        ("hasher", ctypes.c_uint32),
+    ]
+
+
+class BloomInfo(ctypes.Structure):
+    _fields_ = [
+        ("key_bytes", ctypes.c_uint32),
+        ("slot_bytes", ctypes.c_uint32),
+        ("cg_size", ctypes.c_uint32),
+        ("hasher", ctypes.c_uint32),
+        ("num_bits", ctypes.c_uint64),
+        ("num_slots", ctypes.c_uint64),
+        ("num_blocks", ctypes.c_uint64),
+        ("k", ctypes.c_uint64),
+        ("seed", ctypes.c_uint64),
+        ("words", ctypes.c_void_p),
+    ]
+
+
+_vp = ctypes.c_void_p
+_u64 = ctypes.c_uint64
+_u32 = ctypes.c_uint32
+_i = ctypes.c_int
+_pp = ctypes.POINTER(ctypes.c_void_p)
+
+# every symbol the C header declares, with its signature
+SIGNATURES = {
+    "wc_last_error": (ctypes.c_char_p, []),
+    "wc_version": (ctypes.c_char_p, []),
+    "wc_svht_default_config": (None, [ctypes.POINTER(TableConfig), _u32, _u32]),
+    "wc_hashset_default_config": (None, [ctypes.POINTER(TableConfig), _u32]),
+    "wc_counting_default_config": (None, [ctypes.POINTER(TableConfig), _u32, _u32]),
+    "wc_valid_capacity": (_u64, [_u64, _u64]),
+    "wc_svht_create": (_i, [ctypes.POINTER(TableConfig), _u64, _u64, _i, _pp]),
+    "wc_table_destroy": (_i, [_vp]),
+    "wc_table_init": (_i, [_vp, _u64, _vp]),
+    "wc_svht_insert": (_i, [_vp, _vp, _vp, _u64, _vp, _u64, _vp, _i, _u32]),
+    "wc_svht_retrieve": (_i, [_vp, _vp, _u64, _vp, _vp, _u64, _vp, _i, _u32]),
+    "wc_svht_erase": (_i, [_vp, _vp, _u64, _vp, _u64, _vp, _i, _u32]),
+    "wc_table_size": (_i, [_vp, _vp, ctypes.POINTER(_u64)]),
+    "wc_table_retrieve_all": (_i, [_vp, _vp, _vp, ctypes.POINTER(_u64), _vp]),
+    "wc_table_peek_status": (_i, [_vp, _vp, ctypes.POINTER(_u32)]),
+    "wc_table_pop_status": (_i, [_vp, _vp, ctypes.POINTER(_u32)]),
+    "wc_table_get_info": (_i, [_vp, ctypes.POINTER(TableInfo)]),
+    "wc_hashset_create": (_i, [ctypes.POINTER(TableConfig), _u64, _u64, _pp]),
+    "wc_hashset_insert": (_i, [_vp, _vp, _u64, _vp, _u64, _vp, _i, _u32]),
+    "wc_hashset_retrieve": (_i, [_vp, _vp, _u64, _vp, _vp, _u64, _vp, _i, _u32]),
+    "wc_hashset_erase": (_i, [_vp, _vp, _u64, _vp, _u64, _vp, _i, _u32]),
+    "wc_counting_create": (_i, [ctypes.POINTER(TableConfig), _u64, _u64, _u64, _i, _pp]),
+    "wc_counting_insert": (_i, [_vp, _vp, _u64, _vp, _u64, _vp, _i, _u32]),
+    "wc_counting_retrieve": (_i, [_vp, _vp, _u64, _vp, _vp, _u64, _vp, _i, _u32]),
+    "wc_counting_erase": (_i, [_vp, _vp, _u64, _vp, _u64, _vp, _i, _u32]),
+    "wc_bloom_create": (_i, [ctypes.POINTER(BloomConfig), _u64, _u64, _u64, _pp]),
+    "wc_bloom_destroy": (_i, [_vp]),
+    "wc_bloom_init": (_i, [_vp, _u64, _vp]),
+    "wc_bloom_insert": (_i, [_vp, _vp, _u64, _vp]),
+    "wc_bloom_retrieve": (_i, [_vp, _vp, _u64, _vp, _vp]),
+    "wc_bloom_get_info": (_i, [_vp, ctypes.POINTER(BloomInfo)]),
+    "wc_bloom_fpr": (_i, [_vp, _u64, ctypes.POINTER(ctypes.c_double)]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libwarpcore_b200.so (built in-tree by warpcore_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise WarpcoreError(
+                "libwarpcore_b200.so is missing; build it with "
+                "`python -m warpcore_b200.build` (nvcc, sm_100a)")
+        l = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(l, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = l
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise WarpcoreError("warpcore_b200 error %d: %s"
+                            % (rc, lib().wc_last_error().decode()))
+
+
+def valid_capacity(min_capacity, cg_size):
+    """The reference's capacity rule (base.cuh:27-34)."""
+    return lib().wc_valid_capacity(int(min_capacity), int(cg_size))
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    if not t.is_cuda:
+        raise WarpcoreError("buffers must be CUDA tensors (device memory)")
+    if not t.is_contiguous():
+        raise WarpcoreError("buffers must be contiguous")
+    return t.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _check_width(t, nbytes, what):
+    if t is not None and not isinstance(t, int) and t.element_size() != nbytes:
+        raise WarpcoreError("%s must have %d-byte elements, got %s"
+                            % (what, nbytes, t.dtype))
+
+
+def _numel(t, n):
+    if n is not None:
+        return int(n)
+    return t.numel()
+
+
+class _Table:
+    _kind = None
+
+    def _make(self, create, cfg, *args):
+        h = ctypes.c_void_p()
+        _check(create(ctypes.byref(cfg), *args, ctypes.byref(h)))
+        self._h = h
+        self._cfg = cfg
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().wc_table_destroy(h)
+            self._h = None
+
+    def info(self):
+        inf = TableInfo()
+        _check(lib().wc_table_get_info(self._h, ctypes.byref(inf)))
+        return inf
+
+    @property
+    def capacity(self):
+        return self.info().capacity
+
+    def bytes_total(self):
+        return self.info().bytes_total
+
+    @property
+    def seed(self):
+        return self.info().seed
+
+    def is_initialized(self):
+        return bool(self.info().is_initialized)
+
+    @property
+    def key_bytes(self):
+        return self._cfg.key_bytes
+
+    def cg_size(self):
+        return self._cfg.cg_size
+
+    def init(self, seed=None, stream=None):
+        _check(lib().wc_table_init(self._h, int(self.seed if seed is None else seed),
+                                   _stream(stream)))
+
+    def size(self, stream=None):
+        out = _u64()
+        _check(lib().wc_table_size(self._h, _stream(stream), ctypes.byref(out)))
+        return out.value
+
+    def load_factor(self, stream=None):
+        return float(self.size(stream)) / float(self.capacity)
+
+    def storage_density(self, stream=None):
+        return self.load_factor(stream)
+
+    def peek_status(self, stream=None):
+        out = _u32()
+        _check(lib().wc_table_peek_status(self._h, _stream(stream), ctypes.byref(out)))
+        return Status(out.value)
+
+    def pop_status(self, stream=None):
+        out = _u32()
+        _check(lib().wc_table_pop_status(self._h, _stream(stream), ctypes.byref(out)))
+        return Status(out.value)
+
+    def retrieve_all(self, keys_out, values_out=None, stream=None):
+        """Dump all valid (key, value) pairs; returns the count (blocking)."""
+        _check_width(keys_out, self.key_bytes, "keys_out")
+        n = _u64()
+        _check(lib().wc_table_retrieve_all(self._h, _ptr(keys_out), _ptr(values_out),
+                                           ctypes.byref(n), _stream(stream)))
+        return n.value
+
+
+def _table_config(default_fn, key_bytes, value_bytes, empty_key, tombstone_key,
+                  probing, hasher1, hasher2, cg_size):
+    cfg = TableConfig()
+    if value_bytes is None:
+        default_fn(ctypes.byref(cfg), key_bytes)
+    else:
+        default_fn(ctypes.byref(cfg), key_bytes, value_bytes)
+    if empty_key is not None:
+        cfg.empty_key = empty_key
+    if tombstone_key is not None:
+        cfg.tombstone_key = tombstone_key
+    if probing is not None:
+        cfg.probing = probing
+    if hasher1 is not None:
+        cfg.hasher1 = hasher1
+    if hasher2 is not None:
+        cfg.hasher2 = hasher2
+    if cg_size is not None:
+        cfg.cg_size = cg_size
+    return cfg
+
+
+class SingleValueHashTable(_Table):
+    """warpcore::SingleValueHashTable (single_value_hash_table.cuh:29-37)."""
+
+    def __init__(self, min_capacity, seed=DEFAULT_SEED, no_init=False, key_bytes=4,
+                 value_bytes=None, empty_key=None, tombstone_key=None, probing=None,
+                 hasher1=None, hasher2=None, cg_size=None):
+        value_bytes = key_bytes if value_bytes is None else value_bytes
+        cfg = _table_config(lib().wc_svht_default_config, key_bytes, value_bytes, empty_key,
+                            tombstone_key, probing, hasher1, hasher2, cg_size)
+        self._make(lib().wc_svht_create, cfg, int(min_capacity), int(seed), int(bool(no_init)))
+
+    def insert(self, keys_in, values_in, num_in=None, stream=None,
+               probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+               status_handler=None, ignore=0):
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        _check_width(values_in, self._cfg.value_bytes, "values_in")
+        h = _handler(status_out, status_handler)
+        _check(lib().wc_svht_insert(self._h, _ptr(keys_in), _ptr(values_in),
+                                    _numel(keys_in, num_in), _stream(stream),
+                                    int(probing_length), _ptr(status_out), h, int(ignore)))
+
+    def retrieve(self, keys_in, values_out, num_in=None, stream=None,
+                 probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+                 status_handler=None, ignore=0):
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        _check_width(values_out, self._cfg.value_bytes, "values_out")
+        h = _handler(status_out, status_handler)
+        _check(lib().wc_svht_retrieve(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                      _ptr(values_out), _stream(stream), int(probing_length),
+                                      _ptr(status_out), h, int(ignore)))
+
+    def erase(self, keys_in, num_in=None, stream=None,
+              probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+              status_handler=None, ignore=0):
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        h = _handler(status_out, status_handler)
+        _check(lib().wc_svht_erase(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                   _stream(stream), int(probing_length), _ptr(status_out),
+                                   h, int(ignore)))
+
+
+class HashSet(_Table):
+    """warpcore::HashSet (hash_set.cuh:16-22); default CG 16."""
+
+    def __init__(self, min_capacity, seed=DEFAULT_SEED, key_bytes=4, empty_key=None,
+                 tombstone_key=None, probing=None, hasher1=None, hasher2=None,
+                 cg_size=None):
+        cfg = _table_config(lib().wc_hashset_default_config, key_bytes, None, empty_key,
+                            tombstone_key, probing, hasher1, hasher2, cg_size)
+        self._make(lib().wc_hashset_create, cfg, int(min_capacity), int(seed))
+
+    def insert(self, keys_in, num_in=None, stream=None,
+               probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+               status_handler=None, ignore=0):
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        h = _handler(status_out, status_handler)
+        _check(lib().wc_hashset_insert(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                       _stream(stream), int(probing_length),
+                                       _ptr(status_out), h, int(ignore)))
+
+    def retrieve(self, keys_in, flags_out, num_in=None, stream=None,
+                 probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+                 status_handler=None, ignore=0):
+        """Membership flags (one byte per key: bool / uint8 tensor)."""
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        _check_width(flags_out, 1, "flags_out")
+        h = _handler(status_out, status_handler)
+        _check(lib().wc_hashset_retrieve(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                         _ptr(flags_out), _stream(stream),
+                                         int(probing_length), _ptr(status_out), h,
+                                         int(ignore)))
+
+    contains = retrieve
+
+    def erase(self, keys_in, num_in=None, stream=None,
+              probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+              status_handler=None, ignore=0):
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        h = _handler(status_out, status_handler)
+        _check(lib().wc_hashset_erase(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                      _stream(stream), int(probing_length),
+                                      _ptr(status_out), h, int(ignore)))
+
+
+class CountingHashTable(_Table):
+    """warpcore::CountingHashTable (counting_hash_table.cuh:18-26); default CG 4."""
+
+    def __init__(self, min_capacity, seed=DEFAULT_SEED, max_count=None, no_init=False,
+                 key_bytes=4, value_bytes=None, empty_key=None, tombstone_key=None,
+                 probing=None, hasher1=None, hasher2=None, cg_size=None):
+        value_bytes = key_bytes if value_bytes is None else value_bytes
+        if max_count is None:
+            max_count = (1 << (8 * value_bytes)) - 1
+        cfg = _table_config(lib().wc_counting_default_config, key_bytes, value_bytes,
+                            empty_key, tombstone_key, probing, hasher1, hasher2, cg_size)
+        self._make(lib().wc_counting_create, cfg, int(min_capacity), int(seed),
+                   int(max_count), int(bool(no_init)))
+
+    @property
+    def max_count(self):
+        return self.info().max_count
+
+    def insert(self, keys_in, num_in=None, stream=None,
+               probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+               status_handler=None, ignore=0):
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        h = _handler(status_out, status_handler)
+        _check(lib().wc_counting_insert(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                        _stream(stream), int(probing_length),
+                                        _ptr(status_out), h, int(ignore)))
+
+    def retrieve(self, keys_in, values_out, num_in=None, stream=None,
+                 probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+                 status_handler=None, ignore=0):
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        _check_width(values_out, self._cfg.value_bytes, "values_out")
+        h = _handler(status_out, status_handler)
+        _check(lib().wc_counting_retrieve(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                          _ptr(values_out), _stream(stream),
+                                          int(probing_length), _ptr(status_out), h,
+                                          int(ignore)))
+
+    def erase(self, keys_in, num_in=None, stream=None,
+              probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+              status_handler=None, ignore=0):
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        h = _handler(status_out, status_handler)
+        _check(lib().wc_counting_erase(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                       _stream(stream), int(probing_length),
+                                       _ptr(status_out), h, int(ignore)))
+
+
+class BloomFilter:
+    """warpcore::BloomFilter<Key, Hasher, Slot, CGSize> (bloom_filter.cuh:15-20)."""
+
+    def __init__(self, num_bits, k, seed=DEFAULT_SEED, key_bytes=8, slot_bytes=8,
+                 cg_size=1, hasher=HASH_MURMUR):
+        cfg = BloomConfig(key_bytes, slot_bytes, cg_size, hasher)
+        h = ctypes.c_void_p()
+        _check(lib().wc_bloom_create(ctypes.byref(cfg), int(num_bits), int(k), int(seed),
+                                     ctypes.byref(h)))
+        self._h = h
+        self._cfg = cfg
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().wc_bloom_destroy(h)
+            self._h = None
+
+    def info(self):
+        inf = BloomInfo()
+        _check(lib().wc_bloom_get_info(self._h, ctypes.byref(inf)))
+        return inf
+
+    def num_bits(self):
+        return self.info().num_bits
+
+    def num_slots(self):
+        return self.info().num_slots
+
+    def num_blocks(self):
+        return self.info().num_blocks
+
+    def k(self):
+        return self.info().k
+
+    def words_ptr(self):
+        return self.info().words
+
+    def init(self, seed=None, stream=None):
+        _check(lib().wc_bloom_init(self._h, int(self.info().seed if seed is None else seed),
+                                   _stream(stream)))
+
+    def insert(self, keys_in, num_in=None, stream=None):
+        _check_width(keys_in, self._cfg.key_bytes, "keys_in")
+        _check(lib().wc_bloom_insert(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                     _stream(stream)))
+
+    def retrieve(self, keys_in, flags_out, num_in=None, stream=None):
+        _check_width(keys_in, self._cfg.key_bytes, "keys_in")
+        _check_width(flags_out, 1, "flags_out")
+        _check(lib().wc_bloom_retrieve(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                       _ptr(flags_out), _stream(stream)))
+
+    def fpr(self, n):
+        out = ctypes.c_double()
+        _check(lib().wc_bloom_fpr(self._h, int(n), ctypes.byref(out)))
+        return out.value
+
+
+def _handler(status_out, status_handler):
+    if status_handler is not None:
+        return int(status_handler)
+    if status_out is None:
+        return HANDLER_NOTHING
+    return HANDLER_STATUS if status_out.element_size() == 4 else HANDLER_BOOLEAN

@@ -1,0 +1,149 @@
+/*
+ * wc_bloom.cuh -- pattern-blocked Bloom filter kernels
+ * (the reference's BloomFilter::insert / retrieve, bloom_filter.cuh:168-237,
+ * launched by kernels::bloom_filter::insert / retrieve, gpu_engine.cuh:130-171).
+ *
+ * A block is cg_size consecutive slots (words).  The bit pattern of a key is
+ * the reference's: block = h(key+seed) % num_blocks, bit i (i < k) =
+ * h(key+seed+i) % block_bits, owned by word bit / slot_bits of the block, and
+ * the word index wraps modulo num_slots for a ragged last block.  A warp takes
+ * 32 keys; lane l owns key l.  A block is read by TPK lanes with 16-byte
+ * vector loads (one request per block) for all 32 keys before any is tested.
+ * Insert ORs only the words that miss bits (one atomicOr per such word, as
+ * the reference), query tests the whole block and writes one byte per key.
+ */
+#ifndef WC_BLOOM_CUH
+#define WC_BLOOM_CUH
+
+#include "wc_kernels.cuh"
+
+namespace warpcore {
+namespace b200 {
+
+struct BloomArgs {
+    void *words;
+    const void *keys;
+    unsigned char *flags_out;
+    uint64_t n;
+    uint64_t num_slots;
+    uint64_t num_blocks;
+    uint64_t k;
+    uint64_t seed;
+    uint32_t hasher;
+};
+
+template <class S>
+__device__ __forceinline__ S lane_word(const LaneWords &lw, int s)
+{
+    if constexpr (sizeof(S) == 4) return lw.w[s];
+    else return uint64_t(lw.w[2 * s]) | (uint64_t(lw.w[2 * s + 1]) << 32);
+}
+
+template <class T>
+__device__ __forceinline__ T atomic_or_any(T *p, T v)
+{
+    if constexpr (sizeof(T) == 8)
+        return T(atomicOr(reinterpret_cast<unsigned long long *>(p), (unsigned long long)v));
+    else
+        return T(atomicOr(reinterpret_cast<unsigned int *>(p), (unsigned int)v));
+}
+
+template <class K, class S, int CG, bool INSERT>
+__global__ void __launch_bounds__(256) bloom_kernel(const BloomArgs a)
+{
+    constexpr int SB = sizeof(S);
+    constexpr int BB = CG * SB;                 /* block bytes */
+    constexpr int LB = BB < 16 ? BB : 16;       /* bytes per lane */
+    constexpr int TPK = BB / LB;                /* lanes per block */
+    constexpr int SPL = LB / SB;                /* words per lane */
+    constexpr int G = 32 / TPK;
+    constexpr uint64_t kSlotBits = SB * 8;
+    constexpr uint64_t kBlockBits = kSlotBits * CG;
+    constexpr uint32_t kGroupMask = TPK == 32 ? kFull : ((1u << TPK) - 1u);
+
+    const int lane = threadIdx.x & 31;
+    const int g = lane / TPK;
+    const int q = lane % TPK;
+    const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    S *const words = reinterpret_cast<S *>(a.words);
+    const K *const keys = reinterpret_cast<const K *>(a.keys);
+    const K seed = K(a.seed);
+
+    for (uint64_t base = warp * 32; base < a.n; base += nwarps * 32) {
+        const uint64_t i = base + lane;
+        const bool active = i < a.n;
+        const K key = active ? ld_stream(keys + i) : K(0);
+        const uint64_t blk = mod_u64(hash_key<K>(a.hasher, K(key + seed)), a.num_blocks);
+
+        LaneWords win[TPK];
+        bool own_ok[TPK];
+#pragma unroll
+        for (int r = 0; r < TPK; ++r) {
+            const int o = r * G + g; /* owner lane of this round's block */
+            const uint64_t b = shfl_any(blk, o);
+            own_ok[r] = (base + o) < a.n;
+            const uint64_t w0 = b * CG + uint64_t(q) * SPL;
+            if (own_ok[r]) {
+                if (b * CG + CG <= a.num_slots) {
+                    win[r] = load_lane<LB>(words + w0);
+                } else {
+                    /* ragged last block: words wrap to the front */
+#pragma unroll
+                    for (int s = 0; s < SPL; ++s) {
+                        const S v = __ldcg(reinterpret_cast<const S *>(words) + (w0 + s) % a.num_slots);
+                        if constexpr (SB == 4) win[r].w[s] = uint32_t(v);
+                        else { win[r].w[2 * s] = uint32_t(v); win[r].w[2 * s + 1] = uint32_t(uint64_t(v) >> 32); }
+                    }
+                }
+            } else {
+                win[r] = LaneWords{{0u, 0u, 0u, 0u}};
+            }
+        }
+
+        bool my_flag = false;
+#pragma unroll
+        for (int r = 0; r < TPK; ++r) {
+            const int o = r * G + g;
+            const K kr = shfl_any(key, o);
+            const uint64_t b = shfl_any(blk, o);
+            S mask[SPL];
+#pragma unroll
+            for (int s = 0; s < SPL; ++s) mask[s] = 0;
+            for (uint64_t j = 0; j < a.k; ++j) {
+                const uint64_t h = mod_u64(hash_key<K>(a.hasher, K(kr + seed + K(j))), kBlockBits);
+                const int word = int(h / kSlotBits);
+                if (word / SPL == q) {
+#pragma unroll
+                    for (int s = 0; s < SPL; ++s)
+                        if (word % SPL == s) mask[s] |= S(1) << (h % kSlotBits);
+                }
+            }
+            bool ok = true;
+#pragma unroll
+            for (int s = 0; s < SPL; ++s) {
+                const S w = lane_word<S>(win[r], s);
+                const bool missing = (w & mask[s]) != mask[s];
+                ok &= !missing;
+                if (INSERT && own_ok[r] && missing)
+                    atomic_or_any(words + (b * CG + uint64_t(q) * SPL + s) % a.num_slots, mask[s]);
+            }
+            if constexpr (!INSERT) {
+                const unsigned bad = __ballot_sync(kFull, !ok);
+                /* lane r*G + gg owns the block read by group gg this round */
+                if (lane / G == r) {
+                    const int gg = lane - r * G;
+                    my_flag = ((bad >> (gg * TPK)) & kGroupMask) == 0;
+                }
+            }
+        }
+        if constexpr (!INSERT) {
+            if (active) a.flags_out[i] = (unsigned char)my_flag;
+        }
+    }
+}
+
+} // namespace b200
+} // namespace warpcore
+
+#endif /* WC_BLOOM_CUH */

@@ -1,0 +1,754 @@
+/*
+ * wc_capi.cu -- host side of the C ABI declared in include/warpcore_b200.h.
+ *
+ * Owns the device allocations of each table / filter (the reference's
+ * constructors allocate with cudaMalloc and the destructors free,
+ * single_value_hash_table.cuh:112-169, storage.cuh:454-516), checks arguments,
+ * picks the kernel for (slot layout, window width, operation) and sizes the
+ * grid as a whole number of waves: SM count x resident blocks per SM.
+ */
+#include <warpcore_b200.h>
+
+#include "wc_internal.h"
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+
+#include "wc_primes.inc"
+
+using namespace warpcore::b200;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what)
+{
+    return fail(e == cudaErrorMemoryAllocation ? WC_ERR_OUT_OF_MEMORY : WC_ERR_CUDA,
+                "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define WC_CUDA(call)                                                          \
+    do {                                                                       \
+        cudaError_t e_ = (call);                                               \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);                    \
+    } while (0)
+
+/* ---- capacity rule (base.cuh:27-34) over the generated prime table ---- */
+
+const uint64_t *prime_table()
+{
+    static uint64_t *table = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        table = new uint64_t[kNumPrimes];
+        uint64_t p = kPrimeStep + kPrimeGaps[0];
+        table[0] = p;
+        for (uint64_t i = 1; i < kNumPrimes; ++i) {
+            p += kPrimeStep + kPrimeGaps[i];
+            table[i] = p;
+        }
+    });
+    return table;
+}
+
+uint64_t valid_capacity(uint64_t min_capacity, uint64_t cg)
+{
+    const uint64_t *pt = prime_table();
+    const uint64_t x = (min_capacity + cg - 1) / cg;
+    uint64_t lo = 0, hi = kNumPrimes;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) / 2;
+        if (pt[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo == kNumPrimes ? 0 : pt[lo] * cg;
+}
+
+bool valid_cg(uint32_t cg)
+{
+    return cg == 1 || cg == 2 || cg == 4 || cg == 8 || cg == 16 || cg == 32;
+}
+
+/* ---- launch geometry ---- */
+
+struct DeviceProps {
+    int sms = 148;
+};
+
+const DeviceProps &device_props()
+{
+    static std::mutex mu;
+    static std::unordered_map<int, DeviceProps> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(dev);
+    if (it != cache.end()) return it->second;
+    DeviceProps p;
+    cudaDeviceGetAttribute(&p.sms, cudaDevAttrMultiProcessorCount, dev);
+    return cache.emplace(dev, p).first->second;
+}
+
+int blocks_per_sm(const void *kernel, int block)
+{
+    static std::mutex mu;
+    static std::unordered_map<const void *, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(kernel);
+    if (it != cache.end()) return it->second;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, block, 0) != cudaSuccess || n < 1) {
+        cudaGetLastError();
+        n = 1;
+    }
+    cache.emplace(kernel, n);
+    return n;
+}
+
+/* grid for `items` work items of which one block handles `per_block` per
+ * pass; at most one full wave of resident blocks (grid-stride beyond) */
+unsigned grid_for(const void *kernel, int block, uint64_t items, uint64_t per_block)
+{
+    const uint64_t wave = uint64_t(device_props().sms) * blocks_per_sm(kernel, block);
+    uint64_t need = (items + per_block - 1) / per_block;
+    if (need < 1) need = 1;
+    return unsigned(need < wave ? need : wave);
+}
+
+constexpr int kBlock = 256;
+
+} // namespace
+
+/* ------------------------------------------------------------------ */
+/* handles                                                              */
+/* ------------------------------------------------------------------ */
+
+struct wc_table {
+    int kind = 0; /* 0 single-value, 1 hash set, 2 counting */
+    wc_table_config cfg{};
+    int layout = 0;
+    uint32_t slot_bytes = 0;
+    uint64_t capacity = 0;
+    uint64_t num_buckets = 0;
+    uint64_t seed = 0;
+    uint64_t max_count = 0;
+    bool initialized = false;
+    void *slots = nullptr;
+    uint32_t *status = nullptr;            /* device Status word */
+    unsigned long long *counter = nullptr; /* device scratch counter */
+    int device = 0;
+};
+
+struct wc_bloom {
+    wc_bloom_config cfg{};
+    uint64_t num_bits = 0, num_slots = 0, num_blocks = 0, k = 0, seed = 0;
+    void *words = nullptr;
+    int device = 0;
+};
+
+namespace {
+
+uint64_t key_mask(uint32_t key_bytes)
+{
+    return key_bytes == 4 ? 0xffffffffull : ~0ull;
+}
+
+TableView view_of(const wc_table *t)
+{
+    TableView v;
+    v.slots = t->slots;
+    v.status = t->status;
+    v.num_buckets = t->num_buckets;
+    v.seed = t->seed;
+    v.empty_key = t->cfg.empty_key;
+    v.tombstone_key = t->cfg.tombstone_key;
+    v.max_count = t->max_count;
+    v.probing = t->cfg.probing;
+    v.hasher1 = t->cfg.hasher1;
+    v.hasher2 = t->cfg.hasher2;
+    v.cg_size = t->cfg.cg_size;
+    return v;
+}
+
+int check_config(const wc_table_config *cfg, int kind)
+{
+    if (!cfg) return fail(WC_ERR_INVALID_ARGUMENT, "config is NULL");
+    if (cfg->key_bytes != 4 && cfg->key_bytes != 8)
+        return fail(WC_ERR_UNSUPPORTED, "key_bytes must be 4 or 8");
+    if (kind != 1 && cfg->value_bytes != cfg->key_bytes)
+        return fail(WC_ERR_UNSUPPORTED, "value_bytes must equal key_bytes (got %u/%u)",
+                    cfg->key_bytes, cfg->value_bytes);
+    if (!valid_cg(cfg->cg_size))
+        return fail(WC_ERR_INVALID_ARGUMENT, "cg_size must be 1, 2, 4, 8, 16 or 32");
+    if (cfg->probing > WC_PROBING_QUADRATIC)
+        return fail(WC_ERR_INVALID_ARGUMENT, "unknown probing scheme %u", cfg->probing);
+    if (cfg->hasher1 > WC_HASH_IDENTITY64 || cfg->hasher2 > WC_HASH_IDENTITY64)
+        return fail(WC_ERR_INVALID_ARGUMENT, "unknown hasher");
+    const uint64_t km = key_mask(cfg->key_bytes);
+    if ((cfg->empty_key & km) == (cfg->tombstone_key & km))
+        return fail(WC_ERR_INVALID_ARGUMENT, "empty key and tombstone key must differ");
+    return WC_OK;
+}
+
+int fill_slots(wc_table *t, cudaStream_t stream)
+{
+    /* 16 bytes of empty slots: key = empty, payload = 0 */
+    const uint64_t e = t->cfg.empty_key & key_mask(t->cfg.key_bytes);
+    uint32_t w[4];
+    switch (t->layout) {
+    case kLayoutKV32: w[0] = uint32_t(e); w[1] = 0; w[2] = uint32_t(e); w[3] = 0; break;
+    case kLayoutKV64: w[0] = uint32_t(e); w[1] = uint32_t(e >> 32); w[2] = 0; w[3] = 0; break;
+    case kLayoutSet32: w[0] = w[1] = w[2] = w[3] = uint32_t(e); break;
+    default: w[0] = uint32_t(e); w[1] = uint32_t(e >> 32); w[2] = w[0]; w[3] = w[1]; break;
+    }
+    const uint4 pattern = make_uint4(w[0], w[1], w[2], w[3]);
+    const uint64_t n_u32 = t->capacity * t->slot_bytes / 4;
+    const void *kfn = reinterpret_cast<const void *>(fill_kernel<0>);
+    const unsigned grid = grid_for(kfn, kBlock, n_u32 / 4, kBlock);
+    fill_kernel<0><<<grid, kBlock, 0, stream>>>(reinterpret_cast<uint32_t *>(t->slots), n_u32, pattern);
+    WC_CUDA(cudaGetLastError());
+    return WC_OK;
+}
+
+int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, uint64_t seed,
+                 uint64_t max_count, int no_init, wc_table **out)
+{
+    if (!out) return fail(WC_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int rc = check_config(cfg, kind);
+    if (rc) return rc;
+    const uint64_t cap = valid_capacity(min_capacity, cfg->cg_size);
+    if (cap == 0)
+        return fail(WC_ERR_INVALID_ARGUMENT,
+                    "min_capacity %llu exceeds the largest table capacity",
+                    (unsigned long long)min_capacity);
+    auto *t = new wc_table();
+    t->kind = kind;
+    t->cfg = *cfg;
+    if (kind == 1) t->cfg.value_bytes = 0;
+    t->cfg.empty_key &= key_mask(cfg->key_bytes);
+    t->cfg.tombstone_key &= key_mask(cfg->key_bytes);
+    if (kind == 1) {
+        t->layout = cfg->key_bytes == 4 ? kLayoutSet32 : kLayoutSet64;
+        t->slot_bytes = cfg->key_bytes;
+    } else {
+        t->layout = cfg->key_bytes == 4 ? kLayoutKV32 : kLayoutKV64;
+        t->slot_bytes = 2 * cfg->key_bytes;
+    }
+    t->capacity = cap;
+    t->num_buckets = cap / cfg->cg_size;
+    t->seed = seed & key_mask(cfg->key_bytes);
+    const uint64_t vmax = cfg->value_bytes == 4 ? 0xffffffffull : ~0ull;
+    t->max_count = kind == 2 ? (max_count < vmax ? max_count : vmax) : ~0ull;
+    cudaGetDevice(&t->device);
+
+    /* the reference checks free memory before allocating (storage.cuh:464-473) */
+    const uint64_t bytes = cap * t->slot_bytes;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        delete t;
+        return cuda_fail(cudaGetLastError(), "cudaMemGetInfo");
+    }
+    if (bytes + 4096 > free_b) {
+        delete t;
+        return fail(WC_ERR_OUT_OF_MEMORY, "table needs %llu bytes, %llu free",
+                    (unsigned long long)bytes, (unsigned long long)free_b);
+    }
+    cudaError_t e = cudaMalloc(&t->slots, bytes);
+    if (e == cudaSuccess) {
+        void *aux = nullptr;
+        e = cudaMalloc(&aux, 256);
+        if (e == cudaSuccess) {
+            t->status = reinterpret_cast<uint32_t *>(aux);
+            t->counter = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(aux) + 128);
+        }
+    }
+    if (e != cudaSuccess) {
+        if (t->slots) cudaFree(t->slots);
+        delete t;
+        return cuda_fail(e, "cudaMalloc");
+    }
+    e = cudaMemset(t->status, 0, 256);
+    if (e != cudaSuccess) {
+        wc_table_destroy(t);
+        return cuda_fail(e, "cudaMemset");
+    }
+    if (!no_init) {
+        rc = wc_table_init(t, t->seed, nullptr);
+        if (rc) {
+            wc_table_destroy(t);
+            return rc;
+        }
+    }
+    *out = t;
+    return WC_OK;
+}
+
+int check_table(const wc_table *t, int kind_mask)
+{
+    if (!t) return fail(WC_ERR_INVALID_ARGUMENT, "table is NULL");
+    if (!((1 << t->kind) & kind_mask))
+        return fail(WC_ERR_INVALID_ARGUMENT, "operation does not apply to this table kind");
+    if (!t->initialized) return fail(WC_ERR_NOT_INITIALIZED, "table is not initialized");
+    return WC_OK;
+}
+
+TableKernel pick_table_kernel(const wc_table *t, int op)
+{
+    const int W = int(t->cfg.cg_size);
+    switch (t->layout) {
+    case kLayoutKV32: return table_kernel_kv32(W, op);
+    case kLayoutKV64: return table_kernel_kv64(W, op);
+    case kLayoutSet32: return table_kernel_set32(W, op);
+    default: return table_kernel_set64(W, op);
+    }
+}
+
+int table_op(wc_table *t, int op, const void *keys, const void *values, void *out,
+             uint64_t n, wc_stream_t stream, uint64_t probing_length, void *status_out,
+             int handler, uint32_t ignore)
+{
+    if (handler < WC_HANDLER_NOTHING || handler > WC_HANDLER_BOOLEAN)
+        return fail(WC_ERR_INVALID_ARGUMENT, "unknown status handler %d", handler);
+    if (n == 0) return WC_OK;
+    if (!keys) return fail(WC_ERR_INVALID_ARGUMENT, "keys_in is NULL");
+    if (op == kOpInsert && t->kind == 0 && !values)
+        return fail(WC_ERR_INVALID_ARGUMENT, "values_in is NULL");
+    if (op == kOpRetrieve && !out) return fail(WC_ERR_INVALID_ARGUMENT, "output is NULL");
+    TableKernel k = pick_table_kernel(t, op);
+    if (!k) return fail(WC_ERR_UNSUPPORTED, "no kernel for this configuration");
+    TableOpArgs a;
+    a.t = view_of(t);
+    a.keys = keys;
+    a.values = values;
+    a.out = out;
+    a.status_out = handler == WC_HANDLER_NOTHING ? nullptr : status_out;
+    a.n = n;
+    a.max_windows = max_windows(probing_length, t->cfg.cg_size, t->num_buckets);
+    a.bool_mask = (~ignore) ^ 0xFFFu; /* ~Status(Ignore), status.cuh:142-146 */
+    a.handler = handler;
+    a.is_set = t->kind == 1;
+    const unsigned grid = grid_for(reinterpret_cast<const void *>(k), kBlock, n, kBlock);
+    void *args[] = {&a};
+    WC_CUDA(cudaLaunchKernel(reinterpret_cast<const void *>(k), dim3(grid), dim3(kBlock), args, 0,
+                             reinterpret_cast<cudaStream_t>(stream)));
+    return WC_OK;
+}
+
+} // namespace
+
+/* ------------------------------------------------------------------ */
+/* C ABI                                                                 */
+/* ------------------------------------------------------------------ */
+
+extern "C" {
+
+const char *wc_last_error(void) { return g_last_error.c_str(); }
+
+const char *wc_version(void) { return "warpcore-b200 0.1 (sm_100a)"; }
+
+void wc_svht_default_config(wc_table_config *cfg, uint32_t key_bytes, uint32_t value_bytes)
+{
+    if (!cfg) return;
+    cfg->key_bytes = key_bytes;
+    cfg->value_bytes = value_bytes;
+    cfg->empty_key = 0;
+    cfg->tombstone_key = key_mask(key_bytes);
+    cfg->probing = WC_PROBING_DOUBLE;
+    cfg->hasher1 = WC_HASH_MURMUR;
+    cfg->hasher2 = WC_HASH_MURMUR;
+    cfg->cg_size = 8;
+}
+
+void wc_hashset_default_config(wc_table_config *cfg, uint32_t key_bytes)
+{
+    wc_svht_default_config(cfg, key_bytes, 0);
+    if (cfg) cfg->cg_size = 16;
+}
+
+void wc_counting_default_config(wc_table_config *cfg, uint32_t key_bytes, uint32_t value_bytes)
+{
+    wc_svht_default_config(cfg, key_bytes, value_bytes);
+    if (cfg) cfg->cg_size = 4;
+}
+
+uint64_t wc_valid_capacity(uint64_t min_capacity, uint64_t cg_size)
+{
+    if (!valid_cg(uint32_t(cg_size))) return 0;
+    return valid_capacity(min_capacity, cg_size);
+}
+
+int wc_svht_create(const wc_table_config *cfg, uint64_t min_capacity, uint64_t seed, int no_init,
+                   wc_table **out)
+{
+    return table_create(0, cfg, min_capacity, seed, 0, no_init, out);
+}
+
+int wc_hashset_create(const wc_table_config *cfg, uint64_t min_capacity, uint64_t seed,
+                      wc_table **out)
+{
+    return table_create(1, cfg, min_capacity, seed, 0, 0, out);
+}
+
+int wc_counting_create(const wc_table_config *cfg, uint64_t min_capacity, uint64_t seed,
+                       uint64_t max_count, int no_init, wc_table **out)
+{
+    return table_create(2, cfg, min_capacity, seed, max_count, no_init, out);
+}
+
+int wc_table_destroy(wc_table *t)
+{
+    if (!t) return WC_OK;
+    if (t->slots) cudaFree(t->slots);
+    if (t->status) cudaFree(t->status);
+    delete t;
+    return WC_OK;
+}
+
+int wc_table_init(wc_table *t, uint64_t seed, wc_stream_t stream)
+{
+    if (!t) return fail(WC_ERR_INVALID_ARGUMENT, "table is NULL");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    t->initialized = false;
+    t->seed = seed & key_mask(t->cfg.key_bytes);
+    int rc = fill_slots(t, s);
+    if (rc) return rc;
+    WC_CUDA(cudaMemsetAsync(t->status, 0, sizeof(uint32_t), s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    t->initialized = true;
+    return WC_OK;
+}
+
+int wc_svht_insert(wc_table *t, const void *keys_in, const void *values_in, uint64_t num_in,
+                   wc_stream_t stream, uint64_t probing_length, void *status_out,
+                   int status_handler, uint32_t ignore)
+{
+    int rc = check_table(t, 1 << 0);
+    if (rc) return rc;
+    return table_op(t, kOpInsert, keys_in, values_in, nullptr, num_in, stream, probing_length,
+                    status_out, status_handler, ignore);
+}
+
+int wc_svht_retrieve(wc_table *t, const void *keys_in, uint64_t num_in, void *values_out,
+                     wc_stream_t stream, uint64_t probing_length, void *status_out,
+                     int status_handler, uint32_t ignore)
+{
+    int rc = check_table(t, 1 << 0);
+    if (rc) return rc;
+    return table_op(t, kOpRetrieve, keys_in, nullptr, values_out, num_in, stream,
+                    probing_length, status_out, status_handler, ignore);
+}
+
+int wc_svht_erase(wc_table *t, const void *keys_in, uint64_t num_in, wc_stream_t stream,
+                  uint64_t probing_length, void *status_out, int status_handler, uint32_t ignore)
+{
+    int rc = check_table(t, 1 << 0);
+    if (rc) return rc;
+    return table_op(t, kOpErase, keys_in, nullptr, nullptr, num_in, stream, probing_length,
+                    status_out, status_handler, ignore);
+}
+
+int wc_hashset_insert(wc_table *t, const void *keys_in, uint64_t num_in, wc_stream_t stream,
+                      uint64_t probing_length, void *status_out, int status_handler,
+                      uint32_t ignore)
+{
+    int rc = check_table(t, 1 << 1);
+    if (rc) return rc;
+    return table_op(t, kOpInsert, keys_in, nullptr, nullptr, num_in, stream, probing_length,
+                    status_out, status_handler, ignore);
+}
+
+int wc_hashset_retrieve(wc_table *t, const void *keys_in, uint64_t num_in, uint8_t *flags_out,
+                        wc_stream_t stream, uint64_t probing_length, void *status_out,
+                        int status_handler, uint32_t ignore)
+{
+    int rc = check_table(t, 1 << 1);
+    if (rc) return rc;
+    return table_op(t, kOpRetrieve, keys_in, nullptr, flags_out, num_in, stream,
+                    probing_length, status_out, status_handler, ignore);
+}
+
+int wc_hashset_erase(wc_table *t, const void *keys_in, uint64_t num_in, wc_stream_t stream,
+                     uint64_t probing_length, void *status_out, int status_handler,
+                     uint32_t ignore)
+{
+    int rc = check_table(t, 1 << 1);
+    if (rc) return rc;
+    return table_op(t, kOpErase, keys_in, nullptr, nullptr, num_in, stream, probing_length,
+                    status_out, status_handler, ignore);
+}
+
+int wc_counting_insert(wc_table *t, const void *keys_in, uint64_t num_in, wc_stream_t stream,
+                       uint64_t probing_length, void *status_out, int status_handler,
+                       uint32_t ignore)
+{
+    int rc = check_table(t, 1 << 2);
+    if (rc) return rc;
+    return table_op(t, kOpCount, keys_in, nullptr, nullptr, num_in, stream, probing_length,
+                    status_out, status_handler, ignore);
+}
+
+int wc_counting_retrieve(wc_table *t, const void *keys_in, uint64_t num_in, void *values_out,
+                         wc_stream_t stream, uint64_t probing_length, void *status_out,
+                         int status_handler, uint32_t ignore)
+{
+    int rc = check_table(t, 1 << 2);
+    if (rc) return rc;
+    return table_op(t, kOpRetrieve, keys_in, nullptr, values_out, num_in, stream,
+                    probing_length, status_out, status_handler, ignore);
+}
+
+int wc_counting_erase(wc_table *t, const void *keys_in, uint64_t num_in, wc_stream_t stream,
+                      uint64_t probing_length, void *status_out, int status_handler,
+                      uint32_t ignore)
+{
+    int rc = check_table(t, 1 << 2);
+    if (rc) return rc;
+    return table_op(t, kOpErase, keys_in, nullptr, nullptr, num_in, stream, probing_length,
+                    status_out, status_handler, ignore);
+}
+
+int wc_table_size(wc_table *t, wc_stream_t stream, uint64_t *size_out)
+{
+    if (!size_out) return fail(WC_ERR_INVALID_ARGUMENT, "size_out is NULL");
+    *size_out = 0;
+    int rc = check_table(t, 7);
+    if (rc) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    CountKernel k = count_kernel(t->layout);
+    WC_CUDA(cudaMemsetAsync(t->counter, 0, sizeof(unsigned long long), s));
+    const uint64_t nvec = t->capacity * t->slot_bytes / 16;
+    const unsigned grid = grid_for(reinterpret_cast<const void *>(k), kBlock, nvec, kBlock * 4);
+    k<<<grid, kBlock, 0, s>>>(t->slots, t->capacity, t->cfg.empty_key, t->cfg.tombstone_key,
+                              t->counter);
+    WC_CUDA(cudaGetLastError());
+    unsigned long long h = 0;
+    WC_CUDA(cudaMemcpyAsync(&h, t->counter, sizeof(h), cudaMemcpyDeviceToHost, s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    *size_out = h;
+    return WC_OK;
+}
+
+int wc_table_retrieve_all(wc_table *t, void *keys_out, void *values_out, uint64_t *num_out,
+                          wc_stream_t stream)
+{
+    if (!num_out || !keys_out) return fail(WC_ERR_INVALID_ARGUMENT, "NULL output");
+    *num_out = 0;
+    int rc = check_table(t, 7);
+    if (rc) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    DumpKernel k = dump_kernel_ptr(t->layout);
+    WC_CUDA(cudaMemsetAsync(t->counter, 0, sizeof(unsigned long long), s));
+    const unsigned grid = grid_for(reinterpret_cast<const void *>(k), kBlock, t->capacity, kBlock);
+    k<<<grid, kBlock, 0, s>>>(t->slots, t->capacity, t->cfg.empty_key, t->cfg.tombstone_key,
+                              keys_out, t->kind == 1 ? nullptr : values_out, t->counter);
+    WC_CUDA(cudaGetLastError());
+    unsigned long long h = 0;
+    WC_CUDA(cudaMemcpyAsync(&h, t->counter, sizeof(h), cudaMemcpyDeviceToHost, s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    *num_out = h;
+    return WC_OK;
+}
+
+int wc_table_peek_status(wc_table *t, wc_stream_t stream, uint32_t *out)
+{
+    if (!t || !out) return fail(WC_ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t h = 0;
+    WC_CUDA(cudaMemcpyAsync(&h, t->status, sizeof(h), cudaMemcpyDeviceToHost, s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    *out = t->initialized ? h : (h | WC_STATUS_NOT_INITIALIZED);
+    return WC_OK;
+}
+
+int wc_table_pop_status(wc_table *t, wc_stream_t stream, uint32_t *out)
+{
+    int rc = wc_table_peek_status(t, stream, out);
+    if (rc) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    WC_CUDA(cudaMemsetAsync(t->status, 0, sizeof(uint32_t), s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    return WC_OK;
+}
+
+int wc_table_get_info(const wc_table *t, wc_table_info *info)
+{
+    if (!t || !info) return fail(WC_ERR_INVALID_ARGUMENT, "NULL argument");
+    info->kind = uint32_t(t->kind);
+    info->key_bytes = t->cfg.key_bytes;
+    info->value_bytes = t->cfg.value_bytes;
+    info->slot_bytes = t->slot_bytes;
+    info->cg_size = t->cfg.cg_size;
+    info->probing = t->cfg.probing;
+    info->hasher1 = t->cfg.hasher1;
+    info->hasher2 = t->cfg.hasher2;
+    info->capacity = t->capacity;
+    info->num_buckets = t->num_buckets;
+    info->seed = t->seed;
+    info->empty_key = t->cfg.empty_key;
+    info->tombstone_key = t->cfg.tombstone_key;
+    info->max_count = t->max_count;
+    info->bytes_total = t->capacity * t->slot_bytes + 256;
+    info->slots = t->slots;
+    info->status = t->status;
+    info->is_initialized = t->initialized ? 1 : 0;
+    return WC_OK;
+}
+
+/* ---- Bloom filter ---- */
+
+int wc_bloom_create(const wc_bloom_config *cfg, uint64_t num_bits, uint64_t k, uint64_t seed,
+                    wc_bloom **out)
+{
+    if (!out || !cfg) return fail(WC_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    if (cfg->key_bytes != 4 && cfg->key_bytes != 8)
+        return fail(WC_ERR_UNSUPPORTED, "key_bytes must be 4 or 8");
+    if (cfg->slot_bytes != 4 && cfg->slot_bytes != 8)
+        return fail(WC_ERR_UNSUPPORTED, "slot_bytes must be 4 or 8");
+    if (!valid_cg(cfg->cg_size)) return fail(WC_ERR_INVALID_ARGUMENT, "bad cg_size");
+    if (cfg->hasher > WC_HASH_IDENTITY64) return fail(WC_ERR_INVALID_ARGUMENT, "unknown hasher");
+    if (num_bits == 0) return fail(WC_ERR_INVALID_ARGUMENT, "num_bits must be positive");
+    auto *b = new wc_bloom();
+    b->cfg = *cfg;
+    b->num_bits = num_bits;
+    const uint64_t slot_bits = uint64_t(cfg->slot_bytes) * 8;
+    b->num_slots = (num_bits + slot_bits - 1) / slot_bits;
+    b->num_blocks = (b->num_slots + cfg->cg_size - 1) / cfg->cg_size;
+    b->k = k;
+    b->seed = seed & key_mask(cfg->key_bytes);
+    cudaGetDevice(&b->device);
+    /* padded to whole blocks so that full-block vector loads stay inside */
+    const uint64_t bytes = b->num_blocks * cfg->cg_size * cfg->slot_bytes;
+    cudaError_t e = cudaMalloc(&b->words, bytes);
+    if (e != cudaSuccess) {
+        delete b;
+        return cuda_fail(e, "cudaMalloc");
+    }
+    int rc = wc_bloom_init(b, b->seed, nullptr);
+    if (rc) {
+        wc_bloom_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return WC_OK;
+}
+
+int wc_bloom_destroy(wc_bloom *b)
+{
+    if (!b) return WC_OK;
+    if (b->words) cudaFree(b->words);
+    delete b;
+    return WC_OK;
+}
+
+int wc_bloom_init(wc_bloom *b, uint64_t seed, wc_stream_t stream)
+{
+    if (!b) return fail(WC_ERR_INVALID_ARGUMENT, "filter is NULL");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    b->seed = seed & key_mask(b->cfg.key_bytes);
+    const uint64_t bytes = b->num_blocks * b->cfg.cg_size * b->cfg.slot_bytes;
+    WC_CUDA(cudaMemsetAsync(b->words, 0, bytes, s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    return WC_OK;
+}
+
+static int bloom_op(wc_bloom *b, const void *keys, uint64_t n, uint8_t *flags, wc_stream_t stream,
+                    bool insert)
+{
+    if (!b) return fail(WC_ERR_INVALID_ARGUMENT, "filter is NULL");
+    if (n == 0) return WC_OK;
+    if (!keys) return fail(WC_ERR_INVALID_ARGUMENT, "keys_in is NULL");
+    if (!insert && !flags) return fail(WC_ERR_INVALID_ARGUMENT, "flags_out is NULL");
+    BloomKernel k = bloom_kernel_ptr(int(b->cfg.key_bytes), int(b->cfg.slot_bytes),
+                                     int(b->cfg.cg_size), insert);
+    if (!k) return fail(WC_ERR_UNSUPPORTED, "no kernel for this configuration");
+    BloomArgs a;
+    a.words = b->words;
+    a.keys = keys;
+    a.flags_out = flags;
+    a.n = n;
+    a.num_slots = b->num_slots;
+    a.num_blocks = b->num_blocks;
+    a.k = b->k;
+    a.seed = b->seed;
+    a.hasher = b->cfg.hasher;
+    const unsigned grid = grid_for(reinterpret_cast<const void *>(k), kBlock, n, kBlock);
+    void *args[] = {&a};
+    WC_CUDA(cudaLaunchKernel(reinterpret_cast<const void *>(k), dim3(grid), dim3(kBlock), args, 0,
+                             reinterpret_cast<cudaStream_t>(stream)));
+    return WC_OK;
+}
+
+int wc_bloom_insert(wc_bloom *b, const void *keys_in, uint64_t num_in, wc_stream_t stream)
+{
+    return bloom_op(b, keys_in, num_in, nullptr, stream, true);
+}
+
+int wc_bloom_retrieve(wc_bloom *b, const void *keys_in, uint64_t num_in, uint8_t *flags_out,
+                      wc_stream_t stream)
+{
+    return bloom_op(b, keys_in, num_in, flags_out, stream, false);
+}
+
+int wc_bloom_get_info(const wc_bloom *b, wc_bloom_info *info)
+{
+    if (!b || !info) return fail(WC_ERR_INVALID_ARGUMENT, "NULL argument");
+    info->key_bytes = b->cfg.key_bytes;
+    info->slot_bytes = b->cfg.slot_bytes;
+    info->cg_size = b->cfg.cg_size;
+    info->hasher = b->cfg.hasher;
+    info->num_bits = b->num_bits;
+    info->num_slots = b->num_slots;
+    info->num_blocks = b->num_blocks;
+    info->k = b->k;
+    info->seed = b->seed;
+    info->words = b->words;
+    return WC_OK;
+}
+
+/* the reference's analytic estimate, bloom_filter.cuh:342-408, in the same
+ * double arithmetic (it overflows to NaN for very large filters, as the
+ * reference does) */
+int wc_bloom_fpr(const wc_bloom *b, uint64_t n, double *out)
+{
+    if (!b || !out) return fail(WC_ERR_INVALID_ARGUMENT, "NULL argument");
+    const uint64_t block_bits = uint64_t(b->cfg.slot_bytes) * 8 * b->cfg.cg_size;
+    const uint64_t nblocks_int = b->num_bits / block_bits;
+    if (nblocks_int == 0) return fail(WC_ERR_INVALID_ARGUMENT, "filter smaller than one block");
+    const double bl = double(nblocks_int);
+    double res = 0.0;
+    const uint64_t upper = 5 * n / nblocks_int;
+    const uint64_t m = uint64_t(double(b->num_bits) / bl);
+    for (uint64_t i = 0; i < upper; ++i) {
+        double binom = 1.0;
+        for (uint64_t j = n - i + 1; j <= n; ++j) binom *= double(j);
+        for (uint64_t j = 1; j <= i; ++j) binom /= double(j);
+        binom *= std::pow(1.0 / bl, double(i)) * std::pow(1.0 - 1.0 / bl, double(n - i));
+        const double base = std::pow(1.0 - std::pow(1.0 - 1.0 / double(m), double(i * b->k)),
+                                     double(b->k));
+        res += binom * base;
+    }
+    *out = res;
+    return WC_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,35 @@
+/*
+ * wc_internal.h -- kernel registry shared by the translation units of
+ * libwarpcore_b200.so (not a public header).
+ */
+#ifndef WC_INTERNAL_H
+#define WC_INTERNAL_H
+
+#include "wc_bloom.cuh"
+
+namespace warpcore {
+namespace b200 {
+
+enum : int { kLayoutKV32 = 0, kLayoutKV64 = 1, kLayoutSet32 = 2, kLayoutSet64 = 3 };
+
+using TableKernel = void (*)(TableOpArgs);
+using BloomKernel = void (*)(BloomArgs);
+using CountKernel = void (*)(const void *, uint64_t, uint64_t, uint64_t, unsigned long long *);
+using DumpKernel = void (*)(const void *, uint64_t, uint64_t, uint64_t, void *, void *,
+                            unsigned long long *);
+
+/* kernel for (window width W, op); nullptr if the combination is not built */
+TableKernel table_kernel_kv32(int W, int op);
+TableKernel table_kernel_kv64(int W, int op);
+TableKernel table_kernel_set32(int W, int op);
+TableKernel table_kernel_set64(int W, int op);
+
+CountKernel count_kernel(int layout);
+DumpKernel dump_kernel_ptr(int layout);
+
+BloomKernel bloom_kernel_ptr(int key_bytes, int slot_bytes, int cg, bool insert);
+
+} // namespace b200
+} // namespace warpcore
+
+#endif

@@ -1,0 +1,384 @@
+/*
+ * wc_kernels.cuh -- bulk kernels of the B200-native warpcore library.
+ *
+ * One kernel template serves insert / retrieve / erase of
+ * SingleValueHashTable, HashSet and CountingHashTable (the reference's
+ * kernels::insert / retrieve / erase, gpu_engine.cuh:177-262, 352-376, and
+ * the per-key device methods they call).
+ *
+ * Warp-batched probing
+ *   A warp takes 32 keys at a time; lane l OWNS key l (coalesced input and
+ *   output, one status per lane).  The probe windows of the owned keys are
+ *   fetched cooperatively: TPK lanes load one window with 16-byte vector
+ *   loads (one request per window), and the windows of ALL pending keys of
+ *   the warp are requested before any is inspected, so each warp keeps up to
+ *   32 windows in flight.  Match and empty masks go back to the owner lane
+ *   with ballots; the owner then issues its own compare-and-swap, so the
+ *   claims of all 32 keys leave the SM in the same instruction.  Keys whose
+ *   window had no match and no free slot advance to their next bucket and
+ *   are fetched again in the next wave, packed densely onto the lanes.
+ *   Before any atomic, equal keys inside a warp are merged with
+ *   __match_any_sync: one leader inserts (with the count of its peers for
+ *   counting, with the last peer's value for single-value tables) and the
+ *   others report duplicate_key, as they would in the reference.
+ */
+#ifndef WC_KERNELS_CUH
+#define WC_KERNELS_CUH
+
+#include <warpcore/detail/b200_core.cuh>
+
+namespace warpcore {
+namespace b200 {
+
+enum : int { kOpInsert = 0, kOpCount = 1, kOpRetrieve = 2, kOpErase = 3 };
+
+struct TableOpArgs {
+    TableView t;
+    const void *keys;
+    const void *values;   /* insert */
+    void *out;            /* retrieve: values (tables) or uint8 flags (sets) */
+    void *status_out;
+    uint64_t n;
+    uint64_t max_windows;
+    uint32_t bool_mask;   /* ReturnBoolean: status & mask != 0 */
+    int handler;
+    int is_set;
+};
+
+constexpr unsigned kFull = 0xffffffffu;
+
+template <class T>
+__device__ __forceinline__ T shfl_any(T v, int src)
+{
+    if constexpr (sizeof(T) == 8) {
+        const uint32_t lo = __shfl_sync(kFull, uint32_t(v), src);
+        const uint32_t hi = __shfl_sync(kFull, uint32_t(uint64_t(v) >> 32), src);
+        return T(uint64_t(lo) | (uint64_t(hi) << 32));
+    } else {
+        return T(__shfl_sync(kFull, uint32_t(v), src));
+    }
+}
+
+template <class L, int W, int OP>
+__global__ void __launch_bounds__(256) table_op_kernel(const TableOpArgs a)
+{
+    using K = typename L::key_t;
+    using V = typename L::val_t;
+    constexpr int SB = L::kSlotBytes;
+    constexpr int WB = W * SB;
+    constexpr int LB = WB < 16 ? WB : 16; /* bytes per lane per window */
+    constexpr int TPK = WB / LB;          /* lanes per window */
+    constexpr int SPL = LB / SB;          /* slots per lane */
+    constexpr int G = 32 / TPK;           /* windows per warp per round */
+    constexpr uint32_t kGroupMask = TPK == 32 ? kFull : ((1u << TPK) - 1u);
+    static_assert(TPK * LB == WB && SPL * SB == LB, "window split");
+
+    const TableView &t = a.t;
+    const int lane = threadIdx.x & 31;
+    const int g = lane / TPK;
+    const int q = lane % TPK;
+    const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    const K empty = K(t.empty_key);
+    const K tomb = K(t.tombstone_key);
+    unsigned char *const slots = reinterpret_cast<unsigned char *>(t.slots);
+    const K *const keys = reinterpret_cast<const K *>(a.keys);
+    const unsigned lanemask_lt = (1u << lane) - 1u;
+
+    for (uint64_t base = warp * 32; base < a.n; base += nwarps * 32) {
+        const uint64_t i = base + lane;
+        const bool active = i < a.n;
+        K key = active ? ld_stream(keys + i) : empty;
+        V val = 0;
+        if constexpr (OP == kOpInsert && L::kHasValue) {
+            if (active) val = ld_stream(reinterpret_cast<const V *>(a.values) + i);
+        }
+        uint32_t st = kStNone, join = 0;
+        bool pending = active;
+        if (active && (key == empty || key == tomb)) {
+            st = kStInvalidKey;
+            join = kStInvalidKey;
+            pending = false;
+        }
+
+        uint32_t cnt_add = 1;
+        if constexpr (OP == kOpInsert || OP == kOpCount) {
+            /* merge equal keys of this warp before any atomic */
+            const unsigned pmask0 = __ballot_sync(kFull, pending);
+            const unsigned peers =
+                __match_any_sync(kFull, pending ? key : empty) & pmask0;
+            int last = lane;
+            if (pending) {
+                const int leader = __ffs(peers) - 1;
+                last = 31 - __clz(peers);
+                cnt_add = __popc(peers);
+                if (lane != leader) {
+                    st = kStDuplicateKey;
+                    join |= kStDuplicateKey;
+                    pending = false;
+                }
+            }
+            if constexpr (OP == kOpInsert && L::kHasValue) {
+                /* the leader stores the value of the last equal key */
+                val = shfl_any(val, last);
+            }
+        }
+
+        uint64_t bucket = 0, step = 0, wins = 0;
+        bool flag = false;
+        bool have_out = false;
+        V out = 0;
+        if (pending) bucket = probe_begin<K>(t, key);
+
+        while (__any_sync(kFull, pending)) {
+            const unsigned pmask = __ballot_sync(kFull, pending);
+            const int cnt = __popc(pmask);
+            const int rounds = (cnt + G - 1) / G;
+            const int my_rank = __popc(pmask & lanemask_lt);
+            const int my_round = my_rank / G;
+            const int my_g = my_rank % G;
+
+            /* fetch the windows of all pending keys */
+            LaneWords win[TPK];
+            int own[TPK];
+#pragma unroll
+            for (int r = 0; r < TPK; ++r) {
+                own[r] = -1;
+                if (r < rounds) {
+                    const int idx = r * G + g;
+                    const int o = idx < cnt ? nth_set_bit(pmask, idx) : -1;
+                    own[r] = o;
+                    const uint64_t b = shfl_any(bucket, o < 0 ? lane : o);
+                    if (o >= 0)
+                        win[r] = load_lane<LB>(slots + (b * W + uint64_t(q) * SPL) * SB);
+                    else
+                        win[r] = LaneWords{{0u, 0u, 0u, 0u}};
+                }
+            }
+
+            /* match and empty masks back to the owners */
+            uint32_t hit_bits = 0, empty_bits = 0;
+#pragma unroll
+            for (int r = 0; r < TPK; ++r) {
+                if (r < rounds) {
+                    const K kr = shfl_any(key, own[r] < 0 ? lane : own[r]);
+#pragma unroll
+                    for (int s = 0; s < SPL; ++s) {
+                        const K sk = slot_key<L>(win[r], s);
+                        const unsigned hb = __ballot_sync(kFull, own[r] >= 0 && sk == kr);
+                        const unsigned eb = __ballot_sync(kFull, own[r] >= 0 && sk == empty);
+                        if (pending && my_round == r) {
+                            hit_bits |= spread_bits<TPK, SPL>((hb >> (my_g * TPK)) & kGroupMask, s);
+                            empty_bits |= spread_bits<TPK, SPL>((eb >> (my_g * TPK)) & kGroupMask, s);
+                        }
+                    }
+                }
+            }
+
+            if constexpr (OP == kOpRetrieve && L::kHasValue) {
+                /* value of the first matching slot */
+                const int fh = hit_bits ? __ffs(hit_bits) - 1 : 0;
+                const int src = my_g * TPK + fh / SPL;
+                const int s_hit = fh % SPL;
+#pragma unroll
+                for (int r = 0; r < TPK; ++r) {
+                    if (r < rounds) {
+#pragma unroll
+                        for (int s = 0; s < SPL; ++s) {
+                            const V v = shfl_any(slot_val<L>(win[r], s),
+                                                 (pending && my_round == r) ? src : lane);
+                            if (pending && my_round == r && s_hit == s) out = v;
+                        }
+                    }
+                }
+            }
+
+            if (pending) {
+                unsigned char *const bptr = slots + bucket * uint64_t(W) * SB;
+                if (hit_bits) {
+                    const int fh = __ffs(hit_bits) - 1;
+                    unsigned char *const sp = bptr + fh * SB;
+                    if constexpr (OP == kOpRetrieve) {
+                        st = kStNone;
+                        if (a.is_set) flag = true;
+                        else {
+                            if (uint64_t(out) > t.max_count) out = V(t.max_count);
+                            have_out = true;
+                        }
+                    } else if constexpr (OP == kOpInsert) {
+                        st = kStDuplicateKey;
+                        join |= kStDuplicateKey;
+                        store_value<L>(sp, val);
+                    } else if constexpr (OP == kOpCount) {
+                        st = kStDuplicateKey;
+                        join |= kStDuplicateKey;
+                        count_add<L>(sp, cnt_add, t.max_count, st, join);
+                    } else {
+                        store_key<L>(sp, tomb);
+                        st = kStNone;
+                    }
+                    pending = false;
+                } else if (empty_bits) {
+                    if constexpr (OP == kOpRetrieve) {
+                        if (a.is_set) { st = kStNone; flag = false; }
+                        else { st = kStKeyNotFound; join |= kStKeyNotFound; }
+                        pending = false;
+                    } else if constexpr (OP == kOpErase) {
+                        st = a.is_set ? kStNone : kStKeyNotFound;
+                        pending = false;
+                    } else {
+                        uint32_t e = empty_bits;
+                        while (e) {
+                            const int s = __ffs(e) - 1;
+                            e &= e - 1u;
+                            unsigned char *const sp = bptr + s * SB;
+                            K old_key;
+                            const V payload = OP == kOpCount ? V(cnt_add) : val;
+                            if (claim_slot<L>(sp, empty, key, payload, old_key)) {
+                                st = kStNone;
+                                pending = false;
+                                break;
+                            }
+                            if (old_key == key) {
+                                st = kStDuplicateKey;
+                                join |= kStDuplicateKey;
+                                if constexpr (OP == kOpInsert) store_value<L>(sp, val);
+                                else count_add<L>(sp, cnt_add, t.max_count, st, join);
+                                pending = false;
+                                break;
+                            }
+                        }
+                    }
+                }
+                if (pending) {
+                    if (++wins >= a.max_windows) {
+                        pending = false;
+                        if (OP == kOpErase) {
+                            st = a.is_set ? kStNone : kStProbingLengthExceeded;
+                        } else {
+                            st = kStProbingLengthExceeded;
+                            join |= kStProbingLengthExceeded;
+                        }
+                    } else {
+                        if (wins == 1) step = probe_step<K>(t, key);
+                        bucket = probe_next(t, bucket, step);
+                    }
+                }
+            }
+        }
+
+        if (active) {
+            if constexpr (OP == kOpRetrieve) {
+                if (a.is_set) {
+                    if (st == kStNone) reinterpret_cast<unsigned char *>(a.out)[i] = (unsigned char)flag;
+                } else if (have_out) {
+                    st_stream(reinterpret_cast<V *>(a.out) + i, out);
+                }
+            }
+            if (a.status_out) {
+                if (a.handler == kHandlerStatus)
+                    st_stream(reinterpret_cast<uint32_t *>(a.status_out) + i, st);
+                else if (a.handler == kHandlerBoolean)
+                    reinterpret_cast<unsigned char *>(a.status_out)[i] =
+                        (unsigned char)((st & a.bool_mask) != 0);
+            }
+        }
+        const uint32_t wjoin = __reduce_or_sync(kFull, join);
+        if (lane == 0) join_status(t.status, wjoin);
+    }
+}
+
+/* fill the slot array with empty slots (key = empty, payload = 0): the
+ * reference's init_keys / init_values (storage.cuh:523-562) in one pass.
+ * `pattern` is 16 bytes of slots; the array is 16-byte aligned. */
+template <int kUnused = 0>
+__global__ void __launch_bounds__(256) fill_kernel(uint32_t *p, uint64_t n_u32, uint4 pattern)
+{
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    const uint64_t tid = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    uint4 *p4 = reinterpret_cast<uint4 *>(p);
+    const uint64_t n4 = n_u32 / 4;
+    for (uint64_t i = tid; i < n4; i += stride) __stcg(p4 + i, pattern);
+    const uint32_t pw[4] = {pattern.x, pattern.y, pattern.z, pattern.w};
+    if (tid < n_u32 % 4) p[n4 * 4 + tid] = pw[tid];
+}
+
+/* size(): count slots whose key is neither empty nor tombstone
+ * (single_value_hash_table.cuh:535-592) */
+template <class L>
+__global__ void __launch_bounds__(256) count_valid_kernel(const void *slots, uint64_t capacity,
+                                                          uint64_t empty, uint64_t tomb,
+                                                          unsigned long long *count)
+{
+    using K = typename L::key_t;
+    constexpr int SB = L::kSlotBytes;
+    constexpr int SPV = 16 / SB; /* slots per 16-byte vector */
+    const uint64_t nvec = capacity / SPV;
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    unsigned long long c = 0;
+    for (uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < nvec; v += stride) {
+        const LaneWords lw = load_lane<16>(reinterpret_cast<const unsigned char *>(slots) + v * 16);
+#pragma unroll
+        for (int s = 0; s < SPV; ++s) {
+            const K k = slot_key<L>(lw, s);
+            c += (k != K(empty) && k != K(tomb));
+        }
+    }
+    /* ragged tail (capacity not a multiple of SPV) */
+    if (blockIdx.x == 0 && threadIdx.x < capacity % SPV) {
+        const uint64_t sidx = nvec * SPV + threadIdx.x;
+        const K k = *reinterpret_cast<const K *>(reinterpret_cast<const unsigned char *>(slots) + sidx * SB);
+        c += (k != K(empty) && k != K(tomb));
+    }
+    c = __reduce_add_sync(kFull, unsigned(c));
+    __shared__ unsigned long long sm[8];
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long s = 0;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) s += sm[w];
+        if (s) atomicAdd(count, s);
+    }
+}
+
+/* retrieve_all(): compact the valid slots into keys_out / values_out
+ * (single_value_hash_table.cuh:391-417); one atomic per warp */
+template <class L>
+__global__ void __launch_bounds__(256) dump_kernel(const void *slots, uint64_t capacity,
+                                                   uint64_t empty, uint64_t tomb,
+                                                   void *keys_out, void *values_out,
+                                                   unsigned long long *count)
+{
+    using K = typename L::key_t;
+    using V = typename L::val_t;
+    constexpr int SB = L::kSlotBytes;
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const uint64_t start = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t rounds = (capacity + stride - 1) / stride;
+    for (uint64_t r = 0; r < rounds; ++r) {
+        const uint64_t s = start + r * stride;
+        K k = K(empty);
+        V v = 0;
+        if (s < capacity) {
+            const unsigned char *sp = reinterpret_cast<const unsigned char *>(slots) + s * SB;
+            k = *reinterpret_cast<const K *>(sp);
+            if constexpr (L::kHasValue) v = *slot_value_ptr<L>(const_cast<unsigned char *>(sp));
+        }
+        const bool valid = s < capacity && k != K(empty) && k != K(tomb);
+        const unsigned m = __ballot_sync(kFull, valid);
+        unsigned long long base = 0;
+        if (lane == 0 && m) base = atomicAdd(count, (unsigned long long)__popc(m));
+        base = __shfl_sync(kFull, base, 0);
+        if (valid) {
+            const uint64_t o = base + __popc(m & ((1u << lane) - 1u));
+            reinterpret_cast<K *>(keys_out)[o] = k;
+            if (L::kHasValue && values_out) reinterpret_cast<V *>(values_out)[o] = v;
+        }
+    }
+}
+
+} // namespace b200
+} // namespace warpcore
+
+#endif /* WC_KERNELS_CUH */
