@@ -1,0 +1,173 @@
+/*
+ * Timing harness for the REFERENCE warpcore compiled for sm_100a (the GPU
+ * baseline that the B200 library is compared with).  Built by
+ * baseline/build_ref_gpu.sh from the reference's own headers, with the
+ * hpc_helpers stand-in of oracle/ref/, into baseline/_ref/ (git-ignored).
+ *
+ * Each entry point takes device buffers that the caller already filled,
+ * builds the reference structure with its own constructor, and times its
+ * own bulk methods with cudaEvents on the legacy default stream, as the
+ * reference's benchmark driver does (benchmark_common.cuh:116-199): the
+ * table is re-initialised untimed before every insert.  Times are the
+ * minimum over `reps`.  Return value: 0, or a CUDA error code.
+ */
+#include <warpcore/single_value_hash_table.cuh>
+#include <warpcore/hash_set.cuh>
+#include <warpcore/counting_hash_table.cuh>
+#include <warpcore/bloom_filter.cuh>
+
+#include <cfloat>
+#include <cstdint>
+
+namespace wc = warpcore;
+
+namespace {
+
+struct Timer {
+    cudaEvent_t a, b;
+    Timer() { cudaEventCreate(&a); cudaEventCreate(&b); }
+    ~Timer() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    void start() { cudaEventRecord(a, 0); }
+    float stop()
+    {
+        cudaEventRecord(b, 0);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        return ms;
+    }
+};
+
+template <class Set>
+__global__ void set_contains(const typename Set::key_type *keys, uint64_t n, bool *flags, Set s)
+{
+    namespace cg = cooperative_groups;
+    const uint64_t tid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    const uint64_t gid = tid / Set::cg_size();
+    const auto group = cg::tiled_partition<Set::cg_size()>(cg::this_thread_block());
+    if (gid < n) {
+        bool f = false;
+        const wc::Status st = s.retrieve(keys[gid], f, group);
+        if (group.thread_rank() == 0 && !st.has_any()) flags[gid] = f;
+    }
+}
+
+template <class Table, class K, class V>
+int run_table(const K *keys, const V *vals, uint64_t n, const K *q, uint64_t nq, V *out,
+              uint64_t min_cap, int reps, float *ms_insert, float *ms_retrieve,
+              uint64_t *capacity)
+{
+    Table t(min_cap);
+    *capacity = t.capacity();
+    Timer tm;
+    float bi = FLT_MAX, br = FLT_MAX;
+    for (int r = 0; r < reps; ++r) {
+        t.init();
+        cudaDeviceSynchronize();
+        tm.start();
+        t.insert(keys, vals, n);
+        bi = fminf(bi, tm.stop());
+        tm.start();
+        t.retrieve(q, nq, out);
+        br = fminf(br, tm.stop());
+    }
+    *ms_insert = bi;
+    *ms_retrieve = br;
+    return int(cudaDeviceSynchronize());
+}
+
+} // namespace
+
+extern "C" {
+
+int ref_svht64_run(const uint64_t *keys, const uint64_t *vals, uint64_t n, const uint64_t *q,
+                   uint64_t nq, uint64_t *out, uint64_t min_cap, int reps, float *ms_insert,
+                   float *ms_retrieve, uint64_t *capacity)
+{
+    return run_table<wc::SingleValueHashTable<uint64_t, uint64_t>>(
+        keys, vals, n, q, nq, out, min_cap, reps, ms_insert, ms_retrieve, capacity);
+}
+
+int ref_svht32_run(const uint32_t *keys, const uint32_t *vals, uint64_t n, const uint32_t *q,
+                   uint64_t nq, uint32_t *out, uint64_t min_cap, int reps, float *ms_insert,
+                   float *ms_retrieve, uint64_t *capacity)
+{
+    return run_table<wc::SingleValueHashTable<uint32_t, uint32_t>>(
+        keys, vals, n, q, nq, out, min_cap, reps, ms_insert, ms_retrieve, capacity);
+}
+
+/* HashSet<u64>: the host bulk retrieve does not compile (hash_set.cuh:356),
+ * so contains runs the device method from this harness's own kernel */
+int ref_hashset64_run(const uint64_t *keys, uint64_t n, const uint64_t *q, uint64_t nq,
+                      bool *flags, uint64_t min_cap, int reps, float *ms_insert,
+                      float *ms_retrieve, uint64_t *capacity)
+{
+    using Set = wc::HashSet<uint64_t>;
+    Set s(min_cap);
+    *capacity = s.capacity();
+    Timer tm;
+    float bi = FLT_MAX, br = FLT_MAX;
+    for (int r = 0; r < reps; ++r) {
+        s.init();
+        cudaDeviceSynchronize();
+        tm.start();
+        s.insert(keys, n);
+        bi = fminf(bi, tm.stop());
+        tm.start();
+        const uint64_t threads = nq * Set::cg_size();
+        set_contains<Set><<<(threads + 1023) / 1024, 1024>>>(q, nq, flags, s);
+        br = fminf(br, tm.stop());
+    }
+    *ms_insert = bi;
+    *ms_retrieve = br;
+    return int(cudaDeviceSynchronize());
+}
+
+int ref_counting32_run(const uint32_t *keys, uint64_t n, const uint32_t *q, uint64_t nq,
+                       uint32_t *out, uint64_t min_cap, int reps, float *ms_insert,
+                       float *ms_retrieve, uint64_t *capacity)
+{
+    using Table = wc::CountingHashTable<uint32_t, uint32_t>;
+    Table t(min_cap);
+    *capacity = t.capacity();
+    Timer tm;
+    float bi = FLT_MAX, br = FLT_MAX;
+    for (int r = 0; r < reps; ++r) {
+        t.init();
+        cudaDeviceSynchronize();
+        tm.start();
+        t.insert(keys, n);
+        bi = fminf(bi, tm.stop());
+        tm.start();
+        t.retrieve(q, nq, out);
+        br = fminf(br, tm.stop());
+    }
+    *ms_insert = bi;
+    *ms_retrieve = br;
+    return int(cudaDeviceSynchronize());
+}
+
+int ref_bloom64_run(const uint64_t *keys, uint64_t n, const uint64_t *q, uint64_t nq,
+                    bool *flags, uint64_t num_bits, uint64_t k, int reps, float *ms_insert,
+                    float *ms_retrieve)
+{
+    using Filter = wc::BloomFilter<uint64_t, wc::hashers::MurmurHash<uint64_t>, uint64_t, 8>;
+    Filter f(num_bits, k);
+    Timer tm;
+    float bi = FLT_MAX, br = FLT_MAX;
+    for (int r = 0; r < reps; ++r) {
+        f.init();
+        cudaDeviceSynchronize();
+        tm.start();
+        f.insert(keys, n);
+        bi = fminf(bi, tm.stop());
+        tm.start();
+        f.retrieve(q, nq, flags);
+        br = fminf(br, tm.stop());
+    }
+    *ms_insert = bi;
+    *ms_retrieve = br;
+    return int(cudaDeviceSynchronize());
+}
+
+} // extern "C"

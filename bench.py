@@ -263,6 +263,22 @@ class Workload:
     def retrieve(self, stream):
         self.table.retrieve(self.queries, self.out, stream=stream)
 
+    def answers_ok(self, out):
+        """the retrieve output `out` (written by any implementation after an
+        insert of this workload) holds the right answers"""
+        import torch
+        if self.kind in ("svht32", "svht64"):
+            return bool(torch.equal(out[self.hit], self.expected[self.hit]))
+        if self.kind == "hashset64":
+            return bool((out == self.hit.to(torch.uint8)).all())
+        if self.kind == "counting32":
+            got = out[: self.distinct].to(torch.int64)
+            present = self.hist > 0
+            return bool(torch.equal(got[present], self.hist[present]))
+        if self.kind == "bloom64":
+            return bool(out[self.n:].all())
+        return False
+
     def verify(self):
         """size-independent properties of one fresh step"""
         import torch
@@ -320,12 +336,66 @@ def zipf_ranks_t(n_in, s, n_out, gen, device):
     return out
 
 
+def reference_gpu(wl, reps=5):
+    """Time the reference warpcore compiled for sm_100a
+    (baseline/_ref/libwarpcore_ref_bench.so, built by
+    baseline/build_ref_gpu.sh) on the same resident inputs, with the
+    reference's own bulk methods: min over `reps`, table re-initialised
+    untimed before each insert (benchmark_common.cuh:116-199)."""
+    import ctypes
+    import torch
+    path = os.path.join(ROOT, "baseline", "_ref", "libwarpcore_ref_bench.so")
+    if not os.path.exists(path):
+        return None
+    lib = ctypes.CDLL(path)
+    f32 = ctypes.c_float
+    ti, tr, cap = f32(), f32(), ctypes.c_uint64(0)
+    u64 = ctypes.c_uint64
+    vp = ctypes.c_void_p
+    torch.cuda.synchronize()
+    out = torch.empty_like(wl.out)
+    min_cap = int(wl.n / wl.load) if wl.kind != "counting32" else int(wl.distinct / wl.load)
+    if wl.kind in ("svht64", "svht32"):
+        fn = lib.ref_svht64_run if wl.kind == "svht64" else lib.ref_svht32_run
+        rc = fn(vp(wl.keys.data_ptr()), vp(wl.values.data_ptr()), u64(wl.n),
+                vp(wl.queries.data_ptr()), u64(wl.q), vp(out.data_ptr()), u64(min_cap),
+                ctypes.c_int(reps), ctypes.byref(ti), ctypes.byref(tr), ctypes.byref(cap))
+    elif wl.kind == "hashset64":
+        rc = lib.ref_hashset64_run(vp(wl.keys.data_ptr()), u64(wl.n), vp(wl.queries.data_ptr()),
+                                   u64(wl.q), vp(out.data_ptr()), u64(min_cap), ctypes.c_int(reps),
+                                   ctypes.byref(ti), ctypes.byref(tr), ctypes.byref(cap))
+    elif wl.kind == "counting32":
+        out.zero_()
+        rc = lib.ref_counting32_run(vp(wl.keys.data_ptr()), u64(wl.n), vp(wl.queries.data_ptr()),
+                                    u64(wl.q), vp(out.data_ptr()), u64(min_cap), ctypes.c_int(reps),
+                                    ctypes.byref(ti), ctypes.byref(tr), ctypes.byref(cap))
+    elif wl.kind == "bloom64":
+        rc = lib.ref_bloom64_run(vp(wl.keys.data_ptr()), u64(wl.n), vp(wl.queries.data_ptr()),
+                                 u64(wl.q), vp(out.data_ptr()), u64(16 * wl.n), u64(8),
+                                 ctypes.c_int(reps), ctypes.byref(ti), ctypes.byref(tr))
+    else:
+        return None
+    torch.cuda.synchronize()
+    if rc != 0:
+        return {"error": "CUDA error %d" % rc}
+    # the reference's answers on the same inputs must equal ours
+    same = wl.answers_ok(out)
+    ins_g = wl.n / (ti.value * 1e-3) / 1e9
+    ret_g = wl.q / (tr.value * 1e-3) / 1e9
+    return {"insert_gops": round(ins_g, 4), "retrieve_gops": round(ret_g, 4),
+            "value": round((wl.n + wl.q) / ((ti.value + tr.value) * 1e-3) / 1e9, 4),
+            "insert_ms": round(ti.value, 4), "retrieve_ms": round(tr.value, 4),
+            "capacity": int(cap.value) if cap.value else None, "reps": reps,
+            "timing": "cudaEvent min of %d on the reference's own bulk methods" % reps,
+            "same_answers": same}
+
+
 WORKLOAD_NAMES = {
     "svht64": "SingleValueHashTable<u64,u64> CG8 LF0.9: insert 2^{L} + retrieve 2^{L} (50% hit)",
     "svht32": "SingleValueHashTable<u32,u32> CG8: insert 2^{L} + retrieve 2^{L} (50% hit)",
     "hashset64": "HashSet<u64> CG16 LF0.9: insert 2^{L} + contains 2^{L} (50% hit)",
     "counting32": "CountingHashTable<u32,u32> CG4 LF0.85: insert 2^{L} Zipf(1.1) + retrieve distinct+absent",
-    "bloom64": "BloomFilter<u64,Murmur64,u64,CG8> 16 bits/key k=8: insert 2^{L} + query 2^{L+1}",
+    "bloom64": "BloomFilter<u64,Murmur64,u64,CG8> 16 bits/key k=8: insert 2^{L} + query 2^{L1}",
 }
 
 
@@ -403,6 +473,7 @@ def run_ours(args):
 
     # end to end through the public API with host buffers
     e2e = run_e2e(wl, stream, args, world) if not args.no_e2e else None
+    ref_gpu = reference_gpu(wl) if (rank == 0 and not args.no_ref_gpu) else None
 
     if world > 1:
         dist.barrier()
@@ -432,7 +503,7 @@ def run_ours(args):
             "dtype": "u64" if wl.kb == 8 else "u32",
             "data": "synthetic (seeded uniform unique keys, uniform values; inputs resident in HBM)",
             "config": {
-                "workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n),
+                "workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n, L1=args.log2n + 1),
                 "capacity": int(wl.table.capacity) if hasattr(wl.table, "capacity") else None,
                 "ops_per_step": ops_step,
                 "l2": "inputs larger than L2 (no flush)" if args.log2n >= 24 else "inputs may be L2-resident",
@@ -456,6 +527,7 @@ def run_ours(args):
                 "traffic": traffic,
             },
             "cpu_baseline": cpu,
+            "reference_gpu_build": ref_gpu,
             "e2e": e2e,
             "gpu_launches": 3 * args.steps,
             "clocks": clocks,
@@ -583,7 +655,7 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "u64" if args.workload not in ("svht32", "counting32") else "u32",
         "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n),
+        "config": {"workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n, L1=args.log2n + 1),
                    "sample": "2^%d keys per step on the host" % args.cpu_log2n},
         "cpu_baseline": {"value": round(value, 5), "unit": "Gops/s", "cores": threads,
                          "kind": "port",
@@ -608,6 +680,7 @@ def main():
     ap.add_argument("--cpu-log2n", type=int, default=24)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warm-up raised to 3 steps")

@@ -321,6 +321,39 @@ __device__ __forceinline__ bool claim_slot(void *sp, typename L::key_t empty,
     }
 }
 
+/* One compare-and-swap attempt on slot sp, expecting an empty slot with
+ * payload `expect_payload` and installing key with payload v.  Returns the
+ * key found in the slot before the attempt (the attempt succeeded iff that
+ * key is `empty` and *old_payload == expect_payload). */
+template <class L>
+__device__ __forceinline__ typename L::key_t cas_slot(void *sp, typename L::key_t empty,
+                                                      typename L::val_t expect_payload,
+                                                      typename L::key_t key,
+                                                      typename L::val_t v,
+                                                      typename L::val_t *old_payload)
+{
+    if constexpr (L::kSlotBytes == 4) {
+        *old_payload = expect_payload;
+        return atomicCAS(reinterpret_cast<unsigned int *>(sp), empty, key);
+    } else if constexpr (L::kSlotBytes == 8 && !L::kHasValue) {
+        *old_payload = expect_payload;
+        return atomicCAS(reinterpret_cast<unsigned long long *>(sp), (unsigned long long)empty,
+                         (unsigned long long)key);
+    } else if constexpr (L::kSlotBytes == 8) {
+        const unsigned long long old = atomicCAS(
+            reinterpret_cast<unsigned long long *>(sp),
+            (unsigned long long)empty | ((unsigned long long)expect_payload << 32),
+            (unsigned long long)key | ((unsigned long long)v << 32));
+        *old_payload = uint32_t(old >> 32);
+        return uint32_t(old);
+    } else {
+        uint64_t olo, ohi;
+        cas128(sp, empty, expect_payload, key, v, olo, ohi);
+        *old_payload = ohi;
+        return olo;
+    }
+}
+
 template <class L>
 __device__ __forceinline__ typename L::val_t *slot_value_ptr(void *sp)
 {

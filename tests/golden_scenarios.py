@@ -1,0 +1,109 @@
+"""Replays the scenarios of oracle/ref/make_golden.cu (which ran the
+reference's CUDA code on a B200 and recorded its outputs in
+tests/golden/ref_gpu) on any implementation with the oracle's interface, and
+compares every output with the recorded one."""
+import numpy as np
+
+from oracle import oracle as o
+
+SENT64 = 0xA5A5A5A5A5A5A5A5
+
+
+def _dt(kb):
+    return np.uint32 if kb == 4 else np.uint64
+
+
+def svht_scenario(F, tag, kb, make_table):
+    """make_table(min_cap) -> object with insert/retrieve/erase/size/
+    pop_status like oracle.Table"""
+    n, min_cap, kseed, cap, size1, size2, size3, s1, s2, s3, s4, s5 = F[tag + "_meta"].tolist()
+    allk = o.gen_unique_keys(kb, 2 * n, kseed)
+    keys = allk[:n]
+    vals = o.gen_uniform(kb, n, kseed + 1)
+    nd = n // 8
+    km = (1 << (8 * kb)) - 1
+    k2 = np.concatenate([keys[:nd], np.array([0, km], dtype=_dt(kb))])
+    v2 = np.concatenate([o.gen_uniform(kb, nd, kseed + 2), np.array([1, 2], dtype=_dt(kb))])
+    q = np.empty(2 * n, dtype=_dt(kb))
+    q[0::2] = keys
+    q[1::2] = allk[n:]
+    er = np.concatenate([keys[::5], allk[n:n + 16]])
+    fill = np.full(2 * n, SENT64 & km, dtype=_dt(kb))
+
+    t = make_table(min_cap)
+    assert t.capacity == cap
+    assert np.array_equal(t.insert(keys, vals, want_status=True), F[tag + "_insert_status"])
+    assert t.size() == size1
+    assert t.pop_status() == s1
+    assert np.array_equal(t.insert(k2, v2, want_status=True), F[tag + "_insert2_status"])
+    assert t.size() == size2
+    assert t.pop_status() == s2
+    out, st = t.retrieve(q, fill.copy(), want_status=True)
+    assert np.array_equal(out, F[tag + "_retrieve1_values"])
+    assert np.array_equal(st, F[tag + "_retrieve1_status"])
+    assert t.pop_status() == s3
+    assert np.array_equal(t.erase(er, want_status=True), F[tag + "_erase_status"])
+    assert t.size() == size3
+    assert t.pop_status() == s4
+    out, st = t.retrieve(q, fill.copy(), want_status=True)
+    assert np.array_equal(out, F[tag + "_retrieve2_values"])
+    assert np.array_equal(st, F[tag + "_retrieve2_status"])
+    assert t.pop_status() == s5
+
+
+def set_scenario(F, tag, kb, make_set):
+    n, min_cap, kseed, cap, size1, size3, s1, s2, s3 = F[tag + "_meta"].tolist()
+    allk = o.gen_unique_keys(kb, 2 * n, kseed)
+    keys = allk[:n]
+    k2 = np.concatenate([keys[: n // 8], np.array([0], dtype=_dt(kb))])
+    q = np.empty(2 * n, dtype=_dt(kb))
+    q[0::2] = keys
+    q[1::2] = allk[n:]
+    er = keys[::5]
+    s = make_set(min_cap)
+    assert s.capacity == cap
+    assert np.array_equal(s.insert(keys, want_status=True), F[tag + "_insert_status"])
+    assert s.size() == size1
+    assert s.pop_status() == s1
+    assert np.array_equal(s.insert(k2, want_status=True), F[tag + "_insert2_status"])
+    assert s.pop_status() == s2
+    f, st = s.retrieve(q, np.full(2 * n, 7, dtype=np.uint8), want_status=True)
+    assert np.array_equal(f, F[tag + "_contains1"])
+    assert np.array_equal(st, F[tag + "_contains1_status"])
+    assert np.array_equal(s.erase(er, want_status=True), F[tag + "_erase_status"])
+    assert s.size() == size3
+    f, st = s.retrieve(q, np.full(2 * n, 7, dtype=np.uint8), want_status=True)
+    assert np.array_equal(f, F[tag + "_contains2"])
+    assert np.array_equal(st, F[tag + "_contains2_status"])
+    assert s.pop_status() == s3
+
+
+def counting_scenario(F, tag, make_counter):
+    distinct, occ, min_cap, max_count, kseed, cap, size1, s1 = F[tag + "_meta"].tolist()
+    allk = o.gen_unique_keys(4, distinct + distinct // 4, kseed)
+    ranks = o.gen_zipf_ranks(distinct, 1.1, occ, kseed + 3)
+    keys = allk[(ranks - 1).astype(np.int64)]
+    c = make_counter(min_cap, max_count)
+    assert c.capacity == cap
+    c.insert(keys)
+    assert c.pop_status() == s1
+    out, st = c.retrieve(allk, np.full(allk.size, 0xA5A5A5A5, dtype=np.uint32), want_status=True)
+    assert np.array_equal(out, F[tag + "_counts"])
+    assert np.array_equal(st, F[tag + "_status"])
+    assert c.size() == size1
+
+
+def bloom_scenario(F, tag, make_bloom):
+    kb, sb, cg, num_bits, k, n, kseed, num_slots, num_blocks = F[tag + "_meta"].tolist()
+    allk = o.gen_unique_keys(kb, 2 * n, kseed)
+    b = make_bloom(kb, sb, cg, num_bits, k)
+    assert (b.num_slots, b.num_blocks) == (num_slots, num_blocks)
+    b.insert(allk[:n])
+    assert np.array_equal(b.words(), F[tag + "_words"])
+    assert np.array_equal(b.retrieve(allk), F[tag + "_flags"])
+
+
+SVHT_CASES = [("svht_u32u32", 4), ("svht_u64u64", 8)]
+SET_CASES = [("set_u64", 8), ("set_u32", 4)]
+COUNT_CASES = ["count_u32", "count_u32_max10"]
+BLOOM_CASES = ["bloom_u64_s64_cg8", "bloom_u64_s64_cg1", "bloom_u32_s32_cg4", "bloom_u32_s64_cg2"]

@@ -28,7 +28,8 @@ __all__ = [
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libwarpcore_b200.so")
+# WARPCORE_B200_LIB may point at another build of the same library
+LIB_PATH = os.environ.get("WARPCORE_B200_LIB") or os.path.join(_HERE, "libwarpcore_b200.so")
 
 HASH_MURMUR, HASH_NVIDIA, HASH_MUELLER, HASH_IDENTITY32, HASH_IDENTITY64 = range(5)
 PROBING_DOUBLE, PROBING_LINEAR, PROBING_QUADRATIC = range(3)
