@@ -264,6 +264,32 @@ int wc_bloom_get_info(const wc_bloom *b, wc_bloom_info *info);
 /* fpr(n) (bloom_filter.cuh:342-354), the reference's own formula */
 int wc_bloom_fpr(const wc_bloom *b, uint64_t n, double *out);
 
+/* ------------------------------------------------------------------ */
+/* Counting without allocating                                          */
+/* ------------------------------------------------------------------ */
+
+/* Largest slot array wc_slots_size_noalloc accepts (2^34 slots). */
+#define WC_NOALLOC_MAX_SLOTS (1ull << 34)
+
+/* No counterpart in the reference.  Counts the occupied slots (key neither
+ * empty_key nor tombstone_key) of a slot array in this library's layout
+ * (key_bytes 4 or 8; value_bytes 0 for a hash set, else equal to key_bytes)
+ * and writes the count to *size_out, a DEVICE pointer to one uint64, on
+ * `stream`, without allocating any device memory.  It is meant for callers
+ * that hold a table's slots without a handle of this library and may not
+ * allocate: e.g. a process that received the table's memory through CUDA
+ * IPC, or a plugin whose host framework owns all device memory.  Scratch is
+ * a fixed 512 KiB array inside the library (held by every GPU that loads
+ * it); slot arrays above WC_NOALLOC_MAX_SLOTS are rejected with
+ * WC_ERR_INVALID_ARGUMENT.  All calls share that array, so calls that
+ * overlap on the GPU race; the first call on each device resolves the
+ * array's address and should come before any stream capture.  `slots` must
+ * be 16-byte aligned (wc_table_get_info's `slots` is). */
+int wc_slots_size_noalloc(const void *slots, uint64_t capacity, uint32_t key_bytes,
+                          uint32_t value_bytes, uint64_t empty_key,
+                          uint64_t tombstone_key, wc_stream_t stream,
+                          uint64_t *size_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -144,6 +144,7 @@ SIGNATURES = {
     "wc_bloom_retrieve": (_i, [_vp, _vp, _u64, _vp, _vp]),
     "wc_bloom_get_info": (_i, [_vp, ctypes.POINTER(BloomInfo)]),
     "wc_bloom_fpr": (_i, [_vp, _u64, ctypes.POINTER(ctypes.c_double)]),
+    "wc_slots_size_noalloc": (_i, [_vp, _u64, _u32, _u32, _u64, _u64, _vp, _vp]),
 }
 
 _lib = None

@@ -137,6 +137,8 @@ constexpr int kBlock = 256;
 
 } // namespace
 
+void warpcore::b200::set_last_error(const char *msg) { g_last_error = msg; }
+
 /* ------------------------------------------------------------------ */
 /* handles                                                              */
 /* ------------------------------------------------------------------ */

@@ -29,6 +29,9 @@ DumpKernel dump_kernel_ptr(int layout);
 
 BloomKernel bloom_kernel_ptr(int key_bytes, int slot_bytes, int cg, bool insert);
 
+/* message returned by wc_last_error() on the calling thread */
+void set_last_error(const char *msg);
+
 } // namespace b200
 } // namespace warpcore
 
