@@ -129,6 +129,29 @@ __host__ __device__ __forceinline__ uint64_t mod_u64(uint64_t x, uint64_t m)
     return x % m;
 }
 
+/* x % d by Barrett reduction with m = floor((2^64 - 1) / d): the estimate
+ * q = mulhi(x, m) is floor(x / d) or one less for every 64-bit x, so one
+ * conditional subtraction makes the remainder exact. */
+__host__ __device__ __forceinline__ uint64_t barrett_magic(uint64_t d)
+{
+    return d ? ~0ull / d : 0;
+}
+
+__host__ __device__ __forceinline__ uint64_t mulhi64(uint64_t a, uint64_t b)
+{
+#ifdef __CUDA_ARCH__
+    return __umul64hi(a, b);
+#else
+    return uint64_t((unsigned __int128)a * b >> 64);
+#endif
+}
+
+__host__ __device__ __forceinline__ uint64_t fast_mod(uint64_t x, uint64_t d, uint64_t magic)
+{
+    uint64_t r = x - mulhi64(x, magic) * d;
+    return r >= d ? r - d : r;
+}
+
 /* ------------------------------------------------------------------ */
 /* table view and bucket probing                                        */
 /* ------------------------------------------------------------------ */
@@ -141,6 +164,8 @@ struct TableView {
     uint64_t empty_key;
     uint64_t tombstone_key;
     uint64_t max_count;
+    uint64_t magic_nb;   /* barrett_magic(num_buckets) */
+    uint64_t magic_nb1;  /* barrett_magic(num_buckets - 1) */
     uint32_t probing, hasher1, hasher2, cg_size;
 };
 
@@ -148,7 +173,7 @@ template <class K>
 __host__ __device__ __forceinline__ uint64_t probe_begin(const TableView &t, K key)
 {
     const K k = K(key + K(t.seed));
-    return mod_u64(hash_key<K>(t.hasher1, k), t.num_buckets);
+    return fast_mod(hash_key<K>(t.hasher1, k), t.num_buckets, t.magic_nb);
 }
 
 template <class K>
@@ -156,7 +181,7 @@ __host__ __device__ __forceinline__ uint64_t probe_step(const TableView &t, K ke
 {
     if (t.probing != kProbeDouble || t.num_buckets < 2) return 1;
     const K k = K(key + K(t.seed) + K(1));
-    return mod_u64(hash_key<K>(t.hasher2, k), t.num_buckets - 1) + 1;
+    return fast_mod(hash_key<K>(t.hasher2, k), t.num_buckets - 1, t.magic_nb1) + 1;
 }
 
 /* advance to the next bucket; `step` grows by one per window for
@@ -166,7 +191,7 @@ __host__ __device__ __forceinline__ uint64_t probe_next(const TableView &t,
                                                         uint64_t &step)
 {
     uint64_t s = step;
-    if (s >= t.num_buckets) s = mod_u64(s, t.num_buckets);
+    if (s >= t.num_buckets) s = fast_mod(s, t.num_buckets, t.magic_nb);
     b += s;
     if (b >= t.num_buckets) b -= t.num_buckets;
     if (t.probing == kProbeQuadratic) step++;

@@ -27,6 +27,7 @@ struct BloomArgs {
     uint64_t n;
     uint64_t num_slots;
     uint64_t num_blocks;
+    uint64_t magic_blocks; /* barrett_magic(num_blocks) */
     uint64_t k;
     uint64_t seed;
     uint32_t hasher;
@@ -74,7 +75,7 @@ __global__ void __launch_bounds__(256) bloom_kernel(const BloomArgs a)
         const uint64_t i = base + lane;
         const bool active = i < a.n;
         const K key = active ? ld_stream(keys + i) : K(0);
-        const uint64_t blk = mod_u64(hash_key<K>(a.hasher, K(key + seed)), a.num_blocks);
+        const uint64_t blk = fast_mod(hash_key<K>(a.hasher, K(key + seed)), a.num_blocks, a.magic_blocks);
 
         LaneWords win[TPK];
         bool own_ok[TPK];
@@ -125,8 +126,11 @@ __global__ void __launch_bounds__(256) bloom_kernel(const BloomArgs a)
                 const S w = lane_word<S>(win[r], s);
                 const bool missing = (w & mask[s]) != mask[s];
                 ok &= !missing;
-                if (INSERT && own_ok[r] && missing)
-                    atomic_or_any(words + (b * CG + uint64_t(q) * SPL + s) % a.num_slots, mask[s]);
+                if (INSERT && own_ok[r] && missing) {
+                    uint64_t wi = b * CG + uint64_t(q) * SPL + s;
+                    if (wi >= a.num_slots) wi -= a.num_slots; /* ragged last block */
+                    atomic_or_any(words + wi, mask[s]);
+                }
             }
             if constexpr (!INSERT) {
                 const unsigned bad = __ballot_sync(kFull, !ok);

@@ -183,6 +183,8 @@ TableView view_of(const wc_table *t)
     v.empty_key = t->cfg.empty_key;
     v.tombstone_key = t->cfg.tombstone_key;
     v.max_count = t->max_count;
+    v.magic_nb = barrett_magic(t->num_buckets);
+    v.magic_nb1 = barrett_magic(t->num_buckets > 1 ? t->num_buckets - 1 : 1);
     v.probing = t->cfg.probing;
     v.hasher1 = t->cfg.hasher1;
     v.hasher2 = t->cfg.hasher2;
@@ -690,6 +692,7 @@ static int bloom_op(wc_bloom *b, const void *keys, uint64_t n, uint8_t *flags, w
     a.n = n;
     a.num_slots = b->num_slots;
     a.num_blocks = b->num_blocks;
+    a.magic_blocks = barrett_magic(b->num_blocks);
     a.k = b->k;
     a.seed = b->seed;
     a.hasher = b->cfg.hasher;

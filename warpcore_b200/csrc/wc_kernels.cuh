@@ -89,6 +89,10 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
     const unsigned lanemask_lt = (1u << lane) - 1u;
     const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    const int wib = threadIdx.x >> 5;
+    __shared__ uint64_t sh_bucket[8][32];
+    __shared__ K sh_key[8][32];
+    __shared__ uint32_t sh_off[8][32];
 
     /* this warp's contiguous range of keys */
     uint64_t per = (a.n + nwarps - 1) / nwarps;
@@ -117,12 +121,12 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
     /* state of the key this lane owns; a pending key either waits for its
      * window (claiming == false) or for a compare-and-swap on the lowest
      * slot of claim_bits, the free slots its last window showed */
-    bool has = false, pending = false, flag = false, have_out = false, claiming = false;
+    bool has = false, pending = false, flag = false, claiming = false;
     uint32_t claim_bits = 0;
     V claim_expect = 0;
     uint64_t i = 0, bucket = 0, step = 0, wins = 0;
     K key = empty;
-    V val = 0, out = 0;
+    V val = 0;
     uint32_t st = kStNone, join = 0, cnt_add = 1;
 
     for (;;) {
@@ -148,8 +152,6 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
             has = true;
             pending = true;
             flag = false;
-            have_out = false;
-            out = 0;
             st = kStNone;
             cnt_add = 1;
             wins = 0;
@@ -213,20 +215,27 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
             const int my_round = my_rank / G;
             const int my_g = my_rank % G;
 
+            /* owners publish (bucket, key, index) in rank order; group g of
+             * round rr then serves the owner of rank rr * G + g */
+            __syncwarp();
+            if (loading) {
+                sh_bucket[wib][my_rank] = bucket;
+                sh_key[wib][my_rank] = key;
+                sh_off[wib][my_rank] = uint32_t(i - wb);
+            }
+            __syncwarp();
+
             LaneWords win[TPK];
-            int own[TPK];
 #pragma unroll
             for (int rr = 0; rr < TPK; ++rr) {
-                own[rr] = -1;
                 if (rr < rounds) {
                     const int idx = rr * G + g;
-                    const int o = idx < cnt ? nth_set_bit(pmask, idx) : -1;
-                    own[rr] = o;
-                    const uint64_t b = shfl_any(bucket, o < 0 ? lane : o);
-                    if (o >= 0)
+                    if (idx < cnt) {
+                        const uint64_t b = sh_bucket[wib][idx];
                         win[rr] = load_lane<LB>(slots + (b * W + uint64_t(q) * SPL) * SB);
-                    else
+                    } else {
                         win[rr] = LaneWords{{0u, 0u, 0u, 0u}};
+                    }
                 }
             }
 
@@ -244,33 +253,27 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
 #pragma unroll
             for (int rr = 0; rr < TPK; ++rr) {
                 if (rr < rounds) {
-                    const K kr = shfl_any(key, own[rr] < 0 ? lane : own[rr]);
+                    const int idx = rr * G + g;
+                    const bool served = idx < cnt;
+                    const K kr = served ? sh_key[wib][idx] : empty;
 #pragma unroll
                     for (int s = 0; s < SPL; ++s) {
                         const K sk = slot_key<L>(win[rr], s);
-                        const unsigned hb = __ballot_sync(kFull, own[rr] >= 0 && sk == kr);
-                        const unsigned eb = __ballot_sync(kFull, own[rr] >= 0 && sk == empty);
+                        const bool h = served && sk == kr;
+                        const unsigned hb = __ballot_sync(kFull, h);
+                        const unsigned eb = __ballot_sync(kFull, served && sk == empty);
                         if (loading && my_round == rr) {
                             hit_bits |= spread_bits<TPK, SPL>((hb >> (my_g * TPK)) & kGroupMask, s);
                             empty_bits |= spread_bits<TPK, SPL>((eb >> (my_g * TPK)) & kGroupMask, s);
                         }
-                    }
-                }
-            }
-
-            if constexpr (OP == kOpRetrieve && L::kHasValue) {
-                /* value of the first matching slot, from the lane that holds it */
-                const int fh = hit_bits ? __ffs(hit_bits) - 1 : 0;
-                const int src = my_g * TPK + fh / SPL;
-                const int s_hit = fh % SPL;
-#pragma unroll
-                for (int rr = 0; rr < TPK; ++rr) {
-                    if (rr < rounds) {
-#pragma unroll
-                        for (int s = 0; s < SPL; ++s) {
-                            const bool mine = loading && my_round == rr;
-                            const V v = shfl_any(slot_val<L>(win[rr], s), mine ? src : lane);
-                            if (mine && s_hit == s) out = v;
+                        if constexpr (OP == kOpRetrieve && L::kHasValue) {
+                            /* a key occupies at most one slot, so the lane
+                             * that sees it writes the value itself */
+                            if (h && !a.is_set) {
+                                V v = slot_val<L>(win[rr], s);
+                                if (uint64_t(v) > t.max_count) v = V(t.max_count);
+                                st_stream(reinterpret_cast<V *>(a.out) + wb + sh_off[wib][idx], v);
+                            }
                         }
                     }
                 }
@@ -284,12 +287,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
                     unsigned char *const sp = bptr + fh * SB;
                     if constexpr (OP == kOpRetrieve) {
                         st = kStNone;
-                        if (a.is_set) {
-                            flag = true;
-                        } else {
-                            if (uint64_t(out) > t.max_count) out = V(t.max_count);
-                            have_out = true;
-                        }
+                        flag = true;
                     } else if constexpr (OP == kOpInsert) {
                         st = kStDuplicateKey;
                         join |= kStDuplicateKey;
@@ -370,11 +368,8 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
         /* ---- keys that finished this wave write their results ---- */
         if (has && !pending) {
             if constexpr (OP == kOpRetrieve) {
-                if (a.is_set) {
-                    if (st == kStNone) reinterpret_cast<unsigned char *>(a.out)[i] = (unsigned char)flag;
-                } else if (have_out) {
-                    st_stream(reinterpret_cast<V *>(a.out) + i, out);
-                }
+                if (a.is_set && st == kStNone)
+                    reinterpret_cast<unsigned char *>(a.out)[i] = (unsigned char)flag;
             }
             if (a.status_out) {
                 if (a.handler == kHandlerStatus)
