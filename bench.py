@@ -59,7 +59,7 @@ def profile_traffic(name):
         return None
     for line in open(p):
         f = line.split()
-        if len(f) == 3 and f[0] == "dram_bytes_per_launch" and f[1] == name:
+        if len(f) >= 3 and f[0] == "dram_bytes_per_launch" and f[1] == name:
             return float(f[2])
     return None
 

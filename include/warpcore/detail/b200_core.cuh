@@ -382,7 +382,7 @@ __device__ __forceinline__ typename L::key_t cas_slot(void *sp, typename L::key_
 template <class L>
 __device__ __forceinline__ typename L::val_t *slot_value_ptr(void *sp)
 {
-    if constexpr (L::kSlotBytes == 8)
+    if constexpr (L::kSlotBytes == 8 && L::kHasValue)
         return reinterpret_cast<uint32_t *>(sp) + 1;
     else
         return reinterpret_cast<typename L::val_t *>(reinterpret_cast<uint64_t *>(sp) + 1);
