@@ -265,6 +265,96 @@ int wc_bloom_get_info(const wc_bloom *b, wc_bloom_info *info);
 int wc_bloom_fpr(const wc_bloom *b, uint64_t n, double *out);
 
 /* ------------------------------------------------------------------ */
+/* Batches: many requests on many tables in one launch                  */
+/* (no counterpart in the reference, which launches one kernel per bulk */
+/* call, single_value_hash_table.cuh:241-337)                            */
+/* ------------------------------------------------------------------ */
+
+#define WC_OP_INSERT 0
+#define WC_OP_RETRIEVE 2
+
+/* One request of a batch: the arguments of wc_svht_insert or
+ * wc_svht_retrieve for one single-value table. */
+typedef struct wc_batch_request {
+    wc_table *table;
+    int op;               /* WC_OP_INSERT or WC_OP_RETRIEVE */
+    int status_handler;   /* WC_HANDLER_* */
+    uint32_t ignore;      /* ReturnBoolean's Ignore */
+    uint32_t reserved;
+    const void *keys;     /* device, num keys */
+    const void *values;   /* device, insert only */
+    void *values_out;     /* device, retrieve only (written on hits) */
+    void *status_out;     /* device or NULL */
+    uint64_t num;
+} wc_batch_request;
+
+typedef struct wc_batch wc_batch;
+
+/* A batch runner for up to max_requests requests per run.  It owns pinned
+ * and device staging for `depth` runs in flight and one CUDA graph per
+ * staging slot (a descriptor copy and the batch kernel), re-parameterised
+ * for every run. */
+int wc_batch_create(uint32_t max_requests, uint32_t depth, wc_batch **out);
+int wc_batch_destroy(wc_batch *b);
+/* Runs all requests in ONE kernel launch on `stream`, asynchronously.  All
+ * tables must be single-value tables with the same key/value width and
+ * cg_size.  The requests of one run must commute (different tables, or
+ * requests of one kind on a table).  blocks_per_sm = 0 picks the occupancy
+ * limit.  The caller keeps the request buffers alive until the stream has
+ * passed the run; wc_batch_run blocks only when all `depth` staging slots
+ * are still in flight. */
+int wc_batch_run(wc_batch *b, const wc_batch_request *reqs, uint32_t num_requests,
+                 wc_stream_t stream, uint64_t probing_length, uint32_t blocks_per_sm);
+
+/* ------------------------------------------------------------------ */
+/* Serving loop (no counterpart in the reference)                       */
+/* ------------------------------------------------------------------ */
+
+#define WC_SERVE_PLAIN 0
+#define WC_SERVE_BATCHED 1
+
+/* One timestamped request on a resident single-value table. */
+typedef struct wc_serve_request {
+    double arrival_us;    /* arrival time relative to the start of the run */
+    wc_table *table;
+    uint64_t table_id;    /* dense id of the table (0 .. number of tables) */
+    int op;               /* WC_OP_INSERT or WC_OP_RETRIEVE */
+    int reserved;
+    const void *keys;     /* device */
+    const void *values;   /* device, insert */
+    void *values_out;     /* device, retrieve */
+    uint64_t num;
+} wc_serve_request;
+
+typedef struct wc_serve_options {
+    int mode;                    /* WC_SERVE_PLAIN or WC_SERVE_BATCHED */
+    uint32_t streams;            /* streams (0: 4); plain: tables hashed onto them,
+                                    batched: batches round-robin */
+    uint32_t depth;              /* batched: batches in flight per stream (0: 2) */
+    uint32_t max_batch_requests; /* batched: requests per batch (0: 4096) */
+    uint64_t max_batch_keys;     /* batched: keys per batch (0: no limit) */
+    uint32_t blocks_per_sm;      /* batched: 0 = occupancy limit */
+    uint32_t reserved;
+    uint64_t probing_length;
+} wc_serve_options;
+
+typedef struct wc_serve_stats {
+    uint64_t launches, batches, max_keys_in_batch;
+    double host_wall_us;
+    double gpu_batch_us;   /* batched: summed GPU time of the batches */
+    double host_launch_us; /* batched: summed host time to launch them */
+} wc_serve_stats;
+
+/* Replays `num_requests` requests, sorted by arrival, in real time in the
+ * chosen form and writes each request's completion time (device events,
+ * microseconds from the start) to complete_us[] and, if not NULL, the time
+ * it was issued to issue_us[].  Every table sees its requests in arrival
+ * order.  Blocks until all requests are complete. */
+int wc_serve_run(const wc_serve_request *reqs, uint64_t num_requests,
+                 const wc_serve_options *opt, double *issue_us, double *complete_us,
+                 wc_serve_stats *stats);
+
+/* ------------------------------------------------------------------ */
 /* Counting without allocating                                          */
 /* ------------------------------------------------------------------ */
 

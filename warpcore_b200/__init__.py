@@ -24,7 +24,7 @@ __all__ = [
     "HASH_MURMUR", "HASH_NVIDIA", "HASH_MUELLER", "HASH_IDENTITY32",
     "HASH_IDENTITY64", "PROBING_DOUBLE", "PROBING_LINEAR",
     "PROBING_QUADRATIC", "HANDLER_NOTHING", "HANDLER_STATUS",
-    "HANDLER_BOOLEAN", "DEFAULT_SEED", "DEFAULT_PROBING_LENGTH",
+    "HANDLER_BOOLEAN", "DEFAULT_SEED", "DEFAULT_PROBING_LENGTH", "Batch",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -104,6 +104,62 @@ class BloomInfo(ctypes.Structure):
     ]
 
 
+class BatchRequest(ctypes.Structure):
+    _fields_ = [
+        ("table", ctypes.c_void_p),
+        ("op", ctypes.c_int),
+        ("status_handler", ctypes.c_int),
+        ("ignore", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+        ("keys", ctypes.c_void_p),
+        ("values", ctypes.c_void_p),
+        ("values_out", ctypes.c_void_p),
+        ("status_out", ctypes.c_void_p),
+        ("num", ctypes.c_uint64),
+    ]
+
+
+class ServeRequest(ctypes.Structure):
+    _fields_ = [
+        ("arrival_us", ctypes.c_double),
+        ("table", ctypes.c_void_p),
+        ("table_id", ctypes.c_uint64),
+        ("op", ctypes.c_int),
+        ("reserved", ctypes.c_int),
+        ("keys", ctypes.c_void_p),
+        ("values", ctypes.c_void_p),
+        ("values_out", ctypes.c_void_p),
+        ("num", ctypes.c_uint64),
+    ]
+
+
+class ServeOptions(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int),
+        ("streams", ctypes.c_uint32),
+        ("depth", ctypes.c_uint32),
+        ("max_batch_requests", ctypes.c_uint32),
+        ("max_batch_keys", ctypes.c_uint64),
+        ("blocks_per_sm", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+        ("probing_length", ctypes.c_uint64),
+    ]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [
+        ("launches", ctypes.c_uint64),
+        ("batches", ctypes.c_uint64),
+        ("max_keys_in_batch", ctypes.c_uint64),
+        ("host_wall_us", ctypes.c_double),
+        ("gpu_batch_us", ctypes.c_double),
+        ("host_launch_us", ctypes.c_double),
+    ]
+
+
+OP_INSERT, OP_RETRIEVE = 0, 2
+SERVE_PLAIN, SERVE_BATCHED = 0, 1
+
 _vp = ctypes.c_void_p
 _u64 = ctypes.c_uint64
 _u32 = ctypes.c_uint32
@@ -145,6 +201,12 @@ SIGNATURES = {
     "wc_bloom_get_info": (_i, [_vp, ctypes.POINTER(BloomInfo)]),
     "wc_bloom_fpr": (_i, [_vp, _u64, ctypes.POINTER(ctypes.c_double)]),
     "wc_slots_size_noalloc": (_i, [_vp, _u64, _u32, _u32, _u64, _u64, _vp, _vp]),
+    "wc_batch_create": (_i, [_u32, _u32, _pp]),
+    "wc_batch_destroy": (_i, [_vp]),
+    "wc_batch_run": (_i, [_vp, ctypes.POINTER(BatchRequest), _u32, _vp, _u64, _u32]),
+    "wc_serve_run": (_i, [ctypes.POINTER(ServeRequest), _u64, ctypes.POINTER(ServeOptions),
+                          ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                          ctypes.POINTER(ServeStats)]),
 }
 
 _lib = None
@@ -497,6 +559,53 @@ class BloomFilter:
         out = ctypes.c_double()
         _check(lib().wc_bloom_fpr(self._h, int(n), ctypes.byref(out)))
         return out.value
+
+
+class Batch:
+    """Runs many requests on many single-value tables in one launch
+    (wc_batch_run): a list of (table, op, keys, values or values_out)."""
+
+    def __init__(self, max_requests=4096, depth=2):
+        h = ctypes.c_void_p()
+        _check(lib().wc_batch_create(int(max_requests), int(depth), ctypes.byref(h)))
+        self._h = h
+        self.max_requests = max_requests
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().wc_batch_destroy(h)
+            self._h = None
+
+    def run(self, requests, stream=None, probing_length=DEFAULT_PROBING_LENGTH, blocks_per_sm=0):
+        """requests: iterable of (table, "insert"|"retrieve", keys, values_or_out)
+        or dicts with the same fields plus optional status_out/status_handler."""
+        arr = (BatchRequest * len(requests))()
+        keep = []
+        for r, q in zip(arr, requests):
+            if isinstance(q, dict):
+                table, op, keys, buf = q["table"], q["op"], q["keys"], q["buffer"]
+                status_out = q.get("status_out")
+                handler = q.get("status_handler")
+                ignore = q.get("ignore", 0)
+            else:
+                table, op, keys, buf = q
+                status_out, handler, ignore = None, None, 0
+            r.table = table._h.value
+            r.op = OP_INSERT if op == "insert" else OP_RETRIEVE
+            r.keys = _ptr(keys)
+            if r.op == OP_INSERT:
+                r.values = _ptr(buf)
+            else:
+                r.values_out = _ptr(buf)
+            r.status_out = _ptr(status_out)
+            r.status_handler = _handler(status_out, handler)
+            r.ignore = ignore
+            r.num = keys.numel()
+            keep.append((keys, buf, status_out))
+        _check(lib().wc_batch_run(self._h, arr, len(requests), _stream(stream),
+                                  int(probing_length), int(blocks_per_sm)))
+        return keep
 
 
 def _handler(status_out, status_handler):

@@ -18,6 +18,7 @@
 #include <mutex>
 #include <string>
 #include <unordered_map>
+#include <vector>
 
 #include "wc_primes.inc"
 
@@ -753,6 +754,204 @@ int wc_bloom_fpr(const wc_bloom *b, uint64_t n, double *out)
         res += binom * base;
     }
     *out = res;
+    return WC_OK;
+}
+
+} // extern "C"
+
+/* ------------------------------------------------------------------ */
+/* batches (wc_batch.cuh)                                                */
+/* ------------------------------------------------------------------ */
+
+struct wc_batch {
+    uint32_t max_requests = 0;
+    uint32_t depth = 0;
+    uint32_t next = 0;
+    struct Slot {
+        BatchDesc *host = nullptr; /* pinned */
+        BatchDesc *dev = nullptr;
+        cudaEvent_t done = nullptr;
+        bool used = false;
+        /* one instantiated graph per (kernel, grid) seen on this slot */
+        const void *kernel = nullptr;
+        unsigned grid = 0;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cudaGraphNode_t copy_node = nullptr, kernel_node = nullptr;
+        BatchInlineArgs *inline_args = nullptr; /* host copy of small-batch parameters */
+    };
+    std::vector<Slot> slots;
+};
+
+namespace {
+
+void release_graph(wc_batch::Slot &s)
+{
+    if (s.exec) cudaGraphExecDestroy(s.exec);
+    if (s.graph) cudaGraphDestroy(s.graph);
+    s.exec = nullptr;
+    s.graph = nullptr;
+    s.kernel = nullptr;
+}
+
+/* graph of one staging slot: [descriptor copy ->] batch kernel */
+int build_graph(wc_batch::Slot &s, const void *kernel, unsigned grid, void *args, size_t bytes)
+{
+    release_graph(s);
+    WC_CUDA(cudaGraphCreate(&s.graph, 0));
+    const bool with_copy = bytes != 0;
+    if (with_copy)
+        WC_CUDA(cudaGraphAddMemcpyNode1D(&s.copy_node, s.graph, nullptr, 0, s.dev, s.host, bytes,
+                                         cudaMemcpyHostToDevice));
+    else
+        s.copy_node = nullptr;
+    cudaKernelNodeParams kp{};
+    void *kargs[] = {args};
+    kp.func = const_cast<void *>(kernel);
+    kp.gridDim = dim3(grid);
+    kp.blockDim = dim3(kBlock);
+    kp.sharedMemBytes = 0;
+    kp.kernelParams = kargs;
+    WC_CUDA(cudaGraphAddKernelNode(&s.kernel_node, s.graph, with_copy ? &s.copy_node : nullptr,
+                                   with_copy ? 1 : 0, &kp));
+    WC_CUDA(cudaGraphInstantiate(&s.exec, s.graph, 0));
+    s.kernel = kernel;
+    s.grid = grid;
+    return WC_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int wc_batch_create(uint32_t max_requests, uint32_t depth, wc_batch **out)
+{
+    if (!out || max_requests == 0) return fail(WC_ERR_INVALID_ARGUMENT, "bad batch arguments");
+    *out = nullptr;
+    if (depth == 0) depth = 2;
+    auto *b = new wc_batch();
+    b->max_requests = max_requests;
+    b->depth = depth;
+    b->slots.resize(depth);
+    for (auto &s : b->slots) {
+        cudaError_t e = cudaMallocHost(&s.host, sizeof(BatchDesc) * max_requests);
+        if (e == cudaSuccess) e = cudaMalloc(&s.dev, sizeof(BatchDesc) * max_requests);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+        if (e == cudaSuccess) s.inline_args = new BatchInlineArgs();
+        if (e != cudaSuccess) {
+            wc_batch_destroy(b);
+            return cuda_fail(e, "wc_batch_create");
+        }
+    }
+    *out = b;
+    return WC_OK;
+}
+
+int wc_batch_destroy(wc_batch *b)
+{
+    if (!b) return WC_OK;
+    for (auto &s : b->slots) {
+        if (s.done) cudaEventSynchronize(s.done);
+        release_graph(s);
+        if (s.done) cudaEventDestroy(s.done);
+        if (s.host) cudaFreeHost(s.host);
+        if (s.dev) cudaFree(s.dev);
+        delete s.inline_args;
+    }
+    delete b;
+    return WC_OK;
+}
+
+int wc_batch_run(wc_batch *b, const wc_batch_request *reqs, uint32_t num_requests,
+                 wc_stream_t stream, uint64_t probing_length, uint32_t blocks_per_sm_req)
+{
+    if (!b) return fail(WC_ERR_INVALID_ARGUMENT, "batch is NULL");
+    if (num_requests == 0) return WC_OK;
+    if (!reqs) return fail(WC_ERR_INVALID_ARGUMENT, "requests are NULL");
+    if (num_requests > b->max_requests)
+        return fail(WC_ERR_INVALID_ARGUMENT, "%u requests exceed the batch capacity %u",
+                    num_requests, b->max_requests);
+    const wc_table *t0 = reqs[0].table;
+    if (!t0) return fail(WC_ERR_INVALID_ARGUMENT, "request 0 has no table");
+    const int layout = t0->layout;
+    const uint32_t W = t0->cfg.cg_size;
+    const bool inl = num_requests <= uint32_t(kBatchInline);
+    const void *kfn = batch_kernel_ptr(layout, int(W), inl);
+    if (!kfn) return fail(WC_ERR_UNSUPPORTED, "batches serve u32/u32 and u64/u64 single-value tables");
+
+    wc_batch::Slot &s = b->slots[b->next];
+    b->next = (b->next + 1) % b->depth;
+    if (s.used) WC_CUDA(cudaEventSynchronize(s.done)); /* staging slot still in flight */
+
+    BatchInlineArgs *ia = s.inline_args;
+    BatchDesc *descs = inl ? ia->desc : s.host;
+    uint64_t total = 0;
+    for (uint32_t r = 0; r < num_requests; ++r) {
+        const wc_batch_request &q = reqs[r];
+        const wc_table *t = q.table;
+        if (!t || t->kind != 0 || t->layout != layout || t->cfg.cg_size != W)
+            return fail(WC_ERR_INVALID_ARGUMENT,
+                        "request %u: every table of a batch must be a single-value table "
+                        "of the same layout and cg_size",
+                        r);
+        if (!t->initialized) return fail(WC_ERR_NOT_INITIALIZED, "request %u: table not initialized", r);
+        if (q.op != WC_OP_INSERT && q.op != WC_OP_RETRIEVE)
+            return fail(WC_ERR_INVALID_ARGUMENT, "request %u: op must be insert or retrieve", r);
+        if (q.num && (!q.keys || (q.op == WC_OP_INSERT && !q.values) ||
+                      (q.op == WC_OP_RETRIEVE && !q.values_out)))
+            return fail(WC_ERR_INVALID_ARGUMENT, "request %u: missing buffer", r);
+        BatchDesc &d = descs[r];
+        d.t = view_of(t);
+        d.keys = q.keys;
+        d.values = q.values;
+        d.out = q.values_out;
+        d.status_out = q.status_handler == WC_HANDLER_NOTHING ? nullptr : q.status_out;
+        d.begin = total;
+        d.n = q.num;
+        d.max_windows = max_windows(probing_length, W, t->num_buckets);
+        d.bool_mask = (~q.ignore) ^ 0xFFFu;
+        d.op = q.op == WC_OP_INSERT ? kOpInsert : kOpRetrieve;
+        d.handler = q.status_handler;
+        d.pad = 0;
+        total += q.num;
+    }
+    if (total == 0) return WC_OK;
+
+    const uint64_t wave = uint64_t(device_props().sms) *
+                          (blocks_per_sm_req ? blocks_per_sm_req : uint32_t(blocks_per_sm(kfn, kBlock)));
+    const uint64_t need = (total + kBlock - 1) / kBlock;
+    const unsigned grid = unsigned(need < wave ? need : wave);
+
+    BatchArgs args;
+    args.desc = s.dev;
+    args.nreq = num_requests;
+    args.total = total;
+    ia->nreq = num_requests;
+    ia->total = total;
+    void *argp = inl ? static_cast<void *>(ia) : static_cast<void *>(&args);
+    const size_t bytes = inl ? 0 : sizeof(BatchDesc) * num_requests;
+    if (s.kernel != kfn || !s.exec) {
+        /* a graph per staging slot and kernel; grid, argument values and
+         * copy size are updated in place on later runs */
+        const int rc = build_graph(s, kfn, grid, argp, bytes);
+        if (rc) return rc;
+    } else {
+        if (!inl)
+            WC_CUDA(cudaGraphExecMemcpyNodeSetParams1D(s.exec, s.copy_node, s.dev, s.host, bytes,
+                                                       cudaMemcpyHostToDevice));
+        cudaKernelNodeParams kp{};
+        void *kargs[] = {argp};
+        kp.func = const_cast<void *>(kfn);
+        kp.gridDim = dim3(grid);
+        kp.blockDim = dim3(kBlock);
+        kp.sharedMemBytes = 0;
+        kp.kernelParams = kargs;
+        WC_CUDA(cudaGraphExecKernelNodeSetParams(s.exec, s.kernel_node, &kp));
+    }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    WC_CUDA(cudaGraphLaunch(s.exec, st));
+    WC_CUDA(cudaEventRecord(s.done, st));
+    s.used = true;
     return WC_OK;
 }
 

@@ -6,6 +6,7 @@
 #define WC_INTERNAL_H
 
 #include "wc_bloom.cuh"
+#include "wc_batch.cuh"
 
 namespace warpcore {
 namespace b200 {
@@ -28,6 +29,10 @@ CountKernel count_kernel(int layout);
 DumpKernel dump_kernel_ptr(int layout);
 
 BloomKernel bloom_kernel_ptr(int key_bytes, int slot_bytes, int cg, bool insert);
+
+/* multi-table batch kernel for a slot layout (KV32 / KV64) and window width;
+ * inline_desc selects the variant taking BatchInlineArgs */
+const void *batch_kernel_ptr(int layout, int W, bool inline_desc);
 
 /* message returned by wc_last_error() on the calling thread */
 void set_last_error(const char *msg);
