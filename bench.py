@@ -119,61 +119,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-# ---------------------------------------------------------------------------
-# synthetic data on the device (torch int64 holds the uint64 bits)
-# ---------------------------------------------------------------------------
-
-def _srl(x, s):
-    import torch
-    return torch.bitwise_and(torch.bitwise_right_shift(x, s), (1 << (64 - s)) - 1)
-
-
-def fmix64_t(x):
-    """MurmurHash3 fmix64 on int64 tensors (two's complement wrap)"""
-    import torch
-    c1 = 0xFF51AFD7ED558CCD - (1 << 64)
-    c2 = 0xC4CEB9FE1A85EC53 - (1 << 64)
-    x = torch.bitwise_xor(x, _srl(x, 33))
-    x = x * c1
-    x = torch.bitwise_xor(x, _srl(x, 33))
-    x = x * c2
-    x = torch.bitwise_xor(x, _srl(x, 33))
-    return x
-
-
-def unique_keys64(start, n, seed, device):
-    """n distinct uint64 keys: fmix64 is a bijection of the 64-bit index;
-    the two sentinels (0, ~0) are dropped"""
-    import torch
-    off = (seed * 0x9E3779B97F4A7C15) & MASK64
-    off = off - (1 << 64) if off >= (1 << 63) else off  # as a signed int64
-    idx = torch.arange(start, start + n + 4, dtype=torch.int64, device=device) + off
-    k = fmix64_t(idx)
-    k = k[(k != 0) & (k != -1)]
-    return k[:n].contiguous()
-
-
-def unique_keys32(start, n, seed, device):
-    """n distinct uint32 keys (stored in int32): a 32-bit mix of the index"""
-    import torch
-    idx = torch.arange(start, start + n + 4, dtype=torch.int64, device=device)
-    x = (idx + seed * 0x9E3779B9) & 0xFFFFFFFF
-    x = x ^ (x >> 16)
-    x = (x * 0x85EBCA6B) & 0xFFFFFFFF
-    x = x ^ (x >> 13)
-    x = (x * 0xC2B2AE35) & 0xFFFFFFFF
-    x = x ^ (x >> 16)
-    x = x[(x != 0) & (x != 0xFFFFFFFF)][:n]
-    return (x - ((x >= (1 << 31)).to(torch.int64) << 32)).to(torch.int32).contiguous()
-
-
-def uniform_values(n, nbytes, gen, device):
-    import torch
-    if nbytes == 8:
-        return torch.randint(-(1 << 63), (1 << 63) - 1, (n,), dtype=torch.int64,
-                             device=device, generator=gen)
-    return torch.randint(-(1 << 31), (1 << 31) - 1, (n,), dtype=torch.int32,
-                         device=device, generator=gen)
+# synthetic data on the device: warpcore_b200.datagen (int tensors hold the
+# unsigned bit patterns)
+from warpcore_b200.datagen import (unique_keys32, unique_keys64,  # noqa: E402
+                                   uniform_values, zipf_ranks as zipf_ranks_t)
 
 
 # ---------------------------------------------------------------------------
@@ -311,29 +260,6 @@ class Workload:
             torch.cuda.synchronize()
             return bool(self.out[self.n:].all())
         return False
-
-
-def zipf_ranks_t(n_in, s, n_out, gen, device):
-    """Zipf(s) ranks in [0, n_in) on the device by rejection sampling
-    (the published method random_distributions.cuh:285-310 follows)"""
-    import torch
-    t = (float(n_in) ** (1.0 - s) - s) / (1.0 - s)
-    out = torch.empty(n_out, dtype=torch.int64, device=device)
-    filled = 0
-    while filled < n_out:
-        m = int((n_out - filled) * 1.3) + 1024
-        p = torch.rand(m, dtype=torch.float64, device=device, generator=gen)
-        y = torch.rand(m, dtype=torch.float64, device=device, generator=gen)
-        pt = p * t
-        inv_b = torch.where(pt <= 1.0, pt, torch.pow(pt * (1.0 - s) + s, 1.0 / (1.0 - s)))
-        k = torch.floor(inv_b + 1.0)
-        b = torch.where(k <= 1.0, torch.full_like(inv_b, 1.0 / t), torch.pow(inv_b, -s) / t)
-        rat = torch.pow(k, -s) / (b * t)
-        acc = k[y < rat].clamp(max=n_in).to(torch.int64) - 1
-        take = min(acc.numel(), n_out - filled)
-        out[filled:filled + take] = acc[:take]
-        filled += take
-    return out
 
 
 def reference_gpu(wl, reps=5):

@@ -265,6 +265,25 @@ int wc_bloom_get_info(const wc_bloom *b, wc_bloom_info *info);
 int wc_bloom_fpr(const wc_bloom *b, uint64_t n, double *out);
 
 /* ------------------------------------------------------------------ */
+/* Launch tuning (no counterpart in the reference, whose launches are    */
+/* fixed at SDIV(n * cg, WARPCORE_BLOCKSIZE) x WARPCORE_BLOCKSIZE,       */
+/* single_value_hash_table.cuh:255-257)                                  */
+/* ------------------------------------------------------------------ */
+
+/* Buckets of the tuning table: load factor (inserted keys since init over
+ * capacity) < 0.5, < 0.7, < 0.85, >= 0.85; batch size 2^(6+2b) .. 2^(8+2b). */
+#define WC_TUNE_LOAD_BUCKETS 4
+#define WC_TUNE_SIZE_BUCKETS 12
+/* Launch geometry for (key width, op, load bucket, size bucket): threads
+ * per block (multiple of 32, <= 256; 0 = default 256) and resident blocks
+ * per SM (0 = occupancy limit).  op: 0 insert, 1 counting insert,
+ * 2 retrieve, 3 erase.  Written by warpcore_b200.autotune. */
+int wc_tune_set(uint32_t key_bytes, int op, uint32_t load_bucket, uint32_t size_bucket,
+                uint32_t block_threads, uint32_t blocks_per_sm);
+/* forget every tuned entry */
+int wc_tune_reset(void);
+
+/* ------------------------------------------------------------------ */
 /* Batches: many requests on many tables in one launch                  */
 /* (no counterpart in the reference, which launches one kernel per bulk */
 /* call, single_value_hash_table.cuh:241-337)                            */

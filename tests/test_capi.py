@@ -83,3 +83,27 @@ def test_ops_on_null_handle_fail_cleanly():
     lib = wc.lib()
     assert lib.wc_svht_insert(None, None, None, 10, None, 1, None, 0, 0) == -1
     assert lib.wc_table_destroy(None) == 0
+
+
+def test_tune_set_validates_arguments():
+    lib = wc.lib()
+    assert lib.wc_tune_set(4, 0, 0, 0, 64, 0) == 0
+    assert lib.wc_tune_set(3, 0, 0, 0, 64, 0) == -1
+    assert lib.wc_tune_set(4, 5, 0, 0, 64, 0) == -1
+    assert lib.wc_tune_set(4, 0, 4, 0, 64, 0) == -1
+    assert lib.wc_tune_set(4, 0, 0, 12, 64, 0) == -1
+    assert lib.wc_tune_set(4, 0, 0, 0, 48, 0) == -1
+    assert lib.wc_tune_set(4, 0, 0, 0, 512, 0) == -1
+    lib.wc_tune_reset()
+    wc._load_tuning(lib)
+
+
+def test_shipped_tuning_table_is_well_formed():
+    import json
+    import os
+    path = os.path.join(os.path.dirname(wc.__file__), "tuning_b200.json")
+    d = json.load(open(path))
+    assert "B200" in d["device"]
+    for kb, op, lb, sb, block, bps in d["entries"]:
+        assert kb in (4, 8) and op in (0, 1, 2) and 0 <= lb < 4 and 0 <= sb < 12
+        assert block in (32, 64, 128, 256)

@@ -314,3 +314,21 @@ def test_intra_batch_duplicates_keep_one_slot():
     got = host(out)
     for kk, vv in zip(base[:50], got[:50]):
         assert vv in set(vals[keys == kk].tolist())
+
+
+@pytest.mark.parametrize("block", [32, 64, 128, 256])
+def test_results_do_not_depend_on_launch_geometry(block):
+    # force one launch geometry for every tuning bucket of the u32 and u64
+    # tables, run a full round trip, then restore the shipped tuning
+    lib = wc.lib()
+    try:
+        for kb in (4, 8):
+            for op in range(4):
+                for lb in range(4):
+                    for sb in range(12):
+                        assert lib.wc_tune_set(kb, op, lb, sb, block, 1 if block == 32 else 0) == 0
+        svht_round_trip(4, 8, n=5000)
+        svht_round_trip(8, 8, n=5000)
+    finally:
+        lib.wc_tune_reset()
+        wc._load_tuning(lib)

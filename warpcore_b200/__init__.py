@@ -201,6 +201,8 @@ SIGNATURES = {
     "wc_bloom_get_info": (_i, [_vp, ctypes.POINTER(BloomInfo)]),
     "wc_bloom_fpr": (_i, [_vp, _u64, ctypes.POINTER(ctypes.c_double)]),
     "wc_slots_size_noalloc": (_i, [_vp, _u64, _u32, _u32, _u64, _u64, _vp, _vp]),
+    "wc_tune_set": (_i, [_u32, _i, _u32, _u32, _u32, _u32]),
+    "wc_tune_reset": (_i, []),
     "wc_batch_create": (_i, [_u32, _u32, _pp]),
     "wc_batch_destroy": (_i, [_vp]),
     "wc_batch_run": (_i, [_vp, ctypes.POINTER(BatchRequest), _u32, _vp, _u64, _u32]),
@@ -226,7 +228,19 @@ def lib():
             f.restype = res
             f.argtypes = args
         _lib = l
+        _load_tuning(l)
     return _lib
+
+
+def _load_tuning(l):
+    """launch geometry measured by warpcore_b200.autotune (tuning_b200.json)"""
+    import json
+    path = os.environ.get("WARPCORE_B200_TUNING") or os.path.join(_HERE, "tuning_b200.json")
+    if path == "none" or not os.path.exists(path):
+        return
+    with open(path) as f:
+        for kb, op, lb, sb, block, bps in json.load(f)["entries"]:
+            l.wc_tune_set(kb, op, lb, sb, block, bps)
 
 
 def _check(rc):

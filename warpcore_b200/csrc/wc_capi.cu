@@ -111,17 +111,47 @@ const DeviceProps &device_props()
 int blocks_per_sm(const void *kernel, int block)
 {
     static std::mutex mu;
-    static std::unordered_map<const void *, int> cache;
+    static std::unordered_map<const void *, int> cache[6];
+    const int slot = block >= 256 ? 0 : block >= 128 ? 1 : block >= 64 ? 2 : block >= 32 ? 3 : 4;
     std::lock_guard<std::mutex> lock(mu);
-    auto it = cache.find(kernel);
-    if (it != cache.end()) return it->second;
+    auto it = cache[slot].find(kernel);
+    if (it != cache[slot].end()) return it->second;
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, block, 0) != cudaSuccess || n < 1) {
         cudaGetLastError();
         n = 1;
     }
-    cache.emplace(kernel, n);
+    cache[slot].emplace(kernel, n);
     return n;
+}
+
+/* ---- launch tuning table (filled by the autotuner through wc_tune_set) ----
+ * keyed on key width, operation, load-factor bucket and batch-size bucket;
+ * an empty entry means the default geometry (256 threads, occupancy limit) */
+struct TuneEntry {
+    uint32_t block = 0, blocks_per_sm = 0;
+};
+constexpr int kTuneOps = 4, kTuneLoads = WC_TUNE_LOAD_BUCKETS, kTuneSizes = WC_TUNE_SIZE_BUCKETS;
+TuneEntry g_tune[2][kTuneOps][kTuneLoads][kTuneSizes];
+std::mutex g_tune_mu;
+
+int tune_size_bucket(uint64_t n)
+{
+    int lg = 0;
+    while ((1ull << (lg + 1)) <= n && lg < 62) ++lg;
+    int b = (lg - 6) / 2;
+    return b < 0 ? 0 : (b >= kTuneSizes ? kTuneSizes - 1 : b);
+}
+
+int tune_load_bucket(double lf)
+{
+    return lf < 0.5 ? 0 : lf < 0.7 ? 1 : lf < 0.85 ? 2 : 3;
+}
+
+TuneEntry tune_lookup(uint32_t key_bytes, int op, double lf, uint64_t n)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    return g_tune[key_bytes == 8][op & 3][tune_load_bucket(lf)][tune_size_bucket(n)];
 }
 
 /* grid for `items` work items of which one block handles `per_block` per
@@ -158,6 +188,7 @@ struct wc_table {
     uint32_t *status = nullptr;            /* device Status word */
     unsigned long long *counter = nullptr; /* device scratch counter */
     int device = 0;
+    uint64_t keys_inserted = 0; /* since init: an upper bound of size(), for tuning */
 };
 
 struct wc_bloom {
@@ -351,10 +382,21 @@ int table_op(wc_table *t, int op, const void *keys, const void *values, void *ou
     a.bool_mask = (~ignore) ^ 0xFFFu; /* ~Status(Ignore), status.cuh:142-146 */
     a.handler = handler;
     a.is_set = t->kind == 1;
-    const unsigned grid = grid_for(reinterpret_cast<const void *>(k), kBlock, n, kBlock);
+    /* launch geometry: the tuned entry for this key width, operation, load
+     * and batch size, else 256 threads and the occupancy limit */
+    const double lf = t->capacity ? double(t->keys_inserted) / double(t->capacity) : 0.0;
+    const TuneEntry te = tune_lookup(t->cfg.key_bytes, op, lf > 1.0 ? 1.0 : lf, n);
+    const int block = te.block ? int(te.block) : kBlock;
+    const void *kfn = reinterpret_cast<const void *>(k);
+    const int occ = blocks_per_sm(kfn, block);
+    const uint64_t bps = te.blocks_per_sm && int(te.blocks_per_sm) < occ ? te.blocks_per_sm : uint64_t(occ);
+    const uint64_t wave = uint64_t(device_props().sms) * bps;
+    uint64_t need = (n + block - 1) / block;
+    const unsigned grid = unsigned(need < wave ? need : (wave ? wave : 1));
     void *args[] = {&a};
-    WC_CUDA(cudaLaunchKernel(reinterpret_cast<const void *>(k), dim3(grid), dim3(kBlock), args, 0,
+    WC_CUDA(cudaLaunchKernel(kfn, dim3(grid), dim3(block), args, 0,
                              reinterpret_cast<cudaStream_t>(stream)));
+    if (op == kOpInsert || op == kOpCount) t->keys_inserted += n;
     return WC_OK;
 }
 
@@ -433,6 +475,7 @@ int wc_table_init(wc_table *t, uint64_t seed, wc_stream_t stream)
     if (!t) return fail(WC_ERR_INVALID_ARGUMENT, "table is NULL");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     t->initialized = false;
+    t->keys_inserted = 0;
     t->seed = seed & key_mask(t->cfg.key_bytes);
     int rc = fill_slots(t, s);
     if (rc) return rc;
@@ -615,6 +658,31 @@ int wc_table_get_info(const wc_table *t, wc_table_info *info)
     info->slots = t->slots;
     info->status = t->status;
     info->is_initialized = t->initialized ? 1 : 0;
+    return WC_OK;
+}
+
+/* ---- launch tuning ---- */
+
+int wc_tune_set(uint32_t key_bytes, int op, uint32_t load_bucket, uint32_t size_bucket,
+                uint32_t block_threads, uint32_t blocks_per_sm_)
+{
+    if ((key_bytes != 4 && key_bytes != 8) || op < 0 || op > 3 || load_bucket >= uint32_t(kTuneLoads) ||
+        size_bucket >= uint32_t(kTuneSizes))
+        return fail(WC_ERR_INVALID_ARGUMENT, "tuning key out of range");
+    if (block_threads && (block_threads % 32 || block_threads > 256))
+        return fail(WC_ERR_INVALID_ARGUMENT, "block_threads must be a multiple of 32, at most 256");
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune[key_bytes == 8][op][load_bucket][size_bucket] = TuneEntry{block_threads, blocks_per_sm_};
+    return WC_OK;
+}
+
+int wc_tune_reset(void)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    for (auto &a : g_tune)
+        for (auto &b : a)
+            for (auto &c : b)
+                for (auto &e : c) e = TuneEntry{};
     return WC_OK;
 }
 
