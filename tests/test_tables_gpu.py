@@ -332,3 +332,29 @@ def test_results_do_not_depend_on_launch_geometry(block):
     finally:
         lib.wc_tune_reset()
         wc._load_tuning(lib)
+
+
+@pytest.mark.parametrize("kb", [4, 8])
+@pytest.mark.parametrize("skew", ["zipf", "uniform"])
+def test_counting_block_cache_path(kb, skew):
+    # no per-key statuses: counts go through the per-block shared-memory
+    # cache; counts and the table Status word must still match the oracle
+    distinct = 20000
+    occ = 300000
+    g, r = make_pair(o.COUNTING, kb, 3 * distinct, 4)
+    allk = o.gen_unique_keys(kb, distinct + 1000, 61)
+    if skew == "zipf":
+        ranks = o.gen_zipf_ranks(distinct, 1.1, occ, 62).astype(np.int64) - 1
+    else:
+        ranks = np.random.default_rng(63).integers(0, distinct, occ)
+    keys = allk[ranks]
+    # two calls: keys of the second are partly present already
+    for part in (keys[: occ // 2], keys[occ // 2:]):
+        g.insert(dev(part))
+        r.insert(part)
+        assert g.pop_status() == r.pop_status()
+    out = empty_dev(allk.size, kb, SENT[kb])
+    g.retrieve(dev(allk), out)
+    r_out = r.retrieve(allk, np.full(allk.size, SENT[kb], dtype=allk.dtype))
+    assert np.array_equal(host(out), r_out)
+    assert g.size() == r.size()

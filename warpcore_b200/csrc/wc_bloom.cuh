@@ -49,6 +49,29 @@ __device__ __forceinline__ T atomic_or_any(T *p, T v)
         return T(atomicOr(reinterpret_cast<unsigned int *>(p), (unsigned int)v));
 }
 
+#ifndef WC_BLOOM_INSERT_READS_BLOCK
+#define WC_BLOOM_INSERT_READS_BLOCK 1
+#endif
+
+/* bit masks of the CG words of key's block, computed once by the lane that
+ * owns the key */
+template <class K, class S, int CG>
+__device__ __forceinline__ void block_masks(K key, K seed, uint32_t hasher, uint64_t k, S (&m)[CG])
+{
+    constexpr uint64_t kSlotBits = sizeof(S) * 8;
+    constexpr uint64_t kBlockBits = kSlotBits * CG;
+#pragma unroll
+    for (int w = 0; w < CG; ++w) m[w] = 0;
+    for (uint64_t j = 0; j < k; ++j) {
+        const uint64_t h = hash_key<K>(hasher, K(key + seed + K(j))) & (kBlockBits - 1);
+        const int word = int(h / kSlotBits);
+        const S bit = S(1) << (h % kSlotBits);
+#pragma unroll
+        for (int w = 0; w < CG; ++w)
+            if (word == w) m[w] |= bit;
+    }
+}
+
 template <class K, class S, int CG, bool INSERT>
 __global__ void __launch_bounds__(256) bloom_kernel(const BloomArgs a)
 {
@@ -61,6 +84,10 @@ __global__ void __launch_bounds__(256) bloom_kernel(const BloomArgs a)
     constexpr uint64_t kSlotBits = SB * 8;
     constexpr uint64_t kBlockBits = kSlotBits * CG;
     constexpr uint32_t kGroupMask = TPK == 32 ? kFull : ((1u << TPK) - 1u);
+    /* small blocks: the owner computes the masks once and the group lanes
+     * receive their words by shuffles; large blocks: every group lane derives
+     * the masks of its own words */
+    constexpr bool kOwnerMasks = CG * SB <= 64;
 
     const int lane = threadIdx.x & 31;
     const int g = lane / TPK;
@@ -76,16 +103,18 @@ __global__ void __launch_bounds__(256) bloom_kernel(const BloomArgs a)
         const bool active = i < a.n;
         const K key = active ? ld_stream(keys + i) : K(0);
         const uint64_t blk = fast_mod(hash_key<K>(a.hasher, K(key + seed)), a.num_blocks, a.magic_blocks);
+        S own_mask[kOwnerMasks ? CG : 1];
+        if constexpr (kOwnerMasks) block_masks<K, S, CG>(key, seed, a.hasher, a.k, own_mask);
 
+        constexpr bool kRead = !INSERT || WC_BLOOM_INSERT_READS_BLOCK;
         LaneWords win[TPK];
-        bool own_ok[TPK];
 #pragma unroll
         for (int r = 0; r < TPK; ++r) {
             const int o = r * G + g; /* owner lane of this round's block */
             const uint64_t b = shfl_any(blk, o);
-            own_ok[r] = (base + o) < a.n;
             const uint64_t w0 = b * CG + uint64_t(q) * SPL;
-            if (own_ok[r]) {
+            win[r] = LaneWords{{0u, 0u, 0u, 0u}};
+            if (kRead && (base + o) < a.n) {
                 if (b * CG + CG <= a.num_slots) {
                     win[r] = load_lane<LB>(words + w0);
                 } else {
@@ -97,8 +126,6 @@ __global__ void __launch_bounds__(256) bloom_kernel(const BloomArgs a)
                         else { win[r].w[2 * s] = uint32_t(v); win[r].w[2 * s + 1] = uint32_t(uint64_t(v) >> 32); }
                     }
                 }
-            } else {
-                win[r] = LaneWords{{0u, 0u, 0u, 0u}};
             }
         }
 
@@ -106,18 +133,27 @@ __global__ void __launch_bounds__(256) bloom_kernel(const BloomArgs a)
 #pragma unroll
         for (int r = 0; r < TPK; ++r) {
             const int o = r * G + g;
-            const K kr = shfl_any(key, o);
+            const bool own_ok = (base + o) < a.n;
             const uint64_t b = shfl_any(blk, o);
             S mask[SPL];
+            if constexpr (kOwnerMasks) {
 #pragma unroll
-            for (int s = 0; s < SPL; ++s) mask[s] = 0;
-            for (uint64_t j = 0; j < a.k; ++j) {
-                const uint64_t h = mod_u64(hash_key<K>(a.hasher, K(kr + seed + K(j))), kBlockBits);
-                const int word = int(h / kSlotBits);
-                if (word / SPL == q) {
+                for (int w = 0; w < CG; ++w) {
+                    const S m = shfl_any(own_mask[w], o);
+                    if (w / SPL == q) mask[w % SPL] = m;
+                }
+            } else {
+                const K kr = shfl_any(key, o);
 #pragma unroll
-                    for (int s = 0; s < SPL; ++s)
-                        if (word % SPL == s) mask[s] |= S(1) << (h % kSlotBits);
+                for (int s = 0; s < SPL; ++s) mask[s] = 0;
+                for (uint64_t j = 0; j < a.k; ++j) {
+                    const uint64_t h = hash_key<K>(a.hasher, K(kr + seed + K(j))) & (kBlockBits - 1);
+                    const int word = int(h / kSlotBits);
+                    if (word / SPL == q) {
+#pragma unroll
+                        for (int s = 0; s < SPL; ++s)
+                            if (word % SPL == s) mask[s] |= S(1) << (h % kSlotBits);
+                    }
                 }
             }
             bool ok = true;
@@ -126,7 +162,7 @@ __global__ void __launch_bounds__(256) bloom_kernel(const BloomArgs a)
                 const S w = lane_word<S>(win[r], s);
                 const bool missing = (w & mask[s]) != mask[s];
                 ok &= !missing;
-                if (INSERT && own_ok[r] && missing) {
+                if (INSERT && own_ok && mask[s] && (!kRead || missing)) {
                     uint64_t wi = b * CG + uint64_t(q) * SPL + s;
                     if (wi >= a.num_slots) wi -= a.num_slots; /* ragged last block */
                     atomic_or_any(words + wi, mask[s]);

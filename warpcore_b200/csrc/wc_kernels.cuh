@@ -67,6 +67,52 @@ __device__ __forceinline__ T shfl_any(T v, int src)
     }
 }
 
+/* one thread counts c occurrences of key into the table (claim an empty
+ * slot in slot order or add to the key's slot), as the warp kernel does */
+template <class L, int W>
+__device__ void count_one(const TableView &t, typename L::key_t key, uint32_t c,
+                          uint64_t max_windows, uint32_t &join)
+{
+    using K = typename L::key_t;
+    using V = typename L::val_t;
+    constexpr int SB = L::kSlotBytes;
+    const K empty = K(t.empty_key);
+    unsigned char *const slots = reinterpret_cast<unsigned char *>(t.slots);
+    uint64_t b = probe_begin<K>(t, key), step = 0, wins = 0;
+    uint32_t st = kStNone;
+    if (c > 1) join |= kStDuplicateKey;
+    for (;;) {
+        unsigned char *const bptr = slots + b * uint64_t(W) * SB;
+        bool resolved = false;
+        for (int s = 0; s < W && !resolved; ++s) {
+            unsigned char *const sp = bptr + s * SB;
+            const K sk = __ldcg(reinterpret_cast<const typename std::conditional<
+                                    sizeof(K) == 8, unsigned long long, unsigned int>::type *>(sp));
+            if (sk == key) {
+                join |= kStDuplicateKey;
+                count_add<L>(sp, c, t.max_count, st, join);
+                resolved = true;
+            } else if (sk == empty) {
+                K old_key;
+                if (claim_slot<L>(sp, empty, key, V(c), old_key)) {
+                    resolved = true;
+                } else if (old_key == key) {
+                    join |= kStDuplicateKey;
+                    count_add<L>(sp, c, t.max_count, st, join);
+                    resolved = true;
+                }
+            }
+        }
+        if (resolved) return;
+        if (++wins >= max_windows) {
+            join |= kStProbingLengthExceeded;
+            return;
+        }
+        if (wins == 1) step = probe_step<K>(t, key);
+        b = probe_next(t, b, step);
+    }
+}
+
 template <class L, int W, int OP>
 __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(const TableOpArgs a)
 {
@@ -99,7 +145,8 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
     per = (per + 31) & ~uint64_t(31);
     const uint64_t wb = warp * per < a.n ? warp * per : a.n;
     const uint64_t we = wb + per < a.n ? wb + per : a.n;
-    if (wb >= we) return;
+    /* (a warp without keys runs the loop once and leaves it: every warp must
+     * reach the block barriers of the counting cache below) */
 
     const K empty = K(t.empty_key);
     const K tomb = K(t.tombstone_key);
@@ -128,6 +175,22 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
     K key = empty;
     V val = 0;
     uint32_t st = kStNone, join = 0, cnt_add = 1;
+
+    /* Counting inserts without per-key statuses go through a per-block
+     * shared-memory count cache first: equal keys of the block add up there,
+     * and each cached key reaches the table once, when the block flushes.
+     * Skewed (Zipf) streams thus stop serialising atomics on hot slots. */
+    constexpr int kCache = OP == kOpCount ? 1024 : 1;
+    __shared__ K sc_key[kCache];
+    __shared__ V sc_cnt[kCache];
+    const bool use_cache = OP == kOpCount && a.handler == kHandlerNothing;
+    if (use_cache) {
+        for (int c = threadIdx.x; c < kCache; c += blockDim.x) {
+            sc_key[c] = empty;
+            sc_cnt[c] = 0;
+        }
+        __syncthreads();
+    }
 
     for (;;) {
         /* ---- refill lanes whose key is done, in input order ---- */
@@ -196,6 +259,34 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
             if constexpr (kValueIn) {
                 const V lv = shfl_any(val, last);
                 if (fresh) val = lv;
+            }
+        }
+        if constexpr (OP == kOpCount) {
+            if (use_cache && refill && pending) {
+                const uint32_t h = uint32_t((uint64_t(key) * 0x9E3779B97F4A7C15ull) >> 54);
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    const int c = int((h + p) & (kCache - 1));
+                    K cur = *reinterpret_cast<volatile K *>(&sc_key[c]);
+                    bool first = false;
+                    if (cur == empty) {
+                        cur = K(atomicCAS(reinterpret_cast<typename std::conditional<sizeof(K) == 8,
+                                          unsigned long long, unsigned int>::type *>(&sc_key[c]),
+                                          (typename std::conditional<sizeof(K) == 8, unsigned long long,
+                                                                     unsigned int>::type)empty,
+                                          (typename std::conditional<sizeof(K) == 8, unsigned long long,
+                                                                     unsigned int>::type)key));
+                        first = cur == empty;
+                        if (first) cur = key;
+                    }
+                    if (cur == key) {
+                        atomic_add_any(&sc_cnt[c], V(cnt_add));
+                        if (!first) join |= kStDuplicateKey;
+                        st = kStNone;
+                        pending = false;
+                        break;
+                    }
+                }
             }
         }
         if (refill && pending) bucket = probe_begin<K>(t, key);
@@ -379,6 +470,16 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
                         (unsigned char)((st & a.bool_mask) != 0);
             }
             has = false;
+        }
+    }
+    if constexpr (OP == kOpCount) {
+        if (use_cache) {
+            /* flush: every cached key is counted into the table once */
+            __syncthreads();
+            for (int c = threadIdx.x; c < kCache; c += blockDim.x) {
+                const K ck = sc_key[c];
+                if (ck != empty) count_one<L, W>(t, ck, uint32_t(sc_cnt[c]), a.max_windows, join);
+            }
         }
     }
     const uint32_t wjoin = __reduce_or_sync(kFull, join);
