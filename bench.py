@@ -132,7 +132,7 @@ from warpcore_b200.datagen import (unique_keys32, unique_keys64,  # noqa: E402
 class Workload:
     """one step = init + insert(n) + retrieve(q) on resident inputs"""
 
-    def __init__(self, kind, log2n, load, rank, device):
+    def __init__(self, kind, log2n, load, rank, device, world=1, shard=False):
         import torch
         import warpcore_b200 as wc
         self.kind = kind
@@ -148,7 +148,8 @@ class Workload:
         n, q = self.n, self.q
         if kind in ("svht32", "svht64", "hashset64"):
             mk = unique_keys32 if kb == 4 else unique_keys64
-            keys = mk(0, n + q // 2, seed, device)
+            # ranks draw disjoint index ranges of the same bijection
+            keys = mk(rank * (n + q), n + q // 2, 17, device)
             self.keys = keys[:n].contiguous()
             absent = keys[n:n + q // 2]
             self.values = uniform_values(n, kb, gen, device)
@@ -166,6 +167,16 @@ class Workload:
                 self.table = wc.HashSet(int(n / load), key_bytes=8)
                 self.out = torch.empty(q, dtype=torch.uint8, device=device)
                 self.bytes_insert, self.bytes_retrieve = 8 + 32 + 32, 8 + 1 + 32
+            elif shard and kind != "hashset64":
+                # sharded over the ranks: keys are routed to their owner
+                # (partition kernel + NCCL all-to-all) inside every step
+                from warpcore_b200.distributed import DistributedSingleValueHashTable
+                self.table = DistributedSingleValueHashTable(int(world * n / load), key_bytes=kb)
+                self.out = torch.empty(q, dtype=self.values.dtype, device=device)
+                # the table kernel's algorithmic bytes; the timed op also
+                # holds the routing (partition + all-to-all)
+                self.bytes_insert = kb + kb + 32 + 32
+                self.bytes_retrieve = kb + kb + 1 + 32
             else:
                 self.table = wc.SingleValueHashTable(int(n / load), key_bytes=kb)
                 self.out = torch.empty(q, dtype=self.values.dtype, device=device)
@@ -201,16 +212,28 @@ class Workload:
 
     # -- one step's operations --
     def init(self, stream):
-        self.table.init(stream=stream)
+        if self.sharded:
+            self.table.init()
+        else:
+            self.table.init(stream=stream)
 
     def insert(self, stream):
-        if self.kind in ("svht32", "svht64"):
+        if self.sharded:
+            self.table.insert(self.keys, self.values)
+        elif self.kind in ("svht32", "svht64"):
             self.table.insert(self.keys, self.values, stream=stream)
         else:
             self.table.insert(self.keys, stream=stream)
 
     def retrieve(self, stream):
-        self.table.retrieve(self.queries, self.out, stream=stream)
+        if self.sharded:
+            self.table.retrieve(self.queries, self.out)
+        else:
+            self.table.retrieve(self.queries, self.out, stream=stream)
+
+    @property
+    def sharded(self):
+        return type(self.table).__name__ == "DistributedSingleValueHashTable"
 
     def answers_ok(self, out):
         """the retrieve output `out` (written by any implementation after an
@@ -240,7 +263,7 @@ class Workload:
             torch.cuda.synchronize()
             ok_hits = bool(torch.equal(self.out[self.hit], self.expected[self.hit]))
             ok_miss = bool((self.out[~self.hit] == -1).all())
-            ok_size = self.table.size() == self.n
+            ok_size = self.table.size() == self.n * (self.table.world if self.sharded else 1)
             return ok_hits and ok_miss and ok_size
         if self.kind == "hashset64":
             self.out.fill_(7)
@@ -346,11 +369,21 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=device)
+    elif args.shard:
+        import datetime
+        import socket
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            port = so.getsockname()[1]
+        dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0,
+                                world_size=1, timeout=datetime.timedelta(seconds=120),
+                                device_id=device)
 
     import warpcore_b200  # noqa: F401
     warpcore_b200.lib()
 
-    wl = Workload(args.workload, args.log2n, args.load, rank, device)
+    wl = Workload(args.workload, args.log2n, args.load, rank, device, world,
+                  shard=args.shard or world > 1)
     stream = torch.cuda.Stream(device=device)
     torch.cuda.synchronize()
     verified = wl.verify()
@@ -374,14 +407,15 @@ def run_ours(args):
     time.sleep(0.3)
     wall0 = time.perf_counter()
     t0.record(stream)
-    for k in range(args.steps):
-        ev[k][0].record(stream)
-        wl.init(stream)
-        ev[k][1].record(stream)
-        wl.insert(stream)
-        ev[k][2].record(stream)
-        wl.retrieve(stream)
-        ev[k][3].record(stream)
+    with torch.cuda.stream(stream):  # the sharded table runs on the current stream
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            wl.init(stream)
+            ev[k][1].record(stream)
+            wl.insert(stream)
+            ev[k][2].record(stream)
+            wl.retrieve(stream)
+            ev[k][3].record(stream)
     t1.record(stream)
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
@@ -435,7 +469,9 @@ def run_ours(args):
                 "capacity": int(wl.table.capacity) if hasattr(wl.table, "capacity") else None,
                 "ops_per_step": ops_step,
                 "l2": "inputs larger than L2 (no flush)" if args.log2n >= 24 else "inputs may be L2-resident",
-                "parallelism": "independent table per GPU" if world > 1 else "single GPU",
+                "parallelism": ("table sharded over %d GPU(s): keys routed to owners by "
+                                "partition kernel + NCCL all-to-all in every step" % world)
+                               if wl.sharded else "single GPU",
             },
             "insert_gops": round(wl.n / (statistics.mean(ins_ms) * 1e-3) / 1e9, 4),
             "retrieve_gops": round(wl.q / (statistics.mean(ret_ms) * 1e-3) / 1e9, 4),
@@ -457,12 +493,14 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "reference_gpu_build": ref_gpu,
             "e2e": e2e,
-            "gpu_launches": 3 * args.steps,
+            # ours per step: fill + insert + retrieve; sharded adds the three
+            # partition kernels before insert and before retrieve
+            "gpu_launches": (9 if wl.sharded else 3) * args.steps,
             "clocks": clocks,
             "wall_s": round(wall, 3),
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
+    if world > 1 or args.shard:
         dist.barrier()
         dist.destroy_process_group()
 
@@ -509,6 +547,11 @@ def run_e2e(wl, stream, args, world):
         torch.cuda.synchronize()
     wl.keys, wl.values, wl.queries = keys0, vals0, q0
     ms = a.elapsed_time(b)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], dtype=torch.float64, device=wl.keys.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)  # slowest rank
+        ms = float(t.item())
     ops = (wl.n + wl.q) * steps * world
     return {"value": round(ops / (ms * 1e-3) / 1e9, 4), "unit": "Gops/s",
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
@@ -665,6 +708,9 @@ def main():
     ap.add_argument("--load", type=float, default=0.9)
     ap.add_argument("--cpu-log2n", type=int, default=24)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="svht: use the sharded table (partition + NCCL all-to-all) "
+                         "even with one rank; with more ranks it is always used")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--tables", type=int, default=4096)

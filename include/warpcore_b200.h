@@ -374,6 +374,27 @@ int wc_serve_run(const wc_serve_request *reqs, uint64_t num_requests,
                  wc_serve_stats *stats);
 
 /* ------------------------------------------------------------------ */
+/* Key routing for tables sharded over GPUs (no counterpart in the       */
+/* reference, which is single-GPU)                                       */
+/* ------------------------------------------------------------------ */
+
+#define WC_PARTITION_MAX_PARTS 1024
+
+/* Groups keys (and values, if not NULL) by owning shard:
+ * owner(key) = (hi32(fmix64(key ^ salt)) * num_parts) >> 32.  Writes the
+ * grouped keys/values, perm_out[j] = input position of output j, and
+ * counts_out[p] = keys owned by shard p (all device buffers; counts_out is
+ * num_parts uint64, scratch is 2 * num_parts + 1 uint64).  Asynchronous on
+ * `stream`.  The kernels check every output position against n; after the
+ * stream completes, scratch[2 * num_parts] holds the number of keys that
+ * failed the check and were dropped (0 unless the inputs changed while the
+ * call ran). */
+int wc_partition(const void *keys, const void *values, uint64_t n, uint32_t key_bytes,
+                 uint32_t value_bytes, uint32_t num_parts, uint64_t salt, void *keys_out,
+                 void *values_out, uint64_t *perm_out, uint64_t *counts_out,
+                 uint64_t *scratch, wc_stream_t stream);
+
+/* ------------------------------------------------------------------ */
 /* Counting without allocating                                          */
 /* ------------------------------------------------------------------ */
 

@@ -201,6 +201,7 @@ SIGNATURES = {
     "wc_bloom_get_info": (_i, [_vp, ctypes.POINTER(BloomInfo)]),
     "wc_bloom_fpr": (_i, [_vp, _u64, ctypes.POINTER(ctypes.c_double)]),
     "wc_slots_size_noalloc": (_i, [_vp, _u64, _u32, _u32, _u64, _u64, _vp, _vp]),
+    "wc_partition": (_i, [_vp, _vp, _u64, _u32, _u32, _u32, _u64, _vp, _vp, _vp, _vp, _vp, _vp]),
     "wc_tune_set": (_i, [_u32, _i, _u32, _u32, _u32, _u32]),
     "wc_tune_reset": (_i, []),
     "wc_batch_create": (_i, [_u32, _u32, _pp]),

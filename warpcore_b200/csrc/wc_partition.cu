@@ -1,0 +1,180 @@
+/*
+ * wc_partition.cu -- routes keys to the rank that owns them, for tables
+ * sharded over several GPUs (the reference is single-GPU; this is the
+ * exchange step of the sharded form).
+ *
+ * owner(key) = (hi32(fmix64(key ^ salt)) * parts) >> 32: a multiply-shift
+ * range reduction of a mix that is independent of the probing hashers, so
+ * every shard sees a uniform sample of the key space.  The keys (and values)
+ * are grouped by owner with a counting sort: a count pass, an exclusive
+ * scan, and a scatter pass; within an owner the order is unspecified, and
+ * perm_out[j] names the input position of output j so that answers can be
+ * put back.  Atomics are aggregated per warp over lanes with equal owners.
+ * Every output position is checked against n; a key that fails the check
+ * (possible only if the keys change between the count and scatter passes)
+ * is dropped and counted in the error word, so the call cannot write out of
+ * bounds.
+ */
+#include <warpcore_b200.h>
+
+#include "wc_internal.h"
+
+namespace warpcore {
+namespace b200 {
+
+__host__ __device__ __forceinline__ uint32_t partition_owner(uint64_t key, uint64_t salt,
+                                                             uint32_t parts)
+{
+    const uint64_t h = fmix64(key ^ salt);
+    return uint32_t(((h >> 32) * uint64_t(parts)) >> 32);
+}
+
+template <class K>
+__global__ void __launch_bounds__(256) partition_count_kernel(const K *keys, uint64_t n,
+                                                              uint32_t parts, uint64_t salt,
+                                                              unsigned long long *counts)
+{
+    /* The owner is held in a range-checked local and the increments are
+     * aggregated per warp, as in the scatter pass.  Written instead as one
+     * atomicAdd on hist[partition_owner(...)], this kernel counted every key
+     * in hist[0] on sm_100a (CUDA 12.9); the GPU test with one repeated key
+     * whose owner is not 0 guards against that. */
+    __shared__ unsigned int hist[WC_PARTITION_MAX_PARTS];
+    for (uint32_t p = threadIdx.x; p < parts; p += blockDim.x) hist[p] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    const uint64_t start = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t rounds = (n + stride - 1) / stride;
+    for (uint64_t r = 0; r < rounds; ++r) {
+        const uint64_t i = start + r * stride;
+        const bool active = i < n;
+        const K k = active ? keys[i] : K(0);
+        const uint32_t owner = active ? partition_owner(uint64_t(k), salt, parts) : 0xFFFFFFFFu;
+        const unsigned peers = __match_any_sync(kFull, owner);
+        if (owner < parts && lane == __ffs(peers) - 1) atomicAdd(&hist[owner], unsigned(__popc(peers)));
+    }
+    __syncthreads();
+    for (uint32_t p = threadIdx.x; p < parts; p += blockDim.x)
+        if (hist[p]) atomicAdd(&counts[p], (unsigned long long)hist[p]);
+}
+
+__global__ void partition_scan_kernel(const unsigned long long *counts, uint32_t parts,
+                                      unsigned long long *offsets, unsigned long long *cursors,
+                                      unsigned long long *dropped)
+{
+    /* parts <= 1024: one thread does the exclusive scan */
+    if (threadIdx.x == 0) {
+        unsigned long long s = 0;
+        for (uint32_t p = 0; p < parts; ++p) {
+            offsets[p] = s;
+            s += counts[p];
+        }
+    }
+    for (uint32_t p = threadIdx.x; p < parts; p += blockDim.x) cursors[p] = 0;
+    if (threadIdx.x == 0) *dropped = 0;
+}
+
+template <class K, class V>
+__global__ void __launch_bounds__(256) partition_scatter_kernel(
+    const K *keys, const V *values, uint64_t n, uint32_t parts, uint64_t salt,
+    const unsigned long long *offsets, unsigned long long *cursors, K *keys_out, V *values_out,
+    unsigned long long *perm_out, unsigned long long *dropped)
+{
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const uint64_t start = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t rounds = (n + stride - 1) / stride;
+    for (uint64_t r = 0; r < rounds; ++r) {
+        const uint64_t i = start + r * stride;
+        const bool active = i < n;
+        const K k = active ? keys[i] : K(0);
+        const uint32_t owner = active ? partition_owner(uint64_t(k), salt, parts) : 0xFFFFFFFFu;
+        const unsigned peers = __match_any_sync(kFull, owner);
+        const int leader = __ffs(peers) - 1;
+        unsigned long long base = 0;
+        if (active && lane == leader) base = atomicAdd(&cursors[owner], (unsigned long long)__popc(peers));
+        base = __shfl_sync(kFull, base, leader);
+        if (active) {
+            const uint64_t pos = offsets[owner] + base + __popc(peers & ((1u << lane) - 1u));
+            if (pos < n) {
+                keys_out[pos] = k;
+                if (values) values_out[pos] = values[i];
+                perm_out[pos] = i;
+            } else {
+                atomicAdd(dropped, 1ull);
+            }
+        }
+    }
+}
+
+} // namespace b200
+} // namespace warpcore
+
+using namespace warpcore::b200;
+
+extern "C" int wc_partition(const void *keys, const void *values, uint64_t n, uint32_t key_bytes,
+                            uint32_t value_bytes, uint32_t num_parts, uint64_t salt,
+                            void *keys_out, void *values_out, uint64_t *perm_out,
+                            uint64_t *counts_out, uint64_t *scratch, wc_stream_t stream)
+{
+    if (key_bytes != 4 && key_bytes != 8) {
+        set_last_error("key_bytes must be 4 or 8");
+        return WC_ERR_UNSUPPORTED;
+    }
+    if (values && value_bytes != key_bytes) {
+        set_last_error("value_bytes must equal key_bytes");
+        return WC_ERR_UNSUPPORTED;
+    }
+    if (num_parts == 0 || num_parts > WC_PARTITION_MAX_PARTS) {
+        set_last_error("num_parts must be 1 .. WC_PARTITION_MAX_PARTS");
+        return WC_ERR_INVALID_ARGUMENT;
+    }
+    if (!counts_out || !scratch || (n && (!keys || !keys_out || !perm_out || (values && !values_out)))) {
+        set_last_error("NULL buffer");
+        return WC_ERR_INVALID_ARGUMENT;
+    }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    auto *counts = reinterpret_cast<unsigned long long *>(counts_out);
+    auto *offsets = reinterpret_cast<unsigned long long *>(scratch);
+    auto *cursors = offsets + num_parts;
+    auto *dropped = cursors + num_parts;
+    cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(unsigned long long) * num_parts, s);
+    if (e != cudaSuccess) {
+        set_last_error(cudaGetErrorString(e));
+        return WC_ERR_CUDA;
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    uint64_t need = (n + 255) / 256;
+    const unsigned grid = unsigned(need < uint64_t(sms) * 4 ? (need ? need : 1) : uint64_t(sms) * 4);
+    auto *po = reinterpret_cast<unsigned long long *>(perm_out);
+    auto launched = [&]() {
+        e = cudaGetLastError();
+        if (e != cudaSuccess) set_last_error(cudaGetErrorString(e));
+        return e == cudaSuccess;
+    };
+    if (key_bytes == 4) {
+        partition_count_kernel<uint32_t><<<grid, 256, 0, s>>>(
+            reinterpret_cast<const uint32_t *>(keys), n, num_parts, salt, counts);
+        if (!launched()) return WC_ERR_CUDA;
+        partition_scan_kernel<<<1, 256, 0, s>>>(counts, num_parts, offsets, cursors, dropped);
+        if (!launched()) return WC_ERR_CUDA;
+        partition_scatter_kernel<uint32_t, uint32_t><<<grid, 256, 0, s>>>(
+            reinterpret_cast<const uint32_t *>(keys), reinterpret_cast<const uint32_t *>(values), n,
+            num_parts, salt, offsets, cursors, reinterpret_cast<uint32_t *>(keys_out),
+            reinterpret_cast<uint32_t *>(values_out), po, dropped);
+    } else {
+        partition_count_kernel<unsigned long long><<<grid, 256, 0, s>>>(
+            reinterpret_cast<const unsigned long long *>(keys), n, num_parts, salt, counts);
+        if (!launched()) return WC_ERR_CUDA;
+        partition_scan_kernel<<<1, 256, 0, s>>>(counts, num_parts, offsets, cursors, dropped);
+        if (!launched()) return WC_ERR_CUDA;
+        partition_scatter_kernel<unsigned long long, unsigned long long><<<grid, 256, 0, s>>>(
+            reinterpret_cast<const unsigned long long *>(keys),
+            reinterpret_cast<const unsigned long long *>(values), n, num_parts, salt, offsets,
+            cursors, reinterpret_cast<unsigned long long *>(keys_out),
+            reinterpret_cast<unsigned long long *>(values_out), po, dropped);
+    }
+    return launched() ? WC_OK : WC_ERR_CUDA;
+}
