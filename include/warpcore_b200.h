@@ -270,6 +270,26 @@ int wc_bloom_fpr(const wc_bloom *b, uint64_t n, double *out);
 /* single_value_hash_table.cuh:255-257)                                  */
 /* ------------------------------------------------------------------ */
 
+/* ------------------------------------------------------------------ */
+/* L2 persistence for tables that fit in L2 (no counterpart in the       */
+/* reference)                                                            */
+/* ------------------------------------------------------------------ */
+
+/* A table or filter whose slot array fits the device's persisting-L2
+ * maximum (cudaDevAttrMaxPersistingL2CacheSize) launches its kernels with an
+ * access-policy window over that array: its lines persist in L2 while keys
+ * and outputs stream past, and while other work runs between calls.  Arrays
+ * get windows at creation, in order, while the windows of all live arrays
+ * on the device fit the persisting set-aside together; the others launch
+ * without one.  The first such array sets this process's persisting-L2
+ * limit once per device.  On by default (environment variable
+ * WARPCORE_B200_L2_PERSIST=0 in the Python binding turns it off);
+ * `enable` = 0 turns the windows off for later launches and creations
+ * (*previous gets the old setting). */
+int wc_l2_persistence(int enable, int *previous);
+/* the window a table's launches use now: bytes (0 = none) and hit ratio */
+int wc_table_l2_window(const wc_table *t, uint64_t *bytes_out, float *hit_ratio_out);
+
 /* Buckets of the tuning table: load factor (inserted keys since init over
  * capacity) < 0.5, < 0.7, < 0.85, >= 0.85; batch size 2^(6+2b) .. 2^(8+2b). */
 #define WC_TUNE_LOAD_BUCKETS 4

@@ -20,7 +20,7 @@ from ._status import Status  # noqa: F401
 
 __all__ = [
     "Status", "SingleValueHashTable", "HashSet", "CountingHashTable",
-    "BloomFilter", "lib", "valid_capacity", "WarpcoreError",
+    "BloomFilter", "lib", "valid_capacity", "WarpcoreError", "set_l2_persistence",
     "HASH_MURMUR", "HASH_NVIDIA", "HASH_MUELLER", "HASH_IDENTITY32",
     "HASH_IDENTITY64", "PROBING_DOUBLE", "PROBING_LINEAR",
     "PROBING_QUADRATIC", "HANDLER_NOTHING", "HANDLER_STATUS",
@@ -202,6 +202,8 @@ SIGNATURES = {
     "wc_bloom_fpr": (_i, [_vp, _u64, ctypes.POINTER(ctypes.c_double)]),
     "wc_slots_size_noalloc": (_i, [_vp, _u64, _u32, _u32, _u64, _u64, _vp, _vp]),
     "wc_partition": (_i, [_vp, _vp, _u64, _u32, _u32, _u32, _u64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "wc_l2_persistence": (_i, [_i, ctypes.POINTER(ctypes.c_int)]),
+    "wc_table_l2_window": (_i, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(ctypes.c_float)]),
     "wc_tune_set": (_i, [_u32, _i, _u32, _u32, _u32, _u32]),
     "wc_tune_reset": (_i, []),
     "wc_batch_create": (_i, [_u32, _u32, _pp]),
@@ -230,6 +232,8 @@ def lib():
             f.argtypes = args
         _lib = l
         _load_tuning(l)
+        if os.environ.get("WARPCORE_B200_L2_PERSIST", "1") == "0":
+            l.wc_l2_persistence(0, None)
     return _lib
 
 
@@ -253,6 +257,14 @@ def _check(rc):
 def valid_capacity(min_capacity, cg_size):
     """The reference's capacity rule (base.cuh:27-34)."""
     return lib().wc_valid_capacity(int(min_capacity), int(cg_size))
+
+
+def set_l2_persistence(enable):
+    """Turn the L2 access-policy windows of tables that fit in L2 on or off
+    for later launches; returns the previous setting."""
+    prev = ctypes.c_int(0)
+    _check(lib().wc_l2_persistence(int(bool(enable)), ctypes.byref(prev)))
+    return bool(prev.value)
 
 
 def _ptr(t):
@@ -337,6 +349,13 @@ class _Table:
         out = _u64()
         _check(lib().wc_table_size(self._h, _stream(stream), ctypes.byref(out)))
         return out.value
+
+    def l2_window(self):
+        """(bytes, hit ratio) of the L2 persistence window this table's
+        launches use; (0, 0.0) when it has none"""
+        b, r = _u64(0), ctypes.c_float(0.0)
+        _check(lib().wc_table_l2_window(self._h, ctypes.byref(b), ctypes.byref(r)))
+        return int(b.value), float(r.value)
 
     def load_factor(self, stream=None):
         return float(self.size(stream)) / float(self.capacity)

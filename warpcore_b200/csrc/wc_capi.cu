@@ -11,6 +11,7 @@
 
 #include "wc_internal.h"
 
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -92,6 +93,9 @@ bool valid_cg(uint32_t cg)
 
 struct DeviceProps {
     int sms = 148;
+    int l2_bytes = 0;
+    int persist_max = 0; /* cudaDevAttrMaxPersistingL2CacheSize */
+    int window_max = 0;  /* cudaDevAttrMaxAccessPolicyWindowSize */
 };
 
 const DeviceProps &device_props()
@@ -105,7 +109,113 @@ const DeviceProps &device_props()
     if (it != cache.end()) return it->second;
     DeviceProps p;
     cudaDeviceGetAttribute(&p.sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&p.l2_bytes, cudaDevAttrL2CacheSize, dev);
+    cudaDeviceGetAttribute(&p.persist_max, cudaDevAttrMaxPersistingL2CacheSize, dev);
+    cudaDeviceGetAttribute(&p.window_max, cudaDevAttrMaxAccessPolicyWindowSize, dev);
+    cudaGetLastError(); /* an attribute this device lacks reads as 0 */
     return cache.emplace(dev, p).first->second;
+}
+
+/* ---- L2 persistence for tables that fit in L2 ----
+ * A table (or filter) whose slot array fits the device's persisting-L2
+ * maximum gets an access-policy window over that array on each of its own
+ * launches (a launch attribute, so the caller's streams are untouched):
+ * its lines are kept as persisting and the streamed keys and outputs cannot
+ * evict them.  The set-aside is this process's context limit
+ * cudaLimitPersistingL2CacheSize, made once per device when the first
+ * eligible table is created; it ends with the context. */
+std::atomic<int> g_l2_mode{1};
+
+size_t l2_setaside(int dev)
+{
+    static std::mutex mu;
+    static std::unordered_map<int, size_t> done;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = done.find(dev);
+    if (it != done.end()) return it->second;
+    const DeviceProps &p = device_props();
+    size_t want = size_t(p.persist_max);
+    const size_t cap = size_t(p.l2_bytes) / 4 * 3;
+    if (want > cap) want = cap;
+    size_t got = 0;
+    if (want && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) == cudaSuccess)
+        cudaDeviceGetLimit(&got, cudaLimitPersistingL2CacheSize);
+    cudaGetLastError();
+    done.emplace(dev, got);
+    return got;
+}
+
+/* window over [base, base + bytes) if the array fits; 0 bytes = none */
+struct L2Window {
+    void *base = nullptr;
+    uint64_t bytes = 0;
+    float hit_ratio = 0.f;
+    int device = -1;
+};
+
+/* Bytes of the live windows per device.  A new array gets a window only
+ * while all windows together fit the set-aside: with many resident tables
+ * (more than L2 holds), the first ones to fit keep their lines and the
+ * others run as plain launches, instead of all of them evicting each
+ * other's persisting lines and shrinking L2 for everything else. */
+std::mutex g_l2_mu;
+std::unordered_map<int, uint64_t> g_l2_committed;
+
+L2Window l2_window_for(void *base, uint64_t bytes)
+{
+    L2Window w;
+    if (!g_l2_mode.load(std::memory_order_relaxed) || !base || !bytes) return w;
+    const DeviceProps &p = device_props();
+    if (p.persist_max <= 0 || p.window_max <= 0) return w;
+    if (bytes > uint64_t(p.persist_max) || bytes > uint64_t(p.window_max)) return w;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t setaside = l2_setaside(dev);
+    if (!setaside || bytes > setaside) return w;
+    std::lock_guard<std::mutex> lock(g_l2_mu);
+    uint64_t &used = g_l2_committed[dev];
+    if (used + bytes > setaside) return w;
+    used += bytes;
+    w.base = base;
+    w.bytes = bytes;
+    w.hit_ratio = 1.f;
+    w.device = dev;
+    return w;
+}
+
+/* gives the window's bytes back and returns its lines to normal */
+void l2_window_release(L2Window &w)
+{
+    if (!w.bytes) return;
+    {
+        std::lock_guard<std::mutex> lock(g_l2_mu);
+        uint64_t &used = g_l2_committed[w.device];
+        used = used >= w.bytes ? used - w.bytes : 0;
+    }
+    cudaCtxResetPersistingL2Cache();
+    w = L2Window();
+}
+
+cudaError_t launch_in_window(const void *kfn, unsigned grid, unsigned block, void **args,
+                             cudaStream_t s, const L2Window &w)
+{
+    if (!w.bytes || !g_l2_mode.load(std::memory_order_relaxed))
+        return cudaLaunchKernel(kfn, dim3(grid), dim3(block), args, 0, s);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+    attr[0].val.accessPolicyWindow.base_ptr = w.base;
+    attr[0].val.accessPolicyWindow.num_bytes = size_t(w.bytes);
+    attr[0].val.accessPolicyWindow.hitRatio = w.hit_ratio;
+    attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, kfn, args);
 }
 
 int blocks_per_sm(const void *kernel, int block)
@@ -189,6 +299,7 @@ struct wc_table {
     unsigned long long *counter = nullptr; /* device scratch counter */
     int device = 0;
     uint64_t keys_inserted = 0; /* since init: an upper bound of size(), for tuning */
+    L2Window l2;                /* access-policy window over the slots, if they fit */
 };
 
 struct wc_bloom {
@@ -196,6 +307,7 @@ struct wc_bloom {
     uint64_t num_bits = 0, num_slots = 0, num_blocks = 0, k = 0, seed = 0;
     void *words = nullptr;
     int device = 0;
+    L2Window l2;
 };
 
 namespace {
@@ -259,8 +371,11 @@ int fill_slots(wc_table *t, cudaStream_t stream)
     const uint64_t n_u32 = t->capacity * t->slot_bytes / 4;
     const void *kfn = reinterpret_cast<const void *>(fill_kernel<0>);
     const unsigned grid = grid_for(kfn, kBlock, n_u32 / 4, kBlock);
-    fill_kernel<0><<<grid, kBlock, 0, stream>>>(reinterpret_cast<uint32_t *>(t->slots), n_u32, pattern);
-    WC_CUDA(cudaGetLastError());
+    uint32_t *p = reinterpret_cast<uint32_t *>(t->slots);
+    uint64_t n = n_u32;
+    uint4 pat = pattern;
+    void *args[] = {&p, &n, &pat};
+    WC_CUDA(launch_in_window(kfn, grid, kBlock, args, stream, t->l2));
     return WC_OK;
 }
 
@@ -327,6 +442,7 @@ int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, ui
         wc_table_destroy(t);
         return cuda_fail(e, "cudaMemset");
     }
+    t->l2 = l2_window_for(t->slots, bytes);
     if (!no_init) {
         rc = wc_table_init(t, t->seed, nullptr);
         if (rc) {
@@ -394,8 +510,8 @@ int table_op(wc_table *t, int op, const void *keys, const void *values, void *ou
     uint64_t need = (n + block - 1) / block;
     const unsigned grid = unsigned(need < wave ? need : (wave ? wave : 1));
     void *args[] = {&a};
-    WC_CUDA(cudaLaunchKernel(kfn, dim3(grid), dim3(block), args, 0,
-                             reinterpret_cast<cudaStream_t>(stream)));
+    WC_CUDA(launch_in_window(kfn, grid, unsigned(block), args,
+                             reinterpret_cast<cudaStream_t>(stream), t->l2));
     if (op == kOpInsert || op == kOpCount) t->keys_inserted += n;
     return WC_OK;
 }
@@ -466,6 +582,7 @@ int wc_table_destroy(wc_table *t)
     if (!t) return WC_OK;
     if (t->slots) cudaFree(t->slots);
     if (t->status) cudaFree(t->status);
+    l2_window_release(t->l2);
     delete t;
     return WC_OK;
 }
@@ -663,6 +780,22 @@ int wc_table_get_info(const wc_table *t, wc_table_info *info)
 
 /* ---- launch tuning ---- */
 
+int wc_l2_persistence(int enable, int *previous)
+{
+    const int prev = g_l2_mode.exchange(enable ? 1 : 0);
+    if (previous) *previous = prev;
+    return WC_OK;
+}
+
+int wc_table_l2_window(const wc_table *t, uint64_t *bytes_out, float *hit_ratio_out)
+{
+    if (!t || !bytes_out) return fail(WC_ERR_INVALID_ARGUMENT, "NULL argument");
+    const bool on = g_l2_mode.load() != 0;
+    *bytes_out = on ? t->l2.bytes : 0;
+    if (hit_ratio_out) *hit_ratio_out = on ? t->l2.hit_ratio : 0.f;
+    return WC_OK;
+}
+
 int wc_tune_set(uint32_t key_bytes, int op, uint32_t load_bucket, uint32_t size_bucket,
                 uint32_t block_threads, uint32_t blocks_per_sm_)
 {
@@ -716,6 +849,7 @@ int wc_bloom_create(const wc_bloom_config *cfg, uint64_t num_bits, uint64_t k, u
         delete b;
         return cuda_fail(e, "cudaMalloc");
     }
+    b->l2 = l2_window_for(b->words, bytes);
     int rc = wc_bloom_init(b, b->seed, nullptr);
     if (rc) {
         wc_bloom_destroy(b);
@@ -729,6 +863,7 @@ int wc_bloom_destroy(wc_bloom *b)
 {
     if (!b) return WC_OK;
     if (b->words) cudaFree(b->words);
+    l2_window_release(b->l2);
     delete b;
     return WC_OK;
 }
@@ -767,8 +902,8 @@ static int bloom_op(wc_bloom *b, const void *keys, uint64_t n, uint8_t *flags, w
     a.hasher = b->cfg.hasher;
     const unsigned grid = grid_for(reinterpret_cast<const void *>(k), kBlock, n, kBlock);
     void *args[] = {&a};
-    WC_CUDA(cudaLaunchKernel(reinterpret_cast<const void *>(k), dim3(grid), dim3(kBlock), args, 0,
-                             reinterpret_cast<cudaStream_t>(stream)));
+    WC_CUDA(launch_in_window(reinterpret_cast<const void *>(k), grid, kBlock, args,
+                             reinterpret_cast<cudaStream_t>(stream), b->l2));
     return WC_OK;
 }
 

@@ -27,7 +27,7 @@ import numpy as np
 
 from . import (OP_INSERT, OP_RETRIEVE, SERVE_BATCHED, SERVE_PLAIN, ServeOptions,
                ServeRequest, ServeStats, SingleValueHashTable, _check, lib,
-               valid_capacity, DEFAULT_PROBING_LENGTH)
+               set_l2_persistence, valid_capacity, DEFAULT_PROBING_LENGTH)
 
 MASK32 = 0xFFFFFFFF
 _C1, _C2 = 0x85EBCA6B, 0xC2B2AE35
@@ -175,10 +175,20 @@ class ServedWorkload:
         return plan, used
 
     def admit(self):
-        """create the admitted tables; they stay resident for the run"""
+        """create the admitted tables; they stay resident for the run.
+        When the resident tables together exceed L2, none gets an L2
+        persistence window: windows on the first few tables would only
+        take L2 away from the many others (measured: -7 % aggregate at
+        1M requests/s on 41 GiB of tables)."""
+        import torch
         plan, used = self.admission_plan()
-        for t in np.nonzero(plan)[0]:
-            self.tables[t] = SingleValueHashTable(int(self.caps[t]), key_bytes=4)
+        windows = used <= torch.cuda.get_device_properties(0).L2_cache_size
+        prev = set_l2_persistence(windows)
+        try:
+            for t in np.nonzero(plan)[0]:
+                self.tables[t] = SingleValueHashTable(int(self.caps[t]), key_bytes=4)
+        finally:
+            set_l2_persistence(prev)
         self.admitted = plan
         self.table_bytes = used
         self.rejected = int((~plan[self.table]).sum())
