@@ -271,6 +271,37 @@ int wc_bloom_fpr(const wc_bloom *b, uint64_t n, double *out);
 /* ------------------------------------------------------------------ */
 
 /* ------------------------------------------------------------------ */
+/* Bulk operations on host buffers (no counterpart in the reference,     */
+/* whose bulk calls take device pointers only)                           */
+/* ------------------------------------------------------------------ */
+
+/* A pipe stages host buffers through `depth` device slots of `chunk_keys`
+ * keys (0, 0: 2^22 keys, 3 slots; 16 bytes of device memory per staged
+ * key) and owns a copy-in and a copy-out stream.  Chunk i's copy-in, chunk
+ * i-1's kernel and chunk i-2's copy-out run at the same time.  Host
+ * buffers should be pinned (cudaHostAlloc / cudaHostRegister) for copies to
+ * overlap; pageable buffers work but copy synchronously.  One pipe serves
+ * one call at a time. */
+typedef struct wc_host_pipe wc_host_pipe;
+int wc_host_pipe_create(uint64_t chunk_keys, uint32_t depth, wc_host_pipe **out);
+int wc_host_pipe_destroy(wc_host_pipe *p);
+/* Insert (single-value: keys and values; hash set: keys; counting: keys
+ * counted) from host buffers.  Stream-ordered on `stream`: the copies start
+ * after the caller's earlier work on `stream`, the kernels run on it, and
+ * the host buffers must stay valid until `stream` passes the call. */
+int wc_table_insert_host(wc_host_pipe *p, wc_table *t, const void *h_keys, const void *h_values,
+                         uint64_t num_in, wc_stream_t stream, uint64_t probing_length);
+/* Retrieve into a host buffer: values (single-value, counting) or one flag
+ * byte per key (hash set).  Single-value and counting retrieves write hits
+ * only, as the device call does: with miss_fill NULL a miss keeps the
+ * output's content (copied in with the keys); otherwise a miss gets
+ * *miss_fill (one value), which saves that copy.  The output is complete
+ * once `stream` passes the call. */
+int wc_table_retrieve_host(wc_host_pipe *p, wc_table *t, const void *h_keys, uint64_t num_in,
+                           void *h_out, const void *miss_fill, wc_stream_t stream,
+                           uint64_t probing_length);
+
+/* ------------------------------------------------------------------ */
 /* L2 persistence for tables that fit in L2 (no counterpart in the       */
 /* reference)                                                            */
 /* ------------------------------------------------------------------ */

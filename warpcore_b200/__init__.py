@@ -21,6 +21,7 @@ from ._status import Status  # noqa: F401
 __all__ = [
     "Status", "SingleValueHashTable", "HashSet", "CountingHashTable",
     "BloomFilter", "lib", "valid_capacity", "WarpcoreError", "set_l2_persistence",
+    "HostPipe",
     "HASH_MURMUR", "HASH_NVIDIA", "HASH_MUELLER", "HASH_IDENTITY32",
     "HASH_IDENTITY64", "PROBING_DOUBLE", "PROBING_LINEAR",
     "PROBING_QUADRATIC", "HANDLER_NOTHING", "HANDLER_STATUS",
@@ -202,6 +203,10 @@ SIGNATURES = {
     "wc_bloom_fpr": (_i, [_vp, _u64, ctypes.POINTER(ctypes.c_double)]),
     "wc_slots_size_noalloc": (_i, [_vp, _u64, _u32, _u32, _u64, _u64, _vp, _vp]),
     "wc_partition": (_i, [_vp, _vp, _u64, _u32, _u32, _u32, _u64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "wc_host_pipe_create": (_i, [_u64, _u32, _pp]),
+    "wc_host_pipe_destroy": (_i, [_vp]),
+    "wc_table_insert_host": (_i, [_vp, _vp, _vp, _vp, _u64, _vp, _u64]),
+    "wc_table_retrieve_host": (_i, [_vp, _vp, _vp, _u64, _vp, _vp, _vp, _u64]),
     "wc_l2_persistence": (_i, [_i, ctypes.POINTER(ctypes.c_int)]),
     "wc_table_l2_window": (_i, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(ctypes.c_float)]),
     "wc_tune_set": (_i, [_u32, _i, _u32, _u32, _u32, _u32]),
@@ -294,6 +299,16 @@ def _check_width(t, nbytes, what):
                             % (what, nbytes, t.dtype))
 
 
+def _host_ptr(t):
+    if t is None:
+        return None
+    if t.is_cuda:
+        raise WarpcoreError("host-pipe buffers must be CPU tensors")
+    if not t.is_contiguous():
+        raise WarpcoreError("buffers must be contiguous")
+    return t.data_ptr()
+
+
 def _numel(t, n):
     if n is not None:
         return int(n)
@@ -319,6 +334,28 @@ class _Table:
         inf = TableInfo()
         _check(lib().wc_table_get_info(self._h, ctypes.byref(inf)))
         return inf
+
+    def insert_from_host(self, pipe, keys_in, values_in=None, num_in=None, stream=None,
+                         probing_length=DEFAULT_PROBING_LENGTH):
+        """insert from CPU tensors (pinned for overlap) through a HostPipe;
+        values_in for single-value tables only"""
+        _check(lib().wc_table_insert_host(pipe._h, self._h, _host_ptr(keys_in),
+                                          _host_ptr(values_in), _numel(keys_in, num_in),
+                                          _stream(stream), int(probing_length)))
+
+    def retrieve_to_host(self, pipe, keys_in, out, num_in=None, miss_fill=None, stream=None,
+                         probing_length=DEFAULT_PROBING_LENGTH):
+        """retrieve into a CPU tensor through a HostPipe; complete when
+        `stream` passes the call.  Single-value and counting tables write
+        hits only: a miss keeps `out`'s content, or gets `miss_fill`"""
+        fill = None
+        if miss_fill is not None:
+            fill = (ctypes.c_uint64 if out.element_size() == 8 else ctypes.c_uint32)(
+                int(miss_fill) & ((1 << (8 * out.element_size())) - 1))
+        _check(lib().wc_table_retrieve_host(pipe._h, self._h, _host_ptr(keys_in),
+                                            _numel(keys_in, num_in), _host_ptr(out),
+                                            ctypes.byref(fill) if fill is not None else None,
+                                            _stream(stream), int(probing_length)))
 
     @property
     def capacity(self):
@@ -593,6 +630,22 @@ class BloomFilter:
         out = ctypes.c_double()
         _check(lib().wc_bloom_fpr(self._h, int(n), ctypes.byref(out)))
         return out.value
+
+
+class HostPipe:
+    """Device staging for bulk calls on host buffers (wc_host_pipe): copies
+    of one chunk overlap the kernel of the previous one."""
+
+    def __init__(self, chunk_keys=1 << 22, depth=3):
+        h = ctypes.c_void_p()
+        _check(lib().wc_host_pipe_create(int(chunk_keys), int(depth), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().wc_host_pipe_destroy(h)
+            self._h = None
 
 
 class Batch:

@@ -963,6 +963,192 @@ int wc_bloom_fpr(const wc_bloom *b, uint64_t n, double *out)
 } // extern "C"
 
 /* ------------------------------------------------------------------ */
+/* Bulk operations on host buffers, pipelined through device staging     */
+/* ------------------------------------------------------------------ */
+
+struct wc_host_pipe {
+    int device = 0;
+    uint64_t chunk = 0;             /* keys per chunk */
+    uint32_t depth = 0;             /* staging slots */
+    char *stage = nullptr;          /* depth x (chunk x 8 keys | chunk x 8 values/outputs) */
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    std::vector<cudaEvent_t> in_done, kern_done, slot_free;
+    cudaEvent_t call_start = nullptr; /* the caller's stream at entry */
+    std::vector<char> used;
+    uint32_t next = 0;
+};
+
+namespace {
+
+int host_pipe_destroy(wc_host_pipe *p);
+
+} // namespace
+
+extern "C" int wc_host_pipe_create(uint64_t chunk_keys, uint32_t depth, wc_host_pipe **out)
+{
+    if (!out) return fail(WC_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (chunk_keys == 0) chunk_keys = uint64_t(1) << 22;
+    if (depth == 0) depth = 3;
+    if (depth > 64) return fail(WC_ERR_INVALID_ARGUMENT, "depth must be 1 .. 64");
+    if (chunk_keys > (uint64_t(1) << 30)) return fail(WC_ERR_INVALID_ARGUMENT, "chunk_keys > 2^30");
+    auto *p = new wc_host_pipe();
+    cudaGetDevice(&p->device);
+    p->chunk = chunk_keys;
+    p->depth = depth;
+    cudaError_t e = cudaMalloc(&p->stage, size_t(depth) * chunk_keys * 16);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->h2d, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->d2h, cudaStreamNonBlocking);
+    p->in_done.assign(depth, nullptr);
+    p->kern_done.assign(depth, nullptr);
+    p->slot_free.assign(depth, nullptr);
+    p->used.assign(depth, 0);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->call_start, cudaEventDisableTiming);
+    for (uint32_t i = 0; i < depth && e == cudaSuccess; ++i) {
+        e = cudaEventCreateWithFlags(&p->in_done[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->kern_done[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->slot_free[i], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
+        host_pipe_destroy(p);
+        return cuda_fail(e, "wc_host_pipe_create");
+    }
+    *out = p;
+    return WC_OK;
+}
+
+extern "C" int wc_host_pipe_destroy(wc_host_pipe *p)
+{
+    return host_pipe_destroy(p);
+}
+
+namespace {
+
+int host_pipe_destroy(wc_host_pipe *p)
+{
+    if (!p) return WC_OK;
+    if (p->h2d) cudaStreamSynchronize(p->h2d);
+    if (p->d2h) cudaStreamSynchronize(p->d2h);
+    for (uint32_t i = 0; i < p->depth; ++i) {
+        if (p->slot_free[i]) cudaEventSynchronize(p->slot_free[i]);
+        if (p->in_done[i]) cudaEventDestroy(p->in_done[i]);
+        if (p->kern_done[i]) cudaEventDestroy(p->kern_done[i]);
+        if (p->slot_free[i]) cudaEventDestroy(p->slot_free[i]);
+    }
+    if (p->call_start) cudaEventDestroy(p->call_start);
+    if (p->h2d) cudaStreamDestroy(p->h2d);
+    if (p->d2h) cudaStreamDestroy(p->d2h);
+    if (p->stage) cudaFree(p->stage);
+    delete p;
+    return WC_OK;
+}
+
+uint32_t out_bytes_of(const wc_table *t)
+{
+    return t->kind == 1 ? 1u : t->cfg.value_bytes;
+}
+
+int host_op(wc_host_pipe *p, wc_table *t, bool insert, const void *h_keys, const void *h_values,
+            void *h_out, const void *miss_fill, uint64_t n, wc_stream_t stream,
+            uint64_t probing_length)
+{
+    if (!p) return fail(WC_ERR_INVALID_ARGUMENT, "pipe is NULL");
+    int rc = check_table(t, 0x7);
+    if (rc) return rc;
+    if (n == 0) return WC_OK;
+    if (!h_keys) return fail(WC_ERR_INVALID_ARGUMENT, "keys_in is NULL");
+    if (insert && t->kind == 0 && !h_values) return fail(WC_ERR_INVALID_ARGUMENT, "values_in is NULL");
+    if (!insert && !h_out) return fail(WC_ERR_INVALID_ARGUMENT, "output is NULL");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const uint32_t kb = t->cfg.key_bytes;
+    const uint32_t vb = t->cfg.value_bytes;
+    const uint32_t ob = out_bytes_of(t);
+    /* sets write a flag for every key; single-value and counting tables
+     * write hits only, so a miss keeps the output's earlier content: copied
+     * in with the keys, or `miss_fill` */
+    const bool hits_only = !insert && t->kind != 1;
+    const int op = insert ? (t->kind == 2 ? kOpCount : kOpInsert) : kOpRetrieve;
+    const char *hk = static_cast<const char *>(h_keys);
+    const char *hv = static_cast<const char *>(h_values);
+    char *ho = static_cast<char *>(h_out);
+    std::vector<char> touched(p->depth, 0);
+    /* stream order: no copy of this call starts before the caller's
+     * earlier work on `stream` (which may have written the host inputs) */
+    WC_CUDA(cudaEventRecord(p->call_start, s));
+    WC_CUDA(cudaStreamWaitEvent(p->h2d, p->call_start, 0));
+    for (uint64_t off = 0; off < n; off += p->chunk) {
+        const uint64_t m = n - off < p->chunk ? n - off : p->chunk;
+        const uint32_t slot = p->next;
+        p->next = (p->next + 1) % p->depth;
+        char *dk = p->stage + size_t(slot) * p->chunk * 16;
+        char *dv = dk + p->chunk * 8;
+        if (p->used[slot]) WC_CUDA(cudaStreamWaitEvent(p->h2d, p->slot_free[slot], 0));
+        WC_CUDA(cudaMemcpyAsync(dk, hk + off * kb, m * kb, cudaMemcpyHostToDevice, p->h2d));
+        if (insert && t->kind == 0)
+            WC_CUDA(cudaMemcpyAsync(dv, hv + off * vb, m * vb, cudaMemcpyHostToDevice, p->h2d));
+        if (hits_only && !miss_fill)
+            WC_CUDA(cudaMemcpyAsync(dv, ho + off * ob, m * ob, cudaMemcpyHostToDevice, p->h2d));
+        WC_CUDA(cudaEventRecord(p->in_done[slot], p->h2d));
+        WC_CUDA(cudaStreamWaitEvent(s, p->in_done[slot], 0));
+        if (hits_only && miss_fill) {
+            uint32_t w[4];
+            if (ob == 4) {
+                std::memcpy(&w[0], miss_fill, 4);
+                w[1] = w[2] = w[3] = w[0];
+            } else {
+                std::memcpy(&w[0], miss_fill, 8);
+                w[2] = w[0];
+                w[3] = w[1];
+            }
+            uint32_t *fp = reinterpret_cast<uint32_t *>(dv);
+            uint64_t fn = m * ob / 4;
+            uint4 pat = make_uint4(w[0], w[1], w[2], w[3]);
+            void *fargs[] = {&fp, &fn, &pat};
+            const void *fk = reinterpret_cast<const void *>(fill_kernel<0>);
+            WC_CUDA(cudaLaunchKernel(fk, dim3(grid_for(fk, kBlock, fn / 4, kBlock)), dim3(kBlock),
+                                     fargs, 0, s));
+        }
+        rc = table_op(t, op, dk, insert ? dv : nullptr, insert ? nullptr : dv, m, stream,
+                      probing_length, nullptr, WC_HANDLER_NOTHING, 0);
+        if (rc) return rc;
+        if (insert) {
+            WC_CUDA(cudaEventRecord(p->slot_free[slot], s));
+        } else {
+            WC_CUDA(cudaEventRecord(p->kern_done[slot], s));
+            WC_CUDA(cudaStreamWaitEvent(p->d2h, p->kern_done[slot], 0));
+            WC_CUDA(cudaMemcpyAsync(ho + off * ob, dv, m * ob, cudaMemcpyDeviceToHost, p->d2h));
+            WC_CUDA(cudaEventRecord(p->slot_free[slot], p->d2h));
+        }
+        p->used[slot] = 1;
+        touched[slot] = 1;
+    }
+    /* the caller's stream passes this call only when every copy-out is done */
+    if (!insert)
+        for (uint32_t i = 0; i < p->depth; ++i)
+            if (touched[i]) WC_CUDA(cudaStreamWaitEvent(s, p->slot_free[i], 0));
+    return WC_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int wc_table_insert_host(wc_host_pipe *p, wc_table *t, const void *h_keys, const void *h_values,
+                         uint64_t num_in, wc_stream_t stream, uint64_t probing_length)
+{
+    return host_op(p, t, true, h_keys, h_values, nullptr, nullptr, num_in, stream, probing_length);
+}
+
+int wc_table_retrieve_host(wc_host_pipe *p, wc_table *t, const void *h_keys, uint64_t num_in,
+                           void *h_out, const void *miss_fill, wc_stream_t stream,
+                           uint64_t probing_length)
+{
+    return host_op(p, t, false, h_keys, nullptr, h_out, miss_fill, num_in, stream, probing_length);
+}
+
+} // extern "C"
+
+/* ------------------------------------------------------------------ */
 /* batches (wc_batch.cuh)                                                */
 /* ------------------------------------------------------------------ */
 
