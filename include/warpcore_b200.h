@@ -444,6 +444,14 @@ int wc_partition(const void *keys, const void *values, uint64_t n, uint32_t key_
                  uint32_t value_bytes, uint32_t num_parts, uint64_t salt, void *keys_out,
                  void *values_out, uint64_t *perm_out, uint64_t *counts_out,
                  uint64_t *scratch, wc_stream_t stream);
+/* The inverse step of a sharded retrieve: answer j, in the order
+ * wc_partition produced, goes back to input position perm[j].  Its value is
+ * written only if status[j] is 0 (a hit), as retrieve writes hits only; the
+ * status is written if status_out is not NULL.  Entries whose perm[j] is
+ * not below n are skipped.  Asynchronous on `stream`. */
+int wc_partition_restore(const void *values, const uint32_t *status, const uint64_t *perm,
+                         uint64_t n, uint32_t value_bytes, void *values_out,
+                         uint32_t *status_out, wc_stream_t stream);
 
 /* ------------------------------------------------------------------ */
 /* Counting without allocating                                          */

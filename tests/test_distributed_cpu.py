@@ -30,7 +30,8 @@ def _worker(rank, world, port, kb, errq):
         import sys
         sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
         from tests.partition_ref import OracleShard, cpu_partition
-        from warpcore_b200.distributed import DEFAULT_SALT, DistributedSingleValueHashTable
+        from warpcore_b200.distributed import (DEFAULT_SALT, DistributedSingleValueHashTable,
+                                               cpu_restore)
         udt = np.uint32 if kb == 4 else np.uint64
         sdt = np.int32 if kb == 4 else np.int64
         n = 3000
@@ -38,7 +39,8 @@ def _worker(rank, world, port, kb, errq):
         vals = o.gen_uniform(kb, world * n, 6)
         t = DistributedSingleValueHashTable(4 * world * n, key_bytes=kb,
                                             shard_factory=lambda cap: OracleShard(cap, kb),
-                                            partition_fn=cpu_partition(world, DEFAULT_SALT, kb))
+                                            partition_fn=cpu_partition(world, DEFAULT_SALT, kb),
+                                            restore_fn=cpu_restore)
         mine = slice(rank * n, (rank + 1) * n)
         t.insert(torch.from_numpy(allk[mine].view(sdt)), torch.from_numpy(vals[mine].view(sdt)))
         assert t.size() == world * n

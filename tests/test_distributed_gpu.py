@@ -95,3 +95,24 @@ def test_sharded_table_one_rank_nccl():
         assert t.size() == n - allk[:n][::2].size
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("vb", [4, 8])
+def test_partition_restore(vb):
+    from warpcore_b200.distributed import gpu_restore
+    n = 50021
+    rng = np.random.default_rng(7)
+    perm = rng.permutation(n).astype(np.int64)
+    vals = o.gen_uniform(vb, n, 71)
+    status = np.where(rng.random(n) < 0.6, 0, 32).astype(np.uint32)  # 0 = hit, 32 = key_not_found
+    init = o.gen_uniform(vb, n, 72)
+    out = dev(init)
+    st_out = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    gpu_restore(dev(vals), dev(status), torch.from_numpy(perm).cuda(), out, st_out)
+    want = init.copy()
+    hit = status == 0
+    want[perm[hit]] = vals[hit]
+    want_st = np.empty(n, dtype=np.uint32)
+    want_st[perm] = status
+    assert np.array_equal(host(out), want)
+    assert np.array_equal(host(st_out), want_st)

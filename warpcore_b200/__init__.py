@@ -203,6 +203,7 @@ SIGNATURES = {
     "wc_bloom_fpr": (_i, [_vp, _u64, ctypes.POINTER(ctypes.c_double)]),
     "wc_slots_size_noalloc": (_i, [_vp, _u64, _u32, _u32, _u64, _u64, _vp, _vp]),
     "wc_partition": (_i, [_vp, _vp, _u64, _u32, _u32, _u32, _u64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "wc_partition_restore": (_i, [_vp, _vp, _vp, _u64, _u32, _vp, _vp, _vp]),
     "wc_host_pipe_create": (_i, [_u64, _u32, _pp]),
     "wc_host_pipe_destroy": (_i, [_vp]),
     "wc_table_insert_host": (_i, [_vp, _vp, _vp, _vp, _u64, _vp, _u64]),

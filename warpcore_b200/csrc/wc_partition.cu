@@ -29,30 +29,56 @@ __host__ __device__ __forceinline__ uint32_t partition_owner(uint64_t key, uint6
     return uint32_t(((h >> 32) * uint64_t(parts)) >> 32);
 }
 
+/* Both passes walk tiles of kTile = 256 x kKeysPerThread keys; a thread
+ * holds key j of its tile at t0 + j * 256 + threadIdx.x, so every load and
+ * every store of one j is coalesced, and each thread has kKeysPerThread
+ * independent loads in flight. */
+constexpr int kPartThreads = 256;
+constexpr int kKeysPerThread = 8;
+constexpr uint64_t kTile = uint64_t(kPartThreads) * kKeysPerThread;
+
+/* warp-aggregated shared-memory increment of hist[owner] by the lanes that
+ * share `owner`; returns this lane's rank among them, offset by the old
+ * count.  owner >= parts (inactive lanes) takes no part. */
+__device__ __forceinline__ unsigned tile_rank(unsigned int *hist, uint32_t owner, uint32_t parts)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned peers = __match_any_sync(kFull, owner);
+    const int leader = __ffs(peers) - 1;
+    unsigned base = 0;
+    if (owner < parts && lane == leader) base = atomicAdd(&hist[owner], unsigned(__popc(peers)));
+    base = __shfl_sync(kFull, base, leader);
+    return base + unsigned(__popc(peers & ((1u << lane) - 1u)));
+}
+
 template <class K>
-__global__ void __launch_bounds__(256) partition_count_kernel(const K *keys, uint64_t n,
-                                                              uint32_t parts, uint64_t salt,
-                                                              unsigned long long *counts)
+__global__ void __launch_bounds__(kPartThreads) partition_count_kernel(const K *keys, uint64_t n,
+                                                                       uint32_t parts, uint64_t salt,
+                                                                       unsigned long long *counts)
 {
     /* The owner is held in a range-checked local and the increments are
-     * aggregated per warp, as in the scatter pass.  Written instead as one
-     * atomicAdd on hist[partition_owner(...)], this kernel counted every key
-     * in hist[0] on sm_100a (CUDA 12.9); the GPU test with one repeated key
-     * whose owner is not 0 guards against that. */
+     * aggregated per warp.  Written instead as one atomicAdd on
+     * hist[partition_owner(...)], this kernel counted every key in hist[0]
+     * on sm_100a (CUDA 12.9); the GPU test with one repeated key whose owner
+     * is not 0 guards against that. */
     __shared__ unsigned int hist[WC_PARTITION_MAX_PARTS];
     for (uint32_t p = threadIdx.x; p < parts; p += blockDim.x) hist[p] = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-    const uint64_t start = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    const uint64_t rounds = (n + stride - 1) / stride;
-    for (uint64_t r = 0; r < rounds; ++r) {
-        const uint64_t i = start + r * stride;
-        const bool active = i < n;
-        const K k = active ? keys[i] : K(0);
-        const uint32_t owner = active ? partition_owner(uint64_t(k), salt, parts) : 0xFFFFFFFFu;
-        const unsigned peers = __match_any_sync(kFull, owner);
-        if (owner < parts && lane == __ffs(peers) - 1) atomicAdd(&hist[owner], unsigned(__popc(peers)));
+    const uint64_t ntiles = (n + kTile - 1) / kTile;
+    for (uint64_t tb = blockIdx.x; tb < ntiles; tb += gridDim.x) {
+        const uint64_t t0 = tb * kTile;
+        K k[kKeysPerThread];
+#pragma unroll
+        for (int j = 0; j < kKeysPerThread; ++j) {
+            const uint64_t i = t0 + uint64_t(j) * kPartThreads + threadIdx.x;
+            k[j] = i < n ? keys[i] : K(0);
+        }
+#pragma unroll
+        for (int j = 0; j < kKeysPerThread; ++j) {
+            const uint64_t i = t0 + uint64_t(j) * kPartThreads + threadIdx.x;
+            const uint32_t owner = i < n ? partition_owner(uint64_t(k[j]), salt, parts) : 0xFFFFFFFFu;
+            tile_rank(hist, owner, parts);
+        }
     }
     __syncthreads();
     for (uint32_t p = threadIdx.x; p < parts; p += blockDim.x)
@@ -75,36 +101,75 @@ __global__ void partition_scan_kernel(const unsigned long long *counts, uint32_t
     if (threadIdx.x == 0) *dropped = 0;
 }
 
+/* A tile ranks its keys per owner in shared memory, then claims one range
+ * per owner with a single global atomicAdd on that owner's cursor; the
+ * keys of one owner in a tile land in consecutive positions. */
 template <class K, class V>
-__global__ void __launch_bounds__(256) partition_scatter_kernel(
+__global__ void __launch_bounds__(kPartThreads) partition_scatter_kernel(
     const K *keys, const V *values, uint64_t n, uint32_t parts, uint64_t salt,
     const unsigned long long *offsets, unsigned long long *cursors, K *keys_out, V *values_out,
     unsigned long long *perm_out, unsigned long long *dropped)
 {
-    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-    const int lane = threadIdx.x & 31;
-    const uint64_t start = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    const uint64_t rounds = (n + stride - 1) / stride;
-    for (uint64_t r = 0; r < rounds; ++r) {
-        const uint64_t i = start + r * stride;
-        const bool active = i < n;
-        const K k = active ? keys[i] : K(0);
-        const uint32_t owner = active ? partition_owner(uint64_t(k), salt, parts) : 0xFFFFFFFFu;
-        const unsigned peers = __match_any_sync(kFull, owner);
-        const int leader = __ffs(peers) - 1;
-        unsigned long long base = 0;
-        if (active && lane == leader) base = atomicAdd(&cursors[owner], (unsigned long long)__popc(peers));
-        base = __shfl_sync(kFull, base, leader);
-        if (active) {
-            const uint64_t pos = offsets[owner] + base + __popc(peers & ((1u << lane) - 1u));
-            if (pos < n) {
-                keys_out[pos] = k;
-                if (values) values_out[pos] = values[i];
-                perm_out[pos] = i;
-            } else {
-                atomicAdd(dropped, 1ull);
+    __shared__ unsigned int tile_cnt[WC_PARTITION_MAX_PARTS];
+    __shared__ unsigned long long tile_base[WC_PARTITION_MAX_PARTS];
+    const uint64_t ntiles = (n + kTile - 1) / kTile;
+    for (uint64_t tb = blockIdx.x; tb < ntiles; tb += gridDim.x) {
+        for (uint32_t p = threadIdx.x; p < parts; p += blockDim.x) tile_cnt[p] = 0;
+        __syncthreads();
+        const uint64_t t0 = tb * kTile;
+        K k[kKeysPerThread];
+        uint32_t own[kKeysPerThread];
+        unsigned rank[kKeysPerThread];
+#pragma unroll
+        for (int j = 0; j < kKeysPerThread; ++j) {
+            const uint64_t i = t0 + uint64_t(j) * kPartThreads + threadIdx.x;
+            k[j] = i < n ? keys[i] : K(0);
+        }
+#pragma unroll
+        for (int j = 0; j < kKeysPerThread; ++j) {
+            const uint64_t i = t0 + uint64_t(j) * kPartThreads + threadIdx.x;
+            own[j] = i < n ? partition_owner(uint64_t(k[j]), salt, parts) : 0xFFFFFFFFu;
+            rank[j] = tile_rank(tile_cnt, own[j], parts);
+        }
+        __syncthreads();
+        for (uint32_t p = threadIdx.x; p < parts; p += blockDim.x) {
+            const unsigned c = tile_cnt[p];
+            tile_base[p] = c ? atomicAdd(&cursors[p], (unsigned long long)c) : 0ull;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kKeysPerThread; ++j) {
+            const uint64_t i = t0 + uint64_t(j) * kPartThreads + threadIdx.x;
+            if (own[j] < parts) {
+                const uint64_t pos = offsets[own[j]] + tile_base[own[j]] + rank[j];
+                if (pos < n) {
+                    keys_out[pos] = k[j];
+                    if (values) values_out[pos] = values[i];
+                    perm_out[pos] = i;
+                } else {
+                    atomicAdd(dropped, 1ull);
+                }
             }
         }
+        __syncthreads(); /* tile_cnt / tile_base are reused by the next tile */
+    }
+}
+
+/* the inverse step of a sharded retrieve: answer j (in owner order) goes
+ * back to input position perm[j]; its value only on a hit (status 0), as
+ * the reference's retrieve writes hits only */
+template <class V>
+__global__ void __launch_bounds__(256) partition_restore_kernel(
+    const V *values, const uint32_t *status, const unsigned long long *perm, uint64_t n,
+    V *values_out, uint32_t *status_out)
+{
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const unsigned long long p = perm[j];
+        if (p >= n) continue; /* not a permutation of [0, n): nothing to write */
+        const uint32_t st = status[j];
+        if (st == 0) values_out[p] = values[j];
+        if (status_out) status_out[p] = st;
     }
 }
 
@@ -146,7 +211,7 @@ extern "C" int wc_partition(const void *keys, const void *values, uint64_t n, ui
     }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
-    uint64_t need = (n + 255) / 256;
+    const uint64_t need = (n + kTile - 1) / kTile; /* one block per tile, up to 4 per SM */
     const unsigned grid = unsigned(need < uint64_t(sms) * 4 ? (need ? need : 1) : uint64_t(sms) * 4);
     auto *po = reinterpret_cast<unsigned long long *>(perm_out);
     auto launched = [&]() {
@@ -155,26 +220,61 @@ extern "C" int wc_partition(const void *keys, const void *values, uint64_t n, ui
         return e == cudaSuccess;
     };
     if (key_bytes == 4) {
-        partition_count_kernel<uint32_t><<<grid, 256, 0, s>>>(
+        partition_count_kernel<uint32_t><<<grid, kPartThreads, 0, s>>>(
             reinterpret_cast<const uint32_t *>(keys), n, num_parts, salt, counts);
         if (!launched()) return WC_ERR_CUDA;
         partition_scan_kernel<<<1, 256, 0, s>>>(counts, num_parts, offsets, cursors, dropped);
         if (!launched()) return WC_ERR_CUDA;
-        partition_scatter_kernel<uint32_t, uint32_t><<<grid, 256, 0, s>>>(
+        partition_scatter_kernel<uint32_t, uint32_t><<<grid, kPartThreads, 0, s>>>(
             reinterpret_cast<const uint32_t *>(keys), reinterpret_cast<const uint32_t *>(values), n,
             num_parts, salt, offsets, cursors, reinterpret_cast<uint32_t *>(keys_out),
             reinterpret_cast<uint32_t *>(values_out), po, dropped);
     } else {
-        partition_count_kernel<unsigned long long><<<grid, 256, 0, s>>>(
+        partition_count_kernel<unsigned long long><<<grid, kPartThreads, 0, s>>>(
             reinterpret_cast<const unsigned long long *>(keys), n, num_parts, salt, counts);
         if (!launched()) return WC_ERR_CUDA;
         partition_scan_kernel<<<1, 256, 0, s>>>(counts, num_parts, offsets, cursors, dropped);
         if (!launched()) return WC_ERR_CUDA;
-        partition_scatter_kernel<unsigned long long, unsigned long long><<<grid, 256, 0, s>>>(
+        partition_scatter_kernel<unsigned long long, unsigned long long><<<grid, kPartThreads, 0, s>>>(
             reinterpret_cast<const unsigned long long *>(keys),
             reinterpret_cast<const unsigned long long *>(values), n, num_parts, salt, offsets,
             cursors, reinterpret_cast<unsigned long long *>(keys_out),
             reinterpret_cast<unsigned long long *>(values_out), po, dropped);
     }
     return launched() ? WC_OK : WC_ERR_CUDA;
+}
+
+extern "C" int wc_partition_restore(const void *values, const uint32_t *status,
+                                    const uint64_t *perm, uint64_t n, uint32_t value_bytes,
+                                    void *values_out, uint32_t *status_out, wc_stream_t stream)
+{
+    if (n == 0) return WC_OK;
+    if (value_bytes != 4 && value_bytes != 8) {
+        set_last_error("value_bytes must be 4 or 8");
+        return WC_ERR_UNSUPPORTED;
+    }
+    if (!values || !status || !perm || !values_out) {
+        set_last_error("NULL buffer");
+        return WC_ERR_INVALID_ARGUMENT;
+    }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    const uint64_t need = (n + 255) / 256;
+    const unsigned grid = unsigned(need < uint64_t(sms) * 8 ? need : uint64_t(sms) * 8);
+    const auto *pp = reinterpret_cast<const unsigned long long *>(perm);
+    if (value_bytes == 4)
+        partition_restore_kernel<uint32_t><<<grid, 256, 0, s>>>(
+            reinterpret_cast<const uint32_t *>(values), status, pp, n,
+            reinterpret_cast<uint32_t *>(values_out), status_out);
+    else
+        partition_restore_kernel<unsigned long long><<<grid, 256, 0, s>>>(
+            reinterpret_cast<const unsigned long long *>(values), status, pp, n,
+            reinterpret_cast<unsigned long long *>(values_out), status_out);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_last_error(cudaGetErrorString(e));
+        return WC_ERR_CUDA;
+    }
+    return WC_OK;
 }

@@ -16,10 +16,10 @@ runs these steps:
 Every rank must call every operation, in the same order (collectives).
 `size()` is the sum over shards.
 
-`partition_fn` and `shard_factory` exist so that the host logic can be
-tested with the gloo backend on CPU, against the CPU oracle. On a GPU the
-defaults are the CUDA partition kernel and a warpcore_b200 table. There is
-no fallback between the two.
+`partition_fn`, `restore_fn` and `shard_factory` exist so that the host
+logic can be tested with the gloo backend on CPU, against the CPU oracle.
+On a GPU the defaults are the CUDA partition and restore kernels and a
+warpcore_b200 table. There is no fallback between the two.
 """
 import ctypes
 
@@ -58,9 +58,29 @@ def gpu_partition(keys, values, parts, salt, key_bytes):
     return keys_out, values_out, perm, host_buf[:parts]
 
 
+def gpu_restore(values, status, perm, values_out, status_out=None):
+    """put answers (in owner order) back at their input positions on the
+    GPU: values on hits only, statuses if status_out is given"""
+    n = perm.numel()
+    if n == 0:
+        return
+    wc._check(wc.lib().wc_partition_restore(
+        values.data_ptr(), status.data_ptr(), perm.data_ptr(), n, values.element_size(),
+        values_out.data_ptr(), status_out.data_ptr() if status_out is not None else None,
+        torch.cuda.current_stream(values.device).cuda_stream))
+
+
+def cpu_restore(values, status, perm, values_out, status_out=None):
+    """the same step with torch indexing, for CPU tensors"""
+    hit = status == 0
+    values_out[perm[hit]] = values[hit]
+    if status_out is not None:
+        status_out[perm] = status
+
+
 class DistributedSingleValueHashTable:
     def __init__(self, min_capacity, key_bytes=4, seed=wc.DEFAULT_SEED, group=None,
-                 salt=DEFAULT_SALT, shard_factory=None, partition_fn=None):
+                 salt=DEFAULT_SALT, shard_factory=None, partition_fn=None, restore_fn=None):
         self.group = group
         self.world = dist.get_world_size(group)
         self.rank = dist.get_rank(group)
@@ -73,6 +93,7 @@ class DistributedSingleValueHashTable:
             self.shard = shard_factory(shard_cap)
         self._partition = partition_fn or (
             lambda k, v: gpu_partition(k, v, self.world, self.salt, self.key_bytes))
+        self._restore = restore_fn or gpu_restore
 
     # -- exchange helpers --------------------------------------------------
     def _counts(self, send_counts, device):
@@ -101,16 +122,15 @@ class DistributedSingleValueHashTable:
         k, _, perm, send = self._partition(keys, None)
         recv = self._counts(send, keys.device)
         rk = self._a2a(k, send, recv)
-        local_out = torch.zeros(rk.numel(), dtype=values_out.dtype, device=keys.device)
-        local_st = torch.zeros(rk.numel(), dtype=torch.int32, device=keys.device)
+        # the shard writes every status and the values of hits; the restore
+        # step reads a value only where the status is 0
+        local_out = torch.empty(rk.numel(), dtype=values_out.dtype, device=keys.device)
+        local_st = torch.empty(rk.numel(), dtype=torch.int32, device=keys.device)
         if rk.numel():
             self.shard.retrieve(rk, local_out, status_out=local_st)
         back_v = self._a2a(local_out, recv, send)
         back_s = self._a2a(local_st, recv, send)
-        hit = back_s == 0
-        values_out[perm[hit]] = back_v[hit]
-        if status_out is not None:
-            status_out[perm] = back_s
+        self._restore(back_v, back_s, perm, values_out, status_out)
         return status_out
 
     def erase(self, keys):
