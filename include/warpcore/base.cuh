@@ -359,6 +359,7 @@ inline b200::TableView view_from(const wc_table_info &inf)
     b200::TableView v{};
     v.slots = inf.slots;
     v.status = inf.status;
+    v.fps = inf.fingerprints;
     v.num_buckets = inf.num_buckets;
     v.seed = inf.seed;
     v.empty_key = inf.empty_key;

@@ -159,6 +159,7 @@ __host__ __device__ __forceinline__ uint64_t fast_mod(uint64_t x, uint64_t d, ui
 struct TableView {
     void *slots;
     uint32_t *status;
+    unsigned char *fps;   /* one fingerprint byte per slot, or NULL */
     uint64_t num_buckets; /* capacity / cg_size; prime under the capacity rule */
     uint64_t seed;
     uint64_t empty_key;
@@ -196,6 +197,31 @@ __host__ __device__ __forceinline__ uint64_t probe_next(const TableView &t,
     if (b >= t.num_buckets) b -= t.num_buckets;
     if (t.probing == kProbeQuadratic) step++;
     return b;
+}
+
+/* ------------------------------------------------------------------ */
+/* fingerprints                                                          */
+/* ------------------------------------------------------------------ */
+
+/* A table may keep one byte per slot beside the slot array: 0 for an empty
+ * slot, 1 for a tombstone, 2..255 for a key (a multiplicative hash of the
+ * key, independent of the probing hashers).  A bucket's fingerprints are
+ * cg_size bytes, so probing can read them instead of the whole window and
+ * read a slot only where the fingerprint matches.  Every write of a slot
+ * key (claim, erase) writes its fingerprint after it, when the table has
+ * them. */
+enum : uint32_t { kFpEmpty = 0, kFpTomb = 1 };
+
+template <class K>
+__host__ __device__ __forceinline__ uint32_t fingerprint(K key)
+{
+    const uint64_t h = (uint64_t(key) * 0x9E3779B97F4A7C15ull) >> 56; /* 0..255 */
+    return uint32_t((h * 254u) >> 8) + 2u;                             /* 2..255 */
+}
+
+__device__ __forceinline__ void fp_store(const TableView &t, uint64_t slot, uint32_t fp)
+{
+    if (t.fps) *reinterpret_cast<volatile unsigned char *>(t.fps + slot) = (unsigned char)fp;
 }
 
 /* windows the reference visits for a probing length: SDIV(pl, cg) windows

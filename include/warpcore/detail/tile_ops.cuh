@@ -49,7 +49,10 @@ __device__ uint32_t tile_modify(const TableView &t, const Tile &g, typename L::k
             if (hit) {
                 const unsigned leader = __ffs(hit) - 1;
                 if (op == 3) {
-                    if (r == leader) store_key<L>(sp, tomb);
+                    if (r == leader) {
+                        store_key<L>(sp, tomb);
+                        fp_store(t, b * W + r, kFpTomb);
+                    }
                     st = kStNone;
                 } else {
                     st = kStDuplicateKey;
@@ -76,6 +79,7 @@ __device__ uint32_t tile_modify(const TableView &t, const Tile &g, typename L::k
                     K old_key;
                     const V payload = op == 1 ? V(1) : val;
                     if (claim_slot<L>(sp, empty, key, payload, old_key)) {
+                        fp_store(t, b * W + r, fingerprint(key));
                         outcome = 1;
                     } else if (old_key == key) {
                         outcome = 2;

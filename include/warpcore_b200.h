@@ -108,6 +108,9 @@ typedef struct wc_table_info {
     void *slots;            /* device pointer to the slot array */
     uint32_t *status;       /* device pointer to the table's Status word */
     int is_initialized;
+    unsigned char *fingerprints; /* device pointer to one byte per slot, or NULL:
+                                    0 empty, 1 tombstone, else the key's
+                                    fingerprint; writers of slot keys keep it */
 } wc_table_info;
 
 typedef struct wc_table wc_table;
@@ -300,6 +303,32 @@ int wc_table_insert_host(wc_host_pipe *p, wc_table *t, const void *h_keys, const
 int wc_table_retrieve_host(wc_host_pipe *p, wc_table *t, const void *h_keys, uint64_t num_in,
                            void *h_out, const void *miss_fill, wc_stream_t stream,
                            uint64_t probing_length);
+
+/* ------------------------------------------------------------------ */
+/* Fingerprints (no counterpart in the reference)                        */
+/* ------------------------------------------------------------------ */
+
+/* A table may keep one fingerprint byte per slot, so that probing reads a
+ * bucket's cg_size bytes instead of its whole window and reads a slot only
+ * where the fingerprint matches.  Results are the same either way.
+ * AUTO (default): tables whose slot array is larger than L2; ALWAYS /
+ * NEVER: every table.  Applies to tables created after the call.  The
+ * environment variable WARPCORE_B200_FINGERPRINTS (auto, always, never)
+ * sets the mode before the first call. */
+#define WC_FINGERPRINTS_AUTO 0
+#define WC_FINGERPRINTS_ALWAYS 1
+#define WC_FINGERPRINTS_NEVER 2
+int wc_fingerprint_policy(int mode, int *previous);
+/* Which operations read fingerprints first on tables that have them: bit
+ * 0 insert, 1 counting insert, 2 retrieve, 3 erase (default: all four;
+ * an operation whose bit is clear probes whole windows and keeps the
+ * fingerprints up to date).  Bit 4: a fingerprint-first insert loads the
+ * slot it is about to claim before the compare-and-swap.  Bit 5: never
+ * replace a large insert (more than 1/8 of a table whose fingerprints
+ * exceed half of L2) by a whole-window insert without fingerprint writes
+ * followed by a streaming rebuild of all fingerprints, which is the
+ * default. */
+int wc_fingerprint_ops(uint32_t op_mask, uint32_t *previous);
 
 /* ------------------------------------------------------------------ */
 /* L2 persistence for tables that fit in L2 (no counterpart in the       */

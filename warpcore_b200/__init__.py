@@ -21,7 +21,8 @@ from ._status import Status  # noqa: F401
 __all__ = [
     "Status", "SingleValueHashTable", "HashSet", "CountingHashTable",
     "BloomFilter", "lib", "valid_capacity", "WarpcoreError", "set_l2_persistence",
-    "HostPipe",
+    "HostPipe", "set_fingerprint_policy", "set_fingerprint_ops", "FINGERPRINTS_AUTO", "FINGERPRINTS_ALWAYS",
+    "FINGERPRINTS_NEVER",
     "HASH_MURMUR", "HASH_NVIDIA", "HASH_MUELLER", "HASH_IDENTITY32",
     "HASH_IDENTITY64", "PROBING_DOUBLE", "PROBING_LINEAR",
     "PROBING_QUADRATIC", "HANDLER_NOTHING", "HANDLER_STATUS",
@@ -78,6 +79,7 @@ class TableInfo(ctypes.Structure):
         ("slots", ctypes.c_void_p),
         ("status", ctypes.c_void_p),
         ("is_initialized", ctypes.c_int),
+        ("fingerprints", ctypes.c_void_p),
     ]
 
 
@@ -209,6 +211,8 @@ SIGNATURES = {
     "wc_table_insert_host": (_i, [_vp, _vp, _vp, _vp, _u64, _vp, _u64]),
     "wc_table_retrieve_host": (_i, [_vp, _vp, _vp, _u64, _vp, _vp, _vp, _u64]),
     "wc_l2_persistence": (_i, [_i, ctypes.POINTER(ctypes.c_int)]),
+    "wc_fingerprint_policy": (_i, [_i, ctypes.POINTER(ctypes.c_int)]),
+    "wc_fingerprint_ops": (_i, [_u32, ctypes.POINTER(ctypes.c_uint32)]),
     "wc_table_l2_window": (_i, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(ctypes.c_float)]),
     "wc_tune_set": (_i, [_u32, _i, _u32, _u32, _u32, _u32]),
     "wc_tune_reset": (_i, []),
@@ -240,6 +244,7 @@ def lib():
         _load_tuning(l)
         if os.environ.get("WARPCORE_B200_L2_PERSIST", "1") == "0":
             l.wc_l2_persistence(0, None)
+
     return _lib
 
 
@@ -263,6 +268,28 @@ def _check(rc):
 def valid_capacity(min_capacity, cg_size):
     """The reference's capacity rule (base.cuh:27-34)."""
     return lib().wc_valid_capacity(int(min_capacity), int(cg_size))
+
+
+FINGERPRINTS_AUTO, FINGERPRINTS_ALWAYS, FINGERPRINTS_NEVER = 0, 1, 2
+_FP_NAMES = {"auto": FINGERPRINTS_AUTO, "always": FINGERPRINTS_ALWAYS, "never": FINGERPRINTS_NEVER}
+
+
+def set_fingerprint_policy(mode):
+    """Which tables created from now on keep one fingerprint byte per slot:
+    "auto" (slot arrays larger than L2), "always" or "never" (or the
+    FINGERPRINTS_* constants); returns the previous mode as a constant."""
+    m = _FP_NAMES[mode] if isinstance(mode, str) else int(mode)
+    prev = ctypes.c_int(0)
+    _check(lib().wc_fingerprint_policy(m, ctypes.byref(prev)))
+    return prev.value
+
+
+def set_fingerprint_ops(op_mask):
+    """bit mask of operations (1 insert, 2 counting insert, 4 retrieve,
+    8 erase) that read fingerprints first; returns the previous mask"""
+    prev = ctypes.c_uint32(0)
+    _check(lib().wc_fingerprint_ops(int(op_mask), ctypes.byref(prev)))
+    return prev.value
 
 
 def set_l2_persistence(enable):
@@ -387,6 +414,10 @@ class _Table:
         out = _u64()
         _check(lib().wc_table_size(self._h, _stream(stream), ctypes.byref(out)))
         return out.value
+
+    @property
+    def has_fingerprints(self):
+        return bool(self.info().fingerprints)
 
     def l2_window(self):
         """(bytes, hit ratio) of the L2 persistence window this table's

@@ -244,6 +244,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs a)
                 unsigned char *const sp = reinterpret_cast<unsigned char *>(d.t.slots) +
                                           (bucket * W + uint64_t(s)) * SB;
                 if (cas_old == empty && cas_old_payload == claim_expect) {
+                    fp_store(d.t, bucket * W + uint64_t(s), fingerprint(key));
                     st = kStNone;
                     pending = false;
                 } else if (cas_old == key) {

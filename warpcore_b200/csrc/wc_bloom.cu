@@ -44,6 +44,17 @@ CountKernel count_kernel(int layout)
     }
 }
 
+RebuildKernel fp_rebuild_kernel_ptr(int layout)
+{
+    switch (layout) {
+    case kLayoutKV32: return fp_rebuild_kernel<LayoutKV32>;
+    case kLayoutKV64: return fp_rebuild_kernel<LayoutKV64>;
+    case kLayoutSet32: return fp_rebuild_kernel<LayoutSet32>;
+    case kLayoutSet64: return fp_rebuild_kernel<LayoutSet64>;
+    default: return nullptr;
+    }
+}
+
 DumpKernel dump_kernel_ptr(int layout)
 {
     switch (layout) {

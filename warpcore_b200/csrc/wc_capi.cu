@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -125,6 +126,45 @@ const DeviceProps &device_props()
  * cudaLimitPersistingL2CacheSize, made once per device when the first
  * eligible table is created; it ends with the context. */
 std::atomic<int> g_l2_mode{1};
+
+/* Fingerprints (one byte per slot, b200_core.cuh) pay off where probing
+ * reads DRAM: slot arrays larger than L2.  WC_FINGERPRINTS_AUTO gives them
+ * to those tables only; ALWAYS / NEVER override for tables created later. */
+std::atomic<int> g_fp_mode{-1}; /* -1: not yet read from the environment */
+
+/* Operations (bit kOp*) that run the fingerprint-first kernel on tables
+ * with fingerprints; the others run the whole-window kernel, which keeps
+ * the fingerprints up to date.  Bit 4 makes the fingerprint kernel load a
+ * claim's slot before its compare-and-swap.  Measured on B200 with u64
+ * pairs at load 0.9, 2^27 keys: retrieve 13.0 -> 20.5 G/s on fingerprints;
+ * the window insert slows down on a fingerprint table (9.1 G/s, its
+ * fingerprint byte writes miss L2) more than the fingerprint insert does
+ * (11.7 G/s), so every operation reads fingerprints first. */
+std::atomic<uint32_t> g_fp_ops{0xFu};
+
+int fp_mode()
+{
+    int m = g_fp_mode.load(std::memory_order_relaxed);
+    if (m < 0) {
+        /* WARPCORE_B200_FINGERPRINTS = auto | always | never */
+        const char *e = std::getenv("WARPCORE_B200_FINGERPRINTS");
+        int want = WC_FINGERPRINTS_AUTO;
+        if (e && std::strcmp(e, "always") == 0) want = WC_FINGERPRINTS_ALWAYS;
+        if (e && std::strcmp(e, "never") == 0) want = WC_FINGERPRINTS_NEVER;
+        int expect = -1;
+        g_fp_mode.compare_exchange_strong(expect, want);
+        m = g_fp_mode.load(std::memory_order_relaxed);
+    }
+    return m;
+}
+
+bool want_fingerprints(uint64_t slot_bytes_total)
+{
+    const int m = fp_mode();
+    if (m == WC_FINGERPRINTS_ALWAYS) return true;
+    if (m == WC_FINGERPRINTS_NEVER) return false;
+    return slot_bytes_total > uint64_t(device_props().l2_bytes);
+}
 
 size_t l2_setaside(int dev)
 {
@@ -300,6 +340,7 @@ struct wc_table {
     int device = 0;
     uint64_t keys_inserted = 0; /* since init: an upper bound of size(), for tuning */
     L2Window l2;                /* access-policy window over the slots, if they fit */
+    unsigned char *fps = nullptr; /* one fingerprint byte per slot, or NULL */
 };
 
 struct wc_bloom {
@@ -322,6 +363,7 @@ TableView view_of(const wc_table *t)
     TableView v;
     v.slots = t->slots;
     v.status = t->status;
+    v.fps = t->fps;
     v.num_buckets = t->num_buckets;
     v.seed = t->seed;
     v.empty_key = t->cfg.empty_key;
@@ -413,17 +455,19 @@ int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, ui
 
     /* the reference checks free memory before allocating (storage.cuh:464-473) */
     const uint64_t bytes = cap * t->slot_bytes;
+    const uint64_t fp_bytes = want_fingerprints(bytes) ? cap : 0;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
         delete t;
         return cuda_fail(cudaGetLastError(), "cudaMemGetInfo");
     }
-    if (bytes + 4096 > free_b) {
+    if (bytes + fp_bytes + 4096 > free_b) {
         delete t;
         return fail(WC_ERR_OUT_OF_MEMORY, "table needs %llu bytes, %llu free",
-                    (unsigned long long)bytes, (unsigned long long)free_b);
+                    (unsigned long long)(bytes + fp_bytes), (unsigned long long)free_b);
     }
     cudaError_t e = cudaMalloc(&t->slots, bytes);
+    if (e == cudaSuccess && fp_bytes) e = cudaMalloc(&t->fps, fp_bytes);
     if (e == cudaSuccess) {
         void *aux = nullptr;
         e = cudaMalloc(&aux, 256);
@@ -434,6 +478,7 @@ int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, ui
     }
     if (e != cudaSuccess) {
         if (t->slots) cudaFree(t->slots);
+        if (t->fps) cudaFree(t->fps);
         delete t;
         return cuda_fail(e, "cudaMalloc");
     }
@@ -463,14 +508,26 @@ int check_table(const wc_table *t, int kind_mask)
     return WC_OK;
 }
 
-TableKernel pick_table_kernel(const wc_table *t, int op)
+TableKernel pick_window_kernel(const wc_table *t, int op)
 {
     const int W = int(t->cfg.cg_size);
     switch (t->layout) {
-    case kLayoutKV32: return table_kernel_kv32(W, op);
-    case kLayoutKV64: return table_kernel_kv64(W, op);
-    case kLayoutSet32: return table_kernel_set32(W, op);
-    default: return table_kernel_set64(W, op);
+    case kLayoutKV32: return table_kernel_kv32(W, op, false);
+    case kLayoutKV64: return table_kernel_kv64(W, op, false);
+    case kLayoutSet32: return table_kernel_set32(W, op, false);
+    default: return table_kernel_set64(W, op, false);
+    }
+}
+
+TableKernel pick_table_kernel(const wc_table *t, int op)
+{
+    const int W = int(t->cfg.cg_size);
+    const bool fp = t->fps != nullptr && ((g_fp_ops.load(std::memory_order_relaxed) >> op) & 1u);
+    switch (t->layout) {
+    case kLayoutKV32: return table_kernel_kv32(W, op, fp);
+    case kLayoutKV64: return table_kernel_kv64(W, op, fp);
+    case kLayoutSet32: return table_kernel_set32(W, op, fp);
+    default: return table_kernel_set64(W, op, fp);
     }
 }
 
@@ -485,10 +542,18 @@ int table_op(wc_table *t, int op, const void *keys, const void *values, void *ou
     if (op == kOpInsert && t->kind == 0 && !values)
         return fail(WC_ERR_INVALID_ARGUMENT, "values_in is NULL");
     if (op == kOpRetrieve && !out) return fail(WC_ERR_INVALID_ARGUMENT, "output is NULL");
-    TableKernel k = pick_table_kernel(t, op);
+    /* A large insert into a table whose fingerprints exceed half of L2 runs
+     * the whole-window kernel without fingerprint writes and then rebuilds
+     * all fingerprints in one streaming pass (see fp_rebuild_kernel). */
+    const bool rebuild = t->fps && (op == kOpInsert || op == kOpCount) &&
+                         n * 8 > t->capacity &&
+                         t->capacity > uint64_t(device_props().l2_bytes) / 2 &&
+                         (g_fp_ops.load(std::memory_order_relaxed) & 0x20u) == 0;
+    TableKernel k = rebuild ? pick_window_kernel(t, op) : pick_table_kernel(t, op);
     if (!k) return fail(WC_ERR_UNSUPPORTED, "no kernel for this configuration");
     TableOpArgs a;
     a.t = view_of(t);
+    if (rebuild) a.t.fps = nullptr; /* the window kernel writes no fingerprints */
     a.keys = keys;
     a.values = values;
     a.out = out;
@@ -498,6 +563,7 @@ int table_op(wc_table *t, int op, const void *keys, const void *values, void *ou
     a.bool_mask = (~ignore) ^ 0xFFFu; /* ~Status(Ignore), status.cuh:142-146 */
     a.handler = handler;
     a.is_set = t->kind == 1;
+    a.flags = (g_fp_ops.load(std::memory_order_relaxed) & 0x10u) ? kFlagPreloadClaim : 0u;
     /* launch geometry: the tuned entry for this key width, operation, load
      * and batch size, else 256 threads and the occupancy limit */
     const double lf = t->capacity ? double(t->keys_inserted) / double(t->capacity) : 0.0;
@@ -512,6 +578,17 @@ int table_op(wc_table *t, int op, const void *keys, const void *values, void *ou
     void *args[] = {&a};
     WC_CUDA(launch_in_window(kfn, grid, unsigned(block), args,
                              reinterpret_cast<cudaStream_t>(stream), t->l2));
+    if (rebuild) {
+        const RebuildKernel rk = fp_rebuild_kernel_ptr(t->layout);
+        const void *rfn = reinterpret_cast<const void *>(rk);
+        const unsigned rgrid = grid_for(rfn, kBlock, t->capacity * t->slot_bytes / 64 + 1, kBlock);
+        const void *sl = t->slots;
+        uint64_t cap = t->capacity, em = t->cfg.empty_key, tb = t->cfg.tombstone_key;
+        unsigned char *fp = t->fps;
+        void *rargs[] = {&sl, &cap, &em, &tb, &fp};
+        WC_CUDA(cudaLaunchKernel(rfn, dim3(rgrid), dim3(kBlock), rargs, 0,
+                                 reinterpret_cast<cudaStream_t>(stream)));
+    }
     if (op == kOpInsert || op == kOpCount) t->keys_inserted += n;
     return WC_OK;
 }
@@ -581,6 +658,7 @@ int wc_table_destroy(wc_table *t)
 {
     if (!t) return WC_OK;
     if (t->slots) cudaFree(t->slots);
+    if (t->fps) cudaFree(t->fps);
     if (t->status) cudaFree(t->status);
     l2_window_release(t->l2);
     delete t;
@@ -596,6 +674,7 @@ int wc_table_init(wc_table *t, uint64_t seed, wc_stream_t stream)
     t->seed = seed & key_mask(t->cfg.key_bytes);
     int rc = fill_slots(t, s);
     if (rc) return rc;
+    if (t->fps) WC_CUDA(cudaMemsetAsync(t->fps, kFpEmpty, t->capacity, s));
     WC_CUDA(cudaMemsetAsync(t->status, 0, sizeof(uint32_t), s));
     WC_CUDA(cudaStreamSynchronize(s));
     t->initialized = true;
@@ -771,10 +850,29 @@ int wc_table_get_info(const wc_table *t, wc_table_info *info)
     info->empty_key = t->cfg.empty_key;
     info->tombstone_key = t->cfg.tombstone_key;
     info->max_count = t->max_count;
-    info->bytes_total = t->capacity * t->slot_bytes + 256;
+    info->bytes_total = t->capacity * t->slot_bytes + 256 + (t->fps ? t->capacity : 0);
     info->slots = t->slots;
     info->status = t->status;
     info->is_initialized = t->initialized ? 1 : 0;
+    info->fingerprints = t->fps;
+    return WC_OK;
+}
+
+int wc_fingerprint_ops(uint32_t op_mask, uint32_t *previous)
+{
+    const uint32_t prev = g_fp_ops.exchange(op_mask & 0x3Fu);
+    if (previous) *previous = prev;
+    return WC_OK;
+}
+
+int wc_fingerprint_policy(int mode, int *previous)
+{
+    if (mode != WC_FINGERPRINTS_AUTO && mode != WC_FINGERPRINTS_ALWAYS &&
+        mode != WC_FINGERPRINTS_NEVER)
+        return fail(WC_ERR_INVALID_ARGUMENT, "unknown fingerprint policy %d", mode);
+    const int prev = fp_mode();
+    g_fp_mode.store(mode);
+    if (previous) *previous = prev;
     return WC_OK;
 }
 

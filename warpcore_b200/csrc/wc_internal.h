@@ -7,6 +7,7 @@
 
 #include "wc_bloom.cuh"
 #include "wc_batch.cuh"
+#include "wc_fp_kernels.cuh"
 
 namespace warpcore {
 namespace b200 {
@@ -20,12 +21,14 @@ using DumpKernel = void (*)(const void *, uint64_t, uint64_t, uint64_t, void *, 
                             unsigned long long *);
 
 /* kernel for (window width W, op); nullptr if the combination is not built */
-TableKernel table_kernel_kv32(int W, int op);
-TableKernel table_kernel_kv64(int W, int op);
-TableKernel table_kernel_set32(int W, int op);
-TableKernel table_kernel_set64(int W, int op);
+TableKernel table_kernel_kv32(int W, int op, bool fingerprints);
+TableKernel table_kernel_kv64(int W, int op, bool fingerprints);
+TableKernel table_kernel_set32(int W, int op, bool fingerprints);
+TableKernel table_kernel_set64(int W, int op, bool fingerprints);
 
 CountKernel count_kernel(int layout);
+using RebuildKernel = void (*)(const void *, uint64_t, uint64_t, uint64_t, unsigned char *);
+RebuildKernel fp_rebuild_kernel_ptr(int layout);
 DumpKernel dump_kernel_ptr(int layout);
 
 BloomKernel bloom_kernel_ptr(int key_bytes, int slot_bytes, int cg, bool insert);

@@ -43,7 +43,12 @@ struct TableOpArgs {
     uint32_t bool_mask;   /* ReturnBoolean: status & mask != 0 */
     int handler;
     int is_set;
+    uint32_t flags;       /* kFlag* */
 };
+
+/* fingerprint kernel: before the compare-and-swap of a claim, read the
+ * target slot with a plain load (into L2), then CAS on the resident line */
+constexpr uint32_t kFlagPreloadClaim = 1u;
 
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -95,6 +100,7 @@ __device__ void count_one(const TableView &t, typename L::key_t key, uint32_t c,
             } else if (sk == empty) {
                 K old_key;
                 if (claim_slot<L>(sp, empty, key, V(c), old_key)) {
+                    fp_store(t, b * W + s, fingerprint(key));
                     resolved = true;
                 } else if (old_key == key) {
                     join |= kStDuplicateKey;
@@ -389,6 +395,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
                         count_add<L>(sp, cnt_add, t.max_count, st, join);
                     } else {
                         store_key<L>(sp, tomb);
+                        fp_store(t, bucket * W + uint64_t(fh), kFpTomb);
                         st = kStNone;
                     }
                     pending = false;
@@ -420,6 +427,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
                     const int s = __ffs(claim_bits) - 1;
                     unsigned char *const sp = slots + (bucket * W + uint64_t(s)) * SB;
                     if (cas_old == empty && cas_old_payload == claim_expect) {
+                        fp_store(t, bucket * W + uint64_t(s), fingerprint(key));
                         st = kStNone;
                         pending = false;
                     } else if (cas_old == key) {
