@@ -117,6 +117,9 @@ typedef struct wc_table wc_table;
 
 /* last error message of the calling thread ("" if none) */
 const char *wc_last_error(void);
+/* kernels this library has launched in this process, over all devices and
+ * streams (a batch's CUDA graph counts its one kernel) */
+int wc_launch_count(uint64_t *out);
 /* library version string */
 const char *wc_version(void);
 

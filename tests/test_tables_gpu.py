@@ -358,3 +358,19 @@ def test_counting_block_cache_path(kb, skew):
     r_out = r.retrieve(allk, np.full(allk.size, SENT[kb], dtype=allk.dtype))
     assert np.array_equal(host(out), r_out)
     assert g.size() == r.size()
+
+
+def test_launch_count_counts_this_librarys_kernels():
+    # init is one fill kernel; a bulk call on a table without fingerprints
+    # is one kernel; a retrieve on a fingerprint table is one kernel too
+    t = wc.SingleValueHashTable(10000, key_bytes=4)
+    keys = o.gen_unique_keys(4, 5000, 3)
+    vals = o.gen_uniform(4, 5000, 4)
+    dk, dv = dev(keys), dev(vals)
+    out = empty_dev(5000, 4)
+    c0 = wc.launch_count()
+    t.init()
+    t.insert(dk, dv)
+    t.retrieve(dk, out)
+    assert wc.launch_count() - c0 == 3
+    assert np.array_equal(host(out), vals)

@@ -21,7 +21,7 @@ from ._status import Status  # noqa: F401
 __all__ = [
     "Status", "SingleValueHashTable", "HashSet", "CountingHashTable",
     "BloomFilter", "lib", "valid_capacity", "WarpcoreError", "set_l2_persistence",
-    "HostPipe", "set_fingerprint_policy", "set_fingerprint_ops", "FINGERPRINTS_AUTO", "FINGERPRINTS_ALWAYS",
+    "HostPipe", "set_fingerprint_policy", "set_fingerprint_ops", "launch_count", "FINGERPRINTS_AUTO", "FINGERPRINTS_ALWAYS",
     "FINGERPRINTS_NEVER",
     "HASH_MURMUR", "HASH_NVIDIA", "HASH_MUELLER", "HASH_IDENTITY32",
     "HASH_IDENTITY64", "PROBING_DOUBLE", "PROBING_LINEAR",
@@ -213,6 +213,7 @@ SIGNATURES = {
     "wc_l2_persistence": (_i, [_i, ctypes.POINTER(ctypes.c_int)]),
     "wc_fingerprint_policy": (_i, [_i, ctypes.POINTER(ctypes.c_int)]),
     "wc_fingerprint_ops": (_i, [_u32, ctypes.POINTER(ctypes.c_uint32)]),
+    "wc_launch_count": (_i, [ctypes.POINTER(_u64)]),
     "wc_table_l2_window": (_i, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(ctypes.c_float)]),
     "wc_tune_set": (_i, [_u32, _i, _u32, _u32, _u32, _u32]),
     "wc_tune_reset": (_i, []),
@@ -282,6 +283,13 @@ def set_fingerprint_policy(mode):
     prev = ctypes.c_int(0)
     _check(lib().wc_fingerprint_policy(m, ctypes.byref(prev)))
     return prev.value
+
+
+def launch_count():
+    """kernels this library has launched in this process"""
+    out = _u64(0)
+    _check(lib().wc_launch_count(ctypes.byref(out)))
+    return int(out.value)
 
 
 def set_fingerprint_ops(op_mask):

@@ -239,8 +239,11 @@ void l2_window_release(L2Window &w)
 cudaError_t launch_in_window(const void *kfn, unsigned grid, unsigned block, void **args,
                              cudaStream_t s, const L2Window &w)
 {
-    if (!w.bytes || !g_l2_mode.load(std::memory_order_relaxed))
-        return cudaLaunchKernel(kfn, dim3(grid), dim3(block), args, 0, s);
+    if (!w.bytes || !g_l2_mode.load(std::memory_order_relaxed)) {
+        const cudaError_t e = cudaLaunchKernel(kfn, dim3(grid), dim3(block), args, 0, s);
+        if (e == cudaSuccess) note_launches(1);
+        return e;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
@@ -255,7 +258,9 @@ cudaError_t launch_in_window(const void *kfn, unsigned grid, unsigned block, voi
     attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelExC(&cfg, kfn, args);
+    const cudaError_t e = cudaLaunchKernelExC(&cfg, kfn, args);
+    if (e == cudaSuccess) note_launches(1);
+    return e;
 }
 
 int blocks_per_sm(const void *kernel, int block)
@@ -319,6 +324,9 @@ constexpr int kBlock = 256;
 } // namespace
 
 void warpcore::b200::set_last_error(const char *msg) { g_last_error = msg; }
+
+static std::atomic<unsigned long long> g_launches{0};
+void warpcore::b200::note_launches(uint32_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 /* ------------------------------------------------------------------ */
 /* handles                                                              */
@@ -588,6 +596,7 @@ int table_op(wc_table *t, int op, const void *keys, const void *values, void *ou
         void *rargs[] = {&sl, &cap, &em, &tb, &fp};
         WC_CUDA(cudaLaunchKernel(rfn, dim3(rgrid), dim3(kBlock), rargs, 0,
                                  reinterpret_cast<cudaStream_t>(stream)));
+        note_launches(1);
     }
     if (op == kOpInsert || op == kOpCount) t->keys_inserted += n;
     return WC_OK;
@@ -783,6 +792,7 @@ int wc_table_size(wc_table *t, wc_stream_t stream, uint64_t *size_out)
     const unsigned grid = grid_for(reinterpret_cast<const void *>(k), kBlock, nvec, kBlock * 4);
     k<<<grid, kBlock, 0, s>>>(t->slots, t->capacity, t->cfg.empty_key, t->cfg.tombstone_key,
                               t->counter);
+    note_launches(1);
     WC_CUDA(cudaGetLastError());
     unsigned long long h = 0;
     WC_CUDA(cudaMemcpyAsync(&h, t->counter, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -804,6 +814,7 @@ int wc_table_retrieve_all(wc_table *t, void *keys_out, void *values_out, uint64_
     const unsigned grid = grid_for(reinterpret_cast<const void *>(k), kBlock, t->capacity, kBlock);
     k<<<grid, kBlock, 0, s>>>(t->slots, t->capacity, t->cfg.empty_key, t->cfg.tombstone_key,
                               keys_out, t->kind == 1 ? nullptr : values_out, t->counter);
+    note_launches(1);
     WC_CUDA(cudaGetLastError());
     unsigned long long h = 0;
     WC_CUDA(cudaMemcpyAsync(&h, t->counter, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -855,6 +866,13 @@ int wc_table_get_info(const wc_table *t, wc_table_info *info)
     info->status = t->status;
     info->is_initialized = t->initialized ? 1 : 0;
     info->fingerprints = t->fps;
+    return WC_OK;
+}
+
+int wc_launch_count(uint64_t *out)
+{
+    if (!out) return fail(WC_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = g_launches.load(std::memory_order_relaxed);
     return WC_OK;
 }
 
@@ -1205,6 +1223,7 @@ int host_op(wc_host_pipe *p, wc_table *t, bool insert, const void *h_keys, const
             const void *fk = reinterpret_cast<const void *>(fill_kernel<0>);
             WC_CUDA(cudaLaunchKernel(fk, dim3(grid_for(fk, kBlock, fn / 4, kBlock)), dim3(kBlock),
                                      fargs, 0, s));
+            note_launches(1);
         }
         rc = table_op(t, op, dk, insert ? dv : nullptr, insert ? nullptr : dv, m, stream,
                       probing_length, nullptr, WC_HANDLER_NOTHING, 0);
@@ -1437,6 +1456,7 @@ int wc_batch_run(wc_batch *b, const wc_batch_request *reqs, uint32_t num_request
     }
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     WC_CUDA(cudaGraphLaunch(s.exec, st));
+    note_launches(1); /* the graph's one kernel (beside its descriptor copy) */
     WC_CUDA(cudaEventRecord(s.done, st));
     s.used = true;
     return WC_OK;

@@ -40,6 +40,9 @@ const void *batch_kernel_ptr(int layout, int W, bool inline_desc);
 /* message returned by wc_last_error() on the calling thread */
 void set_last_error(const char *msg);
 
+/* kernels this library launched (wc_launch_count) */
+void note_launches(uint32_t n);
+
 } // namespace b200
 } // namespace warpcore
 

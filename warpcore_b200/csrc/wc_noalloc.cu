@@ -135,6 +135,7 @@ int launch_count(const void *slots, uint64_t capacity, uint64_t empty, uint64_t 
         count_chunk_kernel<L><<<unsigned(nchunks), 256, 0, s>>>(slots, capacity, empty, tomb,
                                                                partials);
     sum_partials_kernel<<<1, 256, 0, s>>>(partials, nchunks, out);
+    note_launches(nchunks ? 2u : 1u);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
         return noalloc_fail(WC_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));

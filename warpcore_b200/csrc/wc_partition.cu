@@ -241,7 +241,9 @@ extern "C" int wc_partition(const void *keys, const void *values, uint64_t n, ui
             cursors, reinterpret_cast<unsigned long long *>(keys_out),
             reinterpret_cast<unsigned long long *>(values_out), po, dropped);
     }
-    return launched() ? WC_OK : WC_ERR_CUDA;
+    if (!launched()) return WC_ERR_CUDA;
+    note_launches(3);
+    return WC_OK;
 }
 
 extern "C" int wc_partition_restore(const void *values, const uint32_t *status,
@@ -276,5 +278,6 @@ extern "C" int wc_partition_restore(const void *values, const uint32_t *status,
         set_last_error(cudaGetErrorString(e));
         return WC_ERR_CUDA;
     }
+    note_launches(1);
     return WC_OK;
 }
