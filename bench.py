@@ -137,7 +137,9 @@ class Workload:
         import warpcore_b200 as wc
         self.kind = kind
         self.n = 1 << log2n
-        self.q = 1 << log2n
+        # svht32 is the small configuration: every inserted key queried once
+        # plus as many absent keys; the others query 2^L keys, half of them hits
+        self.q = (2 << log2n) if kind == "svht32" else (1 << log2n)
         self.load = load
         self.device = device
         gen = torch.Generator(device=device)
@@ -340,9 +342,10 @@ def reference_gpu(wl, reps=5):
 
 
 WORKLOAD_NAMES = {
-    "svht64": "SingleValueHashTable<u64,u64> CG8 LF0.9: insert 2^{L} + retrieve 2^{L} (50% hit)",
-    "svht32": "SingleValueHashTable<u32,u32> CG8: insert 2^{L} + retrieve 2^{L} (50% hit)",
-    "hashset64": "HashSet<u64> CG16 LF0.9: insert 2^{L} + contains 2^{L} (50% hit)",
+    "svht64": "SingleValueHashTable<u64,u64> CG8 LF{LF}: insert 2^{L} + retrieve 2^{L} (50% hit)",
+    "svht32": "SingleValueHashTable<u32,u32> CG8 LF{LF}: insert 2^{L} + retrieve 2^{L1} "
+              "(every inserted key + 2^{L} absent)",
+    "hashset64": "HashSet<u64> CG16 LF{LF}: insert 2^{L} + contains 2^{L} (50% hit)",
     "counting32": "CountingHashTable<u32,u32> CG4 LF0.85: insert 2^{L} Zipf(1.1) + retrieve distinct+absent",
     "bloom64": "BloomFilter<u64,Murmur64,u64,CG8> 16 bits/key k=8: insert 2^{L} + query 2^{L1}",
     "served": "4096 SingleValueHashTable<u32,u32> (caps log-uniform 2^10..2^22, LF 0.85), "
@@ -467,7 +470,7 @@ def run_ours(args):
             "dtype": "u64" if wl.kb == 8 else "u32",
             "data": "synthetic (seeded uniform unique keys, uniform values; inputs resident in HBM)",
             "config": {
-                "workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n, L1=args.log2n + 1),
+                "workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n, L1=args.log2n + 1, LF=args.load),
                 "capacity": int(wl.table.capacity) if hasattr(wl.table, "capacity") else None,
                 "ops_per_step": ops_step,
                 "l2": "inputs larger than L2 (no flush)" if args.log2n >= 24 else "inputs may be L2-resident",
@@ -655,7 +658,7 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "u64" if args.workload not in ("svht32", "counting32") else "u32",
         "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n, L1=args.log2n + 1),
+        "config": {"workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n, L1=args.log2n + 1, LF=args.load),
                    "sample": "2^%d keys per step on the host" % args.cpu_log2n},
         "cpu_baseline": {"value": round(value, 5), "unit": "Gops/s", "cores": threads,
                          "kind": "port",
