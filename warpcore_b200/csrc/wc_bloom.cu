@@ -4,10 +4,19 @@
 namespace warpcore {
 namespace b200 {
 
+/* blocks of at most 128 bytes: one key per lane (bloom_lane_kernel);
+ * larger blocks: the cooperative kernel */
+#ifndef WC_BLOOM_LANE
+#define WC_BLOOM_LANE 1
+#endif
+
 template <class K, class S, int CG>
 static BloomKernel pick_bloom(bool insert)
 {
-    return insert ? bloom_kernel<K, S, CG, true> : bloom_kernel<K, S, CG, false>;
+    if constexpr (WC_BLOOM_LANE && CG * sizeof(S) <= 128)
+        return insert ? bloom_lane_kernel<K, S, CG, true> : bloom_lane_kernel<K, S, CG, false>;
+    else
+        return insert ? bloom_kernel<K, S, CG, true> : bloom_kernel<K, S, CG, false>;
 }
 
 template <class K, class S>

@@ -183,6 +183,66 @@ __global__ void __launch_bounds__(256) bloom_kernel(const BloomArgs a)
     }
 }
 
+/* One key per lane, for blocks of at most 128 bytes: the lane computes its
+ * key's masks, reads its own block with BB / 16 vector loads (all lanes'
+ * loads independent, so a warp keeps 32 blocks in flight), tests it, and
+ * ORs only the words that miss bits.  Against the cooperative kernel above
+ * it spends no shuffles on block indices and masks. */
+template <class K, class S, int CG, bool INSERT>
+__global__ void __launch_bounds__(256) bloom_lane_kernel(const BloomArgs a)
+{
+    constexpr int SB = sizeof(S);
+    constexpr int BB = CG * SB;               /* block bytes, <= 128 */
+    constexpr int VB = BB < 16 ? BB : 16;     /* bytes per load */
+    constexpr int NV = BB / VB;               /* loads per block */
+    constexpr int WPV = VB / SB;              /* words per load */
+    static_assert(BB <= 128 && NV * VB == BB && WPV * SB == VB, "block split");
+
+    S *const words = reinterpret_cast<S *>(a.words);
+    const K *const keys = reinterpret_cast<const K *>(a.keys);
+    const K seed = K(a.seed);
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+        const K key = ld_stream(keys + i);
+        const uint64_t blk =
+            fast_mod(hash_key<K>(a.hasher, K(key + seed)), a.num_blocks, a.magic_blocks);
+        S m[CG];
+        block_masks<K, S, CG>(key, seed, a.hasher, a.k, m);
+        const uint64_t w0 = blk * CG;
+        S w[CG];
+        constexpr bool kRead = !INSERT || WC_BLOOM_INSERT_READS_BLOCK;
+        if (kRead) {
+            if (w0 + CG <= a.num_slots) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    const LaneWords lw = load_lane<VB>(words + w0 + uint64_t(v) * WPV);
+#pragma unroll
+                    for (int s = 0; s < WPV; ++s) w[v * WPV + s] = lane_word<S>(lw, s);
+                }
+            } else {
+                /* ragged last block: words wrap to the front */
+#pragma unroll
+                for (int s = 0; s < CG; ++s) w[s] = __ldcg(words + (w0 + s) % a.num_slots);
+            }
+        } else {
+#pragma unroll
+            for (int s = 0; s < CG; ++s) w[s] = 0;
+        }
+        bool ok = true;
+#pragma unroll
+        for (int s = 0; s < CG; ++s) {
+            const bool missing = (w[s] & m[s]) != m[s];
+            ok &= !missing;
+            if (INSERT && m[s] && (!kRead || missing)) {
+                uint64_t wi = w0 + uint64_t(s);
+                if (wi >= a.num_slots) wi -= a.num_slots;
+                atomic_or_any(words + wi, m[s]);
+            }
+        }
+        if constexpr (!INSERT) a.flags_out[i] = (unsigned char)ok;
+    }
+}
+
 } // namespace b200
 } // namespace warpcore
 
