@@ -15,7 +15,7 @@ _LIB_PATH = os.path.join(_HERE, "libwc_oracle.so")
 
 HASH_MURMUR, HASH_NVIDIA, HASH_MUELLER, HASH_IDENTITY32, HASH_IDENTITY64 = range(5)
 PROBE_DOUBLE, PROBE_LINEAR, PROBE_QUADRATIC = range(3)
-SVHT, HASHSET, COUNTING = range(3)
+SVHT, HASHSET, COUNTING, MULTIVALUE = range(4)
 
 ST_NONE = 0
 ST_UNKNOWN_ERROR = 1 << 0
@@ -27,6 +27,9 @@ ST_KEY_NOT_FOUND = 1 << 5
 ST_INDEX_OVERFLOW = 1 << 6
 ST_OUT_OF_MEMORY = 1 << 7
 ST_NOT_INITIALIZED = 1 << 8
+ST_DRY_RUN = 1 << 9
+ST_INVALID_PHASE_OVERLAP = 1 << 10
+ST_MAX_VALUES_REACHED = 1 << 11
 
 DEFAULT_SEED = 0x5AD0DED
 DEFAULT_PROBING_LENGTH = (2**64 - 1) - 1024
@@ -55,6 +58,12 @@ def _load():
         "wco_status_to_bool": (ctypes.c_uint8, [ctypes.c_uint32, ctypes.c_uint32]),
         "wco_table_create": (_vp, [_i, _i, _i, _u64, _u64, _u64, _i, _i, _i, _u64, _u64, _u64]),
         "wco_table_destroy": (None, [_vp]),
+        "wco_mv_create": (_vp, [_i, _i, _u64, _u64, _u64, _i, _i, _i, _u64, _u64, _u64]),
+        "wco_mv_insert": (None, [_vp, _vp, _vp, _u64, _u64, _vp]),
+        "wco_mv_num_values": (_u64, [_vp, _vp, _u64, _vp, _u64, _vp]),
+        "wco_mv_retrieve": (_u64, [_vp, _vp, _u64, _vp, _vp, _vp, _u64, _vp]),
+        "wco_mv_num_keys": (_u64, [_vp]),
+        "wco_mv_unique_keys": (_u64, [_vp, _vp]),
         "wco_table_capacity": (_u64, [_vp]),
         "wco_table_init": (None, [_vp, _u64]),
         "wco_insert": (None, [_vp, _vp, _vp, _u64, _u64, _vp]),
@@ -228,6 +237,63 @@ class Table:
 
     def pop_status(self):
         return lib().wco_pop_status(self.h)
+
+
+class MVTable(Table):
+    """Sequential reference-order MultiValueHashTable."""
+
+    def __init__(self, key_bytes, value_bytes, min_capacity, seed=DEFAULT_SEED, cg=8,
+                 scheme=PROBE_DOUBLE, h1=HASH_MURMUR, h2=HASH_MURMUR, empty_key=0,
+                 tombstone_key=None, max_values_per_key=None):
+        if tombstone_key is None:
+            tombstone_key = (1 << (8 * key_bytes)) - 1
+        if max_values_per_key is None:
+            max_values_per_key = 2**64 - 1
+        self.kind = MULTIVALUE
+        self.key_bytes = key_bytes
+        self.value_bytes = value_bytes
+        self.h = lib().wco_mv_create(key_bytes, value_bytes, int(min_capacity), int(seed), cg,
+                                     scheme, h1, h2, int(empty_key), int(tombstone_key),
+                                     int(max_values_per_key))
+
+    def insert(self, keys, values, probing_length=DEFAULT_PROBING_LENGTH, want_status=False):
+        keys = np.ascontiguousarray(keys)
+        values = np.ascontiguousarray(values)
+        st = np.zeros(len(keys), dtype=np.uint32) if want_status else None
+        lib().wco_mv_insert(self.h, _ptr(keys), _ptr(values), len(keys), int(probing_length),
+                            _ptr(st))
+        return st
+
+    def num_values(self, keys, probing_length=DEFAULT_PROBING_LENGTH):
+        """(total, per-key counts, statuses)"""
+        keys = np.ascontiguousarray(keys)
+        c = np.zeros(len(keys), dtype=np.uint64)
+        st = np.zeros(len(keys), dtype=np.uint32)
+        total = lib().wco_mv_num_values(self.h, _ptr(keys), len(keys), _ptr(c),
+                                        int(probing_length), _ptr(st))
+        return total, c, st
+
+    def retrieve(self, keys, dry_run=False, probing_length=DEFAULT_PROBING_LENGTH):
+        """(begin offsets, end offsets, values, statuses); a dry run gives
+        per-key counts in place of end offsets and no values"""
+        keys = np.ascontiguousarray(keys)
+        n = len(keys)
+        b = np.zeros(n, dtype=np.uint64)
+        e = np.zeros(n, dtype=np.uint64)
+        st = np.zeros(n, dtype=np.uint32)
+        total, _, _ = self.num_values(keys, probing_length) if not dry_run else (0, None, None)
+        vals = None if dry_run else np.zeros(max(int(total), 1), dtype=_kdtype(self.value_bytes))
+        lib().wco_mv_retrieve(self.h, _ptr(keys), n, _ptr(b), _ptr(e), _ptr(vals),
+                              int(probing_length), _ptr(st))
+        return b, e, (vals[:int(total)] if vals is not None else None), st
+
+    def num_keys(self):
+        return lib().wco_mv_num_keys(self.h)
+
+    def unique_keys(self):
+        k = np.empty(max(self.capacity, 1), dtype=_kdtype(self.key_bytes))
+        n = lib().wco_mv_unique_keys(self.h, _ptr(k))
+        return k[:n]
 
 
 class Bloom:

@@ -26,6 +26,7 @@
 #define SDIV(x, y) (((x) + (y) - 1) / (y))
 #define H2D (cudaMemcpyHostToDevice)
 #define D2H (cudaMemcpyDeviceToHost)
+#define D2D (cudaMemcpyDeviceToDevice)
 #define CUERR                                                                  \
     {                                                                          \
         cudaError_t e_ = cudaGetLastError();                                   \

@@ -282,6 +282,7 @@ struct wco_table {
     uint64_t *keys;
     uint64_t *values;
     uint32_t status;
+    uint64_t max_values, num_keys; /* multi-value tables */
 };
 
 wco_table *wco_table_create(int kind, int key_bytes, int value_bytes,
@@ -325,6 +326,7 @@ void wco_table_init(wco_table *t, uint64_t seed)
     if (t->kind == WCO_COUNTING)
         memset(t->values, 0, t->capacity * 8);
     t->status = 0;
+    t->num_keys = 0;
 }
 
 static uint64_t load_elem(const void *p, int bytes, uint64_t i)
@@ -550,6 +552,197 @@ void wco_table_slots(const wco_table *t, uint64_t *keys_out,
 {
     if (keys_out) memcpy(keys_out, t->keys, t->capacity * 8);
     if (values_out) memcpy(values_out, t->values, t->capacity * 8);
+}
+
+/* ------------------------------------------------------------------------ */
+/* MultiValueHashTable (multi_value_hash_table.cuh): every (key, value) pair  */
+/* takes a slot of its own.                                                   */
+/* ------------------------------------------------------------------------ */
+
+wco_table *wco_mv_create(int key_bytes, int value_bytes, uint64_t min_capacity, uint64_t seed,
+                         uint64_t cg, int scheme, int h1, int h2, uint64_t empty_key,
+                         uint64_t tombstone_key, uint64_t max_values_per_key)
+{
+    wco_table *t = wco_table_create(WCO_SVHT, key_bytes, value_bytes, min_capacity, seed, cg,
+                                    scheme, h1, h2, empty_key, tombstone_key, ~0ull);
+    t->kind = WCO_MULTIVALUE;
+    t->max_values = max_values_per_key;
+    return t;
+}
+
+/* insert (multi_value_hash_table.cuh:200-289): along the probe sequence,
+ * count the key's values window by window; stop with duplicate_key +
+ * max_values_for_key_reached once the count reaches max_values_per_key;
+ * otherwise claim the window's first empty slot (lane order).  A key that
+ * had no value yet counts as a new key.  The status is duplicate_key when
+ * the key had values (not joined on success). */
+void wco_mv_insert(wco_table *t, const void *keys, const void *values, uint64_t n,
+                   uint64_t probing_length, uint32_t *status_out)
+{
+    for (uint64_t i = 0; i < n; i++) {
+        const uint64_t key = load_elem(keys, t->key_bytes, i);
+        uint32_t st;
+        if (!valid_key(t, key)) {
+            join(t, WCO_ST_INVALID_KEY);
+            st = WCO_ST_INVALID_KEY;
+        } else {
+            probe_t p;
+            probe_begin(&p, t->scheme, t->h1, t->h2, t->key_bytes, t->cg, t->capacity, key,
+                        t->seed, probing_length);
+            uint64_t num = 0, guard = t->capacity / t->cg + 1;
+            int done = 0;
+            st = WCO_ST_PROBING_LENGTH_EXCEEDED;
+            do {
+                for (uint64_t r = 0; r < t->cg; r++) num += t->keys[p.pos[r]] == key;
+                if (num >= t->max_values) {
+                    st = WCO_ST_DUPLICATE_KEY | WCO_ST_MAX_VALUES_REACHED;
+                    join(t, st);
+                    done = 1;
+                    break;
+                }
+                for (uint64_t r = 0; r < t->cg; r++) {
+                    if (t->keys[p.pos[r]] == t->empty) {
+                        t->keys[p.pos[r]] = key;
+                        t->values[p.pos[r]] = load_elem(values, t->value_bytes, i);
+                        if (num == 0) t->num_keys++;
+                        st = num > 0 ? WCO_ST_DUPLICATE_KEY : WCO_ST_NONE;
+                        done = 1;
+                        break;
+                    }
+                }
+                if (done) break;
+            } while (--guard && probe_next(&p));
+            if (!done) {
+                st = WCO_ST_PROBING_LENGTH_EXCEEDED | (num > 0 ? WCO_ST_DUPLICATE_KEY : 0);
+                join(t, st);
+            }
+        }
+        if (status_out) status_out[i] = st;
+    }
+}
+
+/* for_each over one key's values (multi_value_hash_table.cuh:607-663):
+ * windows of the probe sequence (probing length capped at the capacity),
+ * hits in lane order, until a window holds an empty slot or the count
+ * reaches max_values_per_key.  Writes the values to out (if not NULL) and
+ * returns the status; *num gets the count. */
+static uint32_t mv_for_each(wco_table *t, uint64_t key, uint64_t probing_length, void *out,
+                            uint64_t *num_out)
+{
+    if (!valid_key(t, key)) {
+        *num_out = 0;
+        join(t, WCO_ST_INVALID_KEY);
+        return WCO_ST_INVALID_KEY;
+    }
+    probe_t p;
+    const uint64_t pl = probing_length < t->capacity ? probing_length : t->capacity;
+    probe_begin(&p, t->scheme, t->h1, t->h2, t->key_bytes, t->cg, t->capacity, key, t->seed,
+                pl);
+    uint64_t num = 0, guard = t->capacity / t->cg + 1;
+    do {
+        int any_empty = 0;
+        for (uint64_t r = 0; r < t->cg; r++) {
+            const uint64_t k = t->keys[p.pos[r]];
+            if (k == key) {
+                if (out) store_elem(out, t->value_bytes, num, t->values[p.pos[r]]);
+                num++;
+            }
+            any_empty |= k == t->empty;
+        }
+        if (any_empty || num >= t->max_values) {
+            *num_out = num;
+            if (num == 0) {
+                join(t, WCO_ST_KEY_NOT_FOUND);
+                return WCO_ST_KEY_NOT_FOUND;
+            }
+            return WCO_ST_NONE;
+        }
+    } while (--guard && probe_next(&p));
+    *num_out = num;
+    join(t, WCO_ST_PROBING_LENGTH_EXCEEDED);
+    return WCO_ST_PROBING_LENGTH_EXCEEDED;
+}
+
+/* bulk num_values (multi_value_hash_table.cuh:769-800, gpu_engine.cuh:467-501) */
+uint64_t wco_mv_num_values(wco_table *t, const void *keys, uint64_t n, uint64_t *counts_out,
+                           uint64_t probing_length, uint32_t *status_out)
+{
+    uint64_t total = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t num = 0;
+        const uint32_t st = mv_for_each(t, load_elem(keys, t->key_bytes, i), probing_length,
+                                        NULL, &num);
+        if (counts_out) counts_out[i] = num;
+        total += num;
+        if (status_out) status_out[i] = st;
+    }
+    return total;
+}
+
+/* bulk retrieve (multi_value_hash_table.cuh:371-520, gpu_engine.cuh:305-346):
+ * counts per key, an inclusive scan into end offsets, begin offsets one
+ * behind, then every key's values in probe order at its begin offset.
+ * With values_out NULL it is a dry run: end_offsets get the per-key counts
+ * (not scanned) and every status is dry_run. */
+uint64_t wco_mv_retrieve(wco_table *t, const void *keys, uint64_t n, uint64_t *begin_out,
+                         uint64_t *end_out, void *values_out, uint64_t probing_length,
+                         uint32_t *status_out)
+{
+    const uint64_t total = wco_mv_num_values(t, keys, n, end_out, probing_length, NULL);
+    if (!values_out) {
+        for (uint64_t i = 0; i < n && status_out; i++) status_out[i] = WCO_ST_DRY_RUN;
+        join(t, WCO_ST_DRY_RUN);
+        return total;
+    }
+    uint64_t s = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        begin_out[i] = s;
+        s += end_out[i];
+        end_out[i] = s;
+    }
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t num = 0;
+        char *dst = (char *)values_out + begin_out[i] * (uint64_t)t->value_bytes;
+        uint32_t st = mv_for_each(t, load_elem(keys, t->key_bytes, i), probing_length, dst, &num);
+        if (num != end_out[i] - begin_out[i]) {
+            join(t, WCO_ST_INVALID_PHASE_OVERLAP);
+            st |= WCO_ST_INVALID_PHASE_OVERLAP;
+        }
+        if (status_out) status_out[i] = st;
+    }
+    return total;
+}
+
+uint64_t wco_mv_num_keys(const wco_table *t) { return t->num_keys; }
+
+/* retrieve_all_keys (multi_value_hash_table.cuh:561-598, gpu_engine.cuh:51-93):
+ * a slot's key is output when that slot is the key's first entry along its
+ * probe sequence (the lowest lane of the first window that holds it).
+ * Output in slot order. */
+uint64_t wco_mv_unique_keys(const wco_table *t, void *keys_out)
+{
+    uint64_t n = 0;
+    for (uint64_t gid = 0; gid < t->capacity; gid++) {
+        const uint64_t key = t->keys[gid];
+        if (!valid_key(t, key)) continue;
+        probe_t p;
+        probe_begin(&p, t->scheme, t->h1, t->h2, t->key_bytes, t->cg, t->capacity, key, t->seed,
+                    t->capacity);
+        uint64_t guard = t->capacity / t->cg + 1;
+        do {
+            int64_t leader = -1;
+            for (uint64_t r = 0; r < t->cg && leader < 0; r++)
+                if (t->keys[p.pos[r]] == key) leader = (int64_t)p.pos[r];
+            if (leader >= 0) {
+                if ((uint64_t)leader == gid) {
+                    if (keys_out) store_elem(keys_out, t->key_bytes, n, key);
+                    n++;
+                }
+                break;
+            }
+        } while (--guard && probe_next(&p));
+    }
+    return n;
 }
 
 /* ------------------------------------------------------------------------ */

@@ -46,7 +46,8 @@ enum {
 enum {
     WCO_SVHT = 0,
     WCO_HASHSET = 1,
-    WCO_COUNTING = 2
+    WCO_COUNTING = 2,
+    WCO_MULTIVALUE = 3
 };
 
 /* Status bits (status.cuh:44-68) */
@@ -112,6 +113,20 @@ uint32_t wco_pop_status(wco_table *t);
 void wco_table_slots(const wco_table *t, uint64_t *keys_out, uint64_t *values_out);
 
 /* ---- pattern-blocked Bloom filter (bloom_filter.cuh) ---- */
+/* MultiValueHashTable (multi_value_hash_table.cuh) */
+wco_table *wco_mv_create(int key_bytes, int value_bytes, uint64_t min_capacity, uint64_t seed,
+                         uint64_t cg, int scheme, int h1, int h2, uint64_t empty_key,
+                         uint64_t tombstone_key, uint64_t max_values_per_key);
+void wco_mv_insert(wco_table *t, const void *keys, const void *values, uint64_t n,
+                   uint64_t probing_length, uint32_t *status_out);
+uint64_t wco_mv_num_values(wco_table *t, const void *keys, uint64_t n, uint64_t *counts_out,
+                           uint64_t probing_length, uint32_t *status_out);
+uint64_t wco_mv_retrieve(wco_table *t, const void *keys, uint64_t n, uint64_t *begin_out,
+                         uint64_t *end_out, void *values_out, uint64_t probing_length,
+                         uint32_t *status_out);
+uint64_t wco_mv_num_keys(const wco_table *t);
+uint64_t wco_mv_unique_keys(const wco_table *t, void *keys_out);
+
 typedef struct wco_bloom wco_bloom;
 wco_bloom *wco_bloom_create(int key_bytes, int slot_bytes, uint64_t cg,
                             int hasher, uint64_t num_bits, uint64_t k,

@@ -107,3 +107,44 @@ SVHT_CASES = [("svht_u32u32", 4), ("svht_u64u64", 8)]
 SET_CASES = [("set_u64", 8), ("set_u32", 4)]
 COUNT_CASES = ["count_u32", "count_u32_max10"]
 BLOOM_CASES = ["bloom_u64_s64_cg8", "bloom_u64_s64_cg1", "bloom_u32_s32_cg4", "bloom_u32_s64_cg2"]
+
+
+MV_CASES = [("mv_u32u32_max3", 4), ("mv_u64u64", 8)]
+
+
+def mv_scenario(F, tag, kb, make_table):
+    """make_table(min_cap, max_values_per_key) -> object with insert /
+    num_keys / size / pop_status / retrieve(keys, dry_run) /
+    unique_keys like oracle.MVTable"""
+    (n, min_cap, kseed, cap, max_values, num_keys, size, s1, num_dry, s2, num_out, s3,
+     num_unique) = F[tag + "_meta"].tolist()
+    allk = o.gen_unique_keys(kb, n + n // 4, kseed)
+    keys = allk[:n]
+    t = make_table(min_cap, max_values)
+    assert t.capacity == cap
+    st_all, vals_all = [], []
+    for r in range(5):
+        m = n - r * (n // 5)
+        v = o.gen_uniform(kb, m, kseed + 10 + r)
+        st_all.append(t.insert(keys[:m], v, want_status=True))
+        vals_all.append(v)
+    assert np.array_equal(np.concatenate(st_all), F[tag + "_insert_status"])
+    assert np.array_equal(np.concatenate(vals_all), F[tag + "_insert_values"])
+    assert t.num_keys() == num_keys
+    assert t.size() == size
+    assert t.pop_status() == s1
+    _, counts, _, st = t.retrieve(allk, dry_run=True)
+    assert int(counts.sum()) == num_dry
+    assert np.array_equal(counts, F[tag + "_dry_counts"])
+    assert np.array_equal(st, F[tag + "_dry_status"])
+    assert t.pop_status() == s2
+    b, e, v, st = t.retrieve(allk)
+    assert np.array_equal(b, F[tag + "_begin"])
+    assert np.array_equal(e, F[tag + "_end"])
+    assert v.size == num_out
+    assert np.array_equal(v, F[tag + "_values"])
+    assert np.array_equal(st, F[tag + "_retrieve_status"])
+    assert t.pop_status() == s3
+    uk = np.sort(t.unique_keys())
+    assert uk.size == num_unique
+    assert np.array_equal(uk, F[tag + "_unique_keys_sorted"])

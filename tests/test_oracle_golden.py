@@ -57,3 +57,8 @@ def test_bloom(tag):
     def make(kb, sb, cg, num_bits, k):
         return o.Bloom(num_bits, k, key_bytes=kb, slot_bytes=sb, cg=cg)
     gs.bloom_scenario(F, tag, make)
+
+
+@pytest.mark.parametrize("tag,kb", gs.MV_CASES)
+def test_multi_value(tag, kb):
+    gs.mv_scenario(F, tag, kb, lambda cap, mx: o.MVTable(kb, kb, cap, max_values_per_key=mx))
