@@ -51,6 +51,9 @@ enum : uint32_t {
     kStIndexOverflow = 1u << 6,
     kStOutOfMemory = 1u << 7,
     kStNotInitialized = 1u << 8,
+    kStDryRun = 1u << 9,
+    kStInvalidPhaseOverlap = 1u << 10,
+    kStMaxValuesReached = 1u << 11,
 };
 
 enum : uint32_t {

@@ -234,6 +234,44 @@ int wc_counting_erase(wc_table *t, const void *keys_in, uint64_t num_in,
                       void *status_out, int status_handler, uint32_t ignore);
 
 /* ------------------------------------------------------------------ */
+/* MultiValueHashTable<Key, Value, EmptyKey, TombstoneKey, ProbingScheme> */
+/* (multi_value_hash_table.cuh); kind 3.  Every (key, value) pair takes  */
+/* a slot of its own.  wc_svht_default_config gives the reference's     */
+/* defaults.  size, init, retrieve_all (all pairs), peek/pop_status,    */
+/* get_info and destroy are the wc_table_* calls.                        */
+/* ------------------------------------------------------------------ */
+
+/* MultiValueHashTable(min_capacity, seed, max_values_per_key, no_init)
+ * (multi_value_hash_table.cuh:101-125) */
+int wc_mvht_create(const wc_table_config *cfg, uint64_t min_capacity, uint64_t seed,
+                   uint64_t max_values_per_key, int no_init, wc_table **out);
+/* insert (:200-326): a key that already holds max_values_per_key values
+ * reports duplicate_key + max_values_for_key_reached and is not stored; a
+ * key that held values reports duplicate_key */
+int wc_mvht_insert(wc_table *t, const void *keys_in, const void *values_in, uint64_t num_in,
+                   wc_stream_t stream, uint64_t probing_length, void *status_out,
+                   int status_handler, uint32_t ignore);
+/* num_values (:769-800): values per key into num_per_key_out (device, may
+ * be NULL) and their sum into *num_out (host); synchronises `stream` */
+int wc_mvht_num_values(wc_table *t, const void *keys_in, uint64_t num_in, uint64_t *num_out,
+                       uint64_t *num_per_key_out, wc_stream_t stream, uint64_t probing_length,
+                       void *status_out, int status_handler, uint32_t ignore);
+/* retrieve (:371-520): every key's values, in insertion order, at
+ * values_out[begin_offsets_out[i] .. end_offsets_out[i]); *num_out (host)
+ * gets the total.  With values_out NULL it is a dry run: end_offsets_out
+ * gets the per-key counts (not summed), every status is dry_run.  The
+ * offsets are uint64; synchronises `stream` before the values pass. */
+int wc_mvht_retrieve(wc_table *t, const void *keys_in, uint64_t num_in,
+                     uint64_t *begin_offsets_out, uint64_t *end_offsets_out, void *values_out,
+                     uint64_t *num_out, wc_stream_t stream, uint64_t probing_length,
+                     void *status_out, int status_handler, uint32_t ignore);
+/* retrieve_all_keys (:561-598): each stored key once (order unspecified);
+ * with keys_out NULL *num_out gets num_keys() (a dry run) */
+int wc_mvht_retrieve_all_keys(wc_table *t, void *keys_out, uint64_t *num_out, wc_stream_t stream);
+/* num_keys (:720-735): keys that hold at least one value */
+int wc_mvht_num_keys(wc_table *t, wc_stream_t stream, uint64_t *out);
+
+/* ------------------------------------------------------------------ */
 /* BloomFilter<Key, Hasher, Slot, CGSize>                               */
 /* ------------------------------------------------------------------ */
 

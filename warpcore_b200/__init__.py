@@ -19,7 +19,7 @@ import os
 from ._status import Status  # noqa: F401
 
 __all__ = [
-    "Status", "SingleValueHashTable", "HashSet", "CountingHashTable",
+    "Status", "SingleValueHashTable", "HashSet", "CountingHashTable", "MultiValueHashTable",
     "BloomFilter", "lib", "valid_capacity", "WarpcoreError", "set_l2_persistence",
     "HostPipe", "set_fingerprint_policy", "set_fingerprint_ops", "launch_count", "FINGERPRINTS_AUTO", "FINGERPRINTS_ALWAYS",
     "FINGERPRINTS_NEVER",
@@ -214,6 +214,13 @@ SIGNATURES = {
     "wc_fingerprint_policy": (_i, [_i, ctypes.POINTER(ctypes.c_int)]),
     "wc_fingerprint_ops": (_i, [_u32, ctypes.POINTER(ctypes.c_uint32)]),
     "wc_launch_count": (_i, [ctypes.POINTER(_u64)]),
+    "wc_mvht_create": (_i, [ctypes.POINTER(TableConfig), _u64, _u64, _u64, _i, _pp]),
+    "wc_mvht_insert": (_i, [_vp, _vp, _vp, _u64, _vp, _u64, _vp, _i, _u32]),
+    "wc_mvht_num_values": (_i, [_vp, _vp, _u64, ctypes.POINTER(_u64), _vp, _vp, _u64, _vp, _i, _u32]),
+    "wc_mvht_retrieve": (_i, [_vp, _vp, _u64, _vp, _vp, _vp, ctypes.POINTER(_u64), _vp, _u64, _vp,
+                              _i, _u32]),
+    "wc_mvht_retrieve_all_keys": (_i, [_vp, _vp, ctypes.POINTER(_u64), _vp]),
+    "wc_mvht_num_keys": (_i, [_vp, _vp, ctypes.POINTER(_u64)]),
     "wc_table_l2_window": (_i, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(ctypes.c_float)]),
     "wc_tune_set": (_i, [_u32, _i, _u32, _u32, _u32, _u32]),
     "wc_tune_reset": (_i, []),
@@ -520,6 +527,72 @@ class SingleValueHashTable(_Table):
         _check(lib().wc_svht_erase(self._h, _ptr(keys_in), _numel(keys_in, num_in),
                                    _stream(stream), int(probing_length), _ptr(status_out),
                                    h, int(ignore)))
+
+
+class MultiValueHashTable(_Table):
+    """warpcore::MultiValueHashTable (multi_value_hash_table.cuh:18-27): every
+    (key, value) pair takes a slot of its own; retrieve returns each key's
+    values in insertion order with begin/end offsets."""
+
+    def __init__(self, min_capacity, seed=DEFAULT_SEED, max_values_per_key=2**64 - 1,
+                 no_init=False, key_bytes=4, value_bytes=None, empty_key=None,
+                 tombstone_key=None, probing=None, hasher1=None, hasher2=None, cg_size=None):
+        value_bytes = key_bytes if value_bytes is None else value_bytes
+        cfg = _table_config(lib().wc_svht_default_config, key_bytes, value_bytes, empty_key,
+                            tombstone_key, probing, hasher1, hasher2, cg_size)
+        self._make(lib().wc_mvht_create, cfg, int(min_capacity), int(seed),
+                   int(max_values_per_key), int(bool(no_init)))
+
+    def insert(self, keys_in, values_in, num_in=None, stream=None,
+               probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+               status_handler=None, ignore=0):
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        _check_width(values_in, self._cfg.value_bytes, "values_in")
+        h = _handler(status_out, status_handler)
+        _check(lib().wc_mvht_insert(self._h, _ptr(keys_in), _ptr(values_in),
+                                    _numel(keys_in, num_in), _stream(stream),
+                                    int(probing_length), _ptr(status_out), h, int(ignore)))
+
+    def num_values(self, keys_in, num_per_key_out=None, num_in=None, stream=None,
+                   probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+                   status_handler=None, ignore=0):
+        """values per key (uint64 tensor, optional); returns their sum"""
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        h = _handler(status_out, status_handler)
+        out = _u64(0)
+        _check(lib().wc_mvht_num_values(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                        ctypes.byref(out), _ptr(num_per_key_out),
+                                        _stream(stream), int(probing_length), _ptr(status_out),
+                                        h, int(ignore)))
+        return int(out.value)
+
+    def retrieve(self, keys_in, begin_offsets_out, end_offsets_out, values_out=None,
+                 num_in=None, stream=None, probing_length=DEFAULT_PROBING_LENGTH,
+                 status_out=None, status_handler=None, ignore=0):
+        """values_out None: dry run (end_offsets_out gets the counts);
+        returns the total number of values"""
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        if values_out is not None:
+            _check_width(values_out, self._cfg.value_bytes, "values_out")
+        h = _handler(status_out, status_handler)
+        out = _u64(0)
+        _check(lib().wc_mvht_retrieve(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                      _ptr(begin_offsets_out), _ptr(end_offsets_out),
+                                      _ptr(values_out), ctypes.byref(out), _stream(stream),
+                                      int(probing_length), _ptr(status_out), h, int(ignore)))
+        return int(out.value)
+
+    def retrieve_all_keys(self, keys_out=None, stream=None):
+        """each stored key once; keys_out None: only the count"""
+        out = _u64(0)
+        _check(lib().wc_mvht_retrieve_all_keys(self._h, _ptr(keys_out), ctypes.byref(out),
+                                               _stream(stream)))
+        return int(out.value)
+
+    def num_keys(self, stream=None):
+        out = _u64(0)
+        _check(lib().wc_mvht_num_keys(self._h, _stream(stream), ctypes.byref(out)))
+        return int(out.value)
 
 
 class HashSet(_Table):

@@ -349,6 +349,11 @@ struct wc_table {
     uint64_t keys_inserted = 0; /* since init: an upper bound of size(), for tuning */
     L2Window l2;                /* access-policy window over the slots, if they fit */
     unsigned char *fps = nullptr; /* one fingerprint byte per slot, or NULL */
+    /* multi-value tables */
+    uint64_t max_values = ~0ull;
+    unsigned long long *num_keys = nullptr; /* device: keys holding at least one value */
+    void *scratch = nullptr;                /* device: scan tile sums, grown on demand */
+    uint64_t scratch_bytes = 0;
 };
 
 struct wc_bloom {
@@ -463,7 +468,7 @@ int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, ui
 
     /* the reference checks free memory before allocating (storage.cuh:464-473) */
     const uint64_t bytes = cap * t->slot_bytes;
-    const uint64_t fp_bytes = want_fingerprints(bytes) ? cap : 0;
+    const uint64_t fp_bytes = (kind != 3 && want_fingerprints(bytes)) ? cap : 0;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
         delete t;
@@ -482,6 +487,7 @@ int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, ui
         if (e == cudaSuccess) {
             t->status = reinterpret_cast<uint32_t *>(aux);
             t->counter = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(aux) + 128);
+            t->num_keys = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(aux) + 192);
         }
     }
     if (e != cudaSuccess) {
@@ -669,6 +675,7 @@ int wc_table_destroy(wc_table *t)
     if (t->slots) cudaFree(t->slots);
     if (t->fps) cudaFree(t->fps);
     if (t->status) cudaFree(t->status);
+    if (t->scratch) cudaFree(t->scratch);
     l2_window_release(t->l2);
     delete t;
     return WC_OK;
@@ -685,6 +692,7 @@ int wc_table_init(wc_table *t, uint64_t seed, wc_stream_t stream)
     if (rc) return rc;
     if (t->fps) WC_CUDA(cudaMemsetAsync(t->fps, kFpEmpty, t->capacity, s));
     WC_CUDA(cudaMemsetAsync(t->status, 0, sizeof(uint32_t), s));
+    if (t->kind == 3) WC_CUDA(cudaMemsetAsync(t->num_keys, 0, sizeof(unsigned long long), s));
     WC_CUDA(cudaStreamSynchronize(s));
     t->initialized = true;
     return WC_OK;
@@ -783,7 +791,7 @@ int wc_table_size(wc_table *t, wc_stream_t stream, uint64_t *size_out)
 {
     if (!size_out) return fail(WC_ERR_INVALID_ARGUMENT, "size_out is NULL");
     *size_out = 0;
-    int rc = check_table(t, 7);
+    int rc = check_table(t, 0xF); /* every table kind */
     if (rc) return rc;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     CountKernel k = count_kernel(t->layout);
@@ -806,7 +814,7 @@ int wc_table_retrieve_all(wc_table *t, void *keys_out, void *values_out, uint64_
 {
     if (!num_out || !keys_out) return fail(WC_ERR_INVALID_ARGUMENT, "NULL output");
     *num_out = 0;
-    int rc = check_table(t, 7);
+    int rc = check_table(t, 0xF); /* every table kind: all (key, value) pairs */
     if (rc) return rc;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     DumpKernel k = dump_kernel_ptr(t->layout);
@@ -866,6 +874,232 @@ int wc_table_get_info(const wc_table *t, wc_table_info *info)
     info->status = t->status;
     info->is_initialized = t->initialized ? 1 : 0;
     info->fingerprints = t->fps;
+    return WC_OK;
+}
+
+/* ---- MultiValueHashTable (multi_value_hash_table.cuh) ---- */
+
+int wc_mvht_create(const wc_table_config *cfg, uint64_t min_capacity, uint64_t seed,
+                   uint64_t max_values_per_key, int no_init, wc_table **out)
+{
+    if (max_values_per_key == 0)
+        return fail(WC_ERR_INVALID_ARGUMENT, "max_values_per_key must be at least 1");
+    int rc = table_create(3, cfg, min_capacity, seed, 0, 1, out);
+    if (rc) return rc;
+    (*out)->max_values = max_values_per_key;
+    if (!no_init) {
+        rc = wc_table_init(*out, (*out)->seed, nullptr);
+        if (rc) {
+            wc_table_destroy(*out);
+            *out = nullptr;
+            return rc;
+        }
+    }
+    return WC_OK;
+}
+
+namespace {
+
+MvArgs mv_args(wc_table *t, const void *keys, uint64_t n, uint64_t probing_length, bool find,
+               void *status_out, int handler, uint32_t ignore)
+{
+    MvArgs a{};
+    a.t = view_of(t);
+    a.keys = keys;
+    a.n = n;
+    /* for_each caps the probing length at the capacity (:623) */
+    const uint64_t pl = find && probing_length > t->capacity ? t->capacity : probing_length;
+    a.max_windows = max_windows(pl, t->cfg.cg_size, t->num_buckets);
+    a.max_values = t->max_values;
+    a.status_out = handler == WC_HANDLER_NOTHING ? nullptr : status_out;
+    a.handler = handler;
+    a.bool_mask = (~ignore) ^ 0xFFFu;
+    return a;
+}
+
+int mv_launch(const void *k, wc_table *t, uint64_t items, MvArgs &a, cudaStream_t s)
+{
+    void *args[] = {&a};
+    const unsigned grid = grid_for(k, kBlock, items, kBlock);
+    WC_CUDA(cudaLaunchKernel(k, dim3(grid), dim3(kBlock), args, 0, s));
+    note_launches(1);
+    return WC_OK;
+}
+
+/* per-key counts (and their sum, read back to the host) */
+int mv_count(wc_table *t, const void *keys, uint64_t n, uint64_t *counts_dev, uint64_t *total,
+             cudaStream_t s, uint64_t probing_length, void *status_out, int handler,
+             uint32_t ignore)
+{
+    const MvKernels k = mv_kernels(t->layout, int(t->cfg.cg_size));
+    if (!k.count) return fail(WC_ERR_UNSUPPORTED, "no kernel for this configuration");
+    WC_CUDA(cudaMemsetAsync(t->counter, 0, sizeof(unsigned long long), s));
+    MvArgs a = mv_args(t, keys, n, probing_length, true, status_out, handler, ignore);
+    a.counts_out = reinterpret_cast<unsigned long long *>(counts_dev);
+    a.total = t->counter;
+    int rc = mv_launch(k.count, t, n, a, s);
+    if (rc) return rc;
+    unsigned long long h = 0;
+    WC_CUDA(cudaMemcpyAsync(&h, t->counter, sizeof(h), cudaMemcpyDeviceToHost, s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    *total = h;
+    return WC_OK;
+}
+
+/* counts in end -> end = inclusive prefix sums, begin = exclusive ones */
+int mv_scan(wc_table *t, uint64_t *begin, uint64_t *end, uint64_t n, cudaStream_t s)
+{
+    const MvScanKernels k = mv_scan_kernels();
+    const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
+    const uint64_t need = ntiles * sizeof(unsigned long long);
+    if (need > t->scratch_bytes) {
+        WC_CUDA(cudaStreamSynchronize(s));
+        if (t->scratch) cudaFree(t->scratch);
+        t->scratch = nullptr;
+        t->scratch_bytes = 0;
+        WC_CUDA(cudaMalloc(&t->scratch, need));
+        t->scratch_bytes = need;
+    }
+    auto *e = reinterpret_cast<unsigned long long *>(end);
+    auto *b = reinterpret_cast<unsigned long long *>(begin);
+    auto *ts = reinterpret_cast<unsigned long long *>(t->scratch);
+    uint64_t nn = n, nt = ntiles;
+    void *a1[] = {&e, &nn, &ts};
+    WC_CUDA(cudaLaunchKernel(k.tile_sums, dim3(unsigned(ntiles)), dim3(kScanThreads), a1, 0, s));
+    void *a2[] = {&ts, &nt};
+    WC_CUDA(cudaLaunchKernel(k.tile_offsets, dim3(1), dim3(kScanThreads), a2, 0, s));
+    void *a3[] = {&e, &b, &nn, &ts};
+    WC_CUDA(cudaLaunchKernel(k.apply, dim3(unsigned(ntiles)), dim3(kScanThreads), a3, 0, s));
+    note_launches(3);
+    return WC_OK;
+}
+
+int mv_join(wc_table *t, uint32_t bits, cudaStream_t s)
+{
+    uint32_t cur = 0;
+    WC_CUDA(cudaMemcpyAsync(&cur, t->status, sizeof(cur), cudaMemcpyDeviceToHost, s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    cur |= bits;
+    WC_CUDA(cudaMemcpyAsync(t->status, &cur, sizeof(cur), cudaMemcpyHostToDevice, s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    return WC_OK;
+}
+
+} // namespace
+
+int wc_mvht_insert(wc_table *t, const void *keys_in, const void *values_in, uint64_t num_in,
+                   wc_stream_t stream, uint64_t probing_length, void *status_out,
+                   int status_handler, uint32_t ignore)
+{
+    int rc = check_table(t, 1 << 3);
+    if (rc) return rc;
+    if (num_in == 0) return WC_OK;
+    if (!keys_in || !values_in) return fail(WC_ERR_INVALID_ARGUMENT, "keys_in / values_in is NULL");
+    const MvKernels k = mv_kernels(t->layout, int(t->cfg.cg_size));
+    if (!k.insert) return fail(WC_ERR_UNSUPPORTED, "no kernel for this configuration");
+    MvArgs a = mv_args(t, keys_in, num_in, probing_length, false, status_out, status_handler,
+                       ignore);
+    a.values = values_in;
+    a.num_keys = t->num_keys;
+    return mv_launch(k.insert, t, num_in, a, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int wc_mvht_num_values(wc_table *t, const void *keys_in, uint64_t num_in, uint64_t *num_out,
+                       uint64_t *num_per_key_out, wc_stream_t stream, uint64_t probing_length,
+                       void *status_out, int status_handler, uint32_t ignore)
+{
+    int rc = check_table(t, 1 << 3);
+    if (rc) return rc;
+    if (!num_out) return fail(WC_ERR_INVALID_ARGUMENT, "num_out is NULL");
+    *num_out = 0;
+    if (num_in == 0) return WC_OK;
+    if (!keys_in) return fail(WC_ERR_INVALID_ARGUMENT, "keys_in is NULL");
+    return mv_count(t, keys_in, num_in, num_per_key_out, num_out,
+                    reinterpret_cast<cudaStream_t>(stream), probing_length, status_out,
+                    status_handler, ignore);
+}
+
+int wc_mvht_retrieve(wc_table *t, const void *keys_in, uint64_t num_in,
+                     uint64_t *begin_offsets_out, uint64_t *end_offsets_out, void *values_out,
+                     uint64_t *num_out, wc_stream_t stream, uint64_t probing_length,
+                     void *status_out, int status_handler, uint32_t ignore)
+{
+    int rc = check_table(t, 1 << 3);
+    if (rc) return rc;
+    if (!num_out) return fail(WC_ERR_INVALID_ARGUMENT, "num_out is NULL");
+    *num_out = 0;
+    if (num_in == 0) return WC_OK;
+    if (!keys_in || !end_offsets_out || (values_out && !begin_offsets_out))
+        return fail(WC_ERR_INVALID_ARGUMENT, "NULL buffer");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    /* pass 1: counts per key into end_offsets (no per-key status) */
+    rc = mv_count(t, keys_in, num_in, end_offsets_out, num_out, s, probing_length, nullptr,
+                  WC_HANDLER_NOTHING, 0);
+    if (rc) return rc;
+    if (!values_out) {
+        /* dry run: per-key counts, status dry_run for every key */
+        if (status_out && status_handler != WC_HANDLER_NOTHING) {
+            const MvScanKernels k = mv_scan_kernels();
+            uint64_t nn = num_in;
+            int h = status_handler;
+            uint32_t mask = (~ignore) ^ 0xFFFu;
+            void *args[] = {&status_out, &nn, &h, &mask};
+            WC_CUDA(cudaLaunchKernel(k.dry_status, dim3(grid_for(k.dry_status, kBlock, num_in, kBlock)),
+                                     dim3(kBlock), args, 0, s));
+            note_launches(1);
+        }
+        return mv_join(t, kStDryRun, s);
+    }
+    /* pass 2: offsets; pass 3: values, each key at its begin offset */
+    rc = mv_scan(t, begin_offsets_out, end_offsets_out, num_in, s);
+    if (rc) return rc;
+    const MvKernels k = mv_kernels(t->layout, int(t->cfg.cg_size));
+    MvArgs a = mv_args(t, keys_in, num_in, probing_length, true, status_out, status_handler,
+                       ignore);
+    a.values_out = values_out;
+    a.begin = reinterpret_cast<const unsigned long long *>(begin_offsets_out);
+    a.end = reinterpret_cast<const unsigned long long *>(end_offsets_out);
+    return mv_launch(k.values, t, num_in, a, s);
+}
+
+int wc_mvht_retrieve_all_keys(wc_table *t, void *keys_out, uint64_t *num_out, wc_stream_t stream)
+{
+    int rc = check_table(t, 1 << 3);
+    if (rc) return rc;
+    if (!num_out) return fail(WC_ERR_INVALID_ARGUMENT, "num_out is NULL");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (!keys_out) {
+        rc = wc_mvht_num_keys(t, stream, num_out);
+        if (rc) return rc;
+        return mv_join(t, kStDryRun, s);
+    }
+    const MvKernels k = mv_kernels(t->layout, int(t->cfg.cg_size));
+    if (!k.unique) return fail(WC_ERR_UNSUPPORTED, "no kernel for this configuration");
+    WC_CUDA(cudaMemsetAsync(t->counter, 0, sizeof(unsigned long long), s));
+    TableView v = view_of(t);
+    uint64_t cap = t->capacity;
+    unsigned long long *cnt = t->counter;
+    void *args[] = {&v, &cap, &keys_out, &cnt};
+    WC_CUDA(cudaLaunchKernel(k.unique, dim3(grid_for(k.unique, kBlock, cap, kBlock)), dim3(kBlock),
+                             args, 0, s));
+    note_launches(1);
+    unsigned long long h = 0;
+    WC_CUDA(cudaMemcpyAsync(&h, t->counter, sizeof(h), cudaMemcpyDeviceToHost, s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    *num_out = h;
+    return WC_OK;
+}
+
+int wc_mvht_num_keys(wc_table *t, wc_stream_t stream, uint64_t *out)
+{
+    int rc = check_table(t, 1 << 3);
+    if (rc) return rc;
+    if (!out) return fail(WC_ERR_INVALID_ARGUMENT, "out is NULL");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    unsigned long long h = 0;
+    WC_CUDA(cudaMemcpyAsync(&h, t->num_keys, sizeof(h), cudaMemcpyDeviceToHost, s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    *out = h;
     return WC_OK;
 }
 

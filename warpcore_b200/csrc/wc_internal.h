@@ -8,6 +8,7 @@
 #include "wc_bloom.cuh"
 #include "wc_batch.cuh"
 #include "wc_fp_kernels.cuh"
+#include "wc_mv.cuh"
 
 namespace warpcore {
 namespace b200 {
@@ -36,6 +37,17 @@ BloomKernel bloom_kernel_ptr(int key_bytes, int slot_bytes, int cg, bool insert)
 /* multi-table batch kernel for a slot layout (KV32 / KV64) and window width;
  * inline_desc selects the variant taking BatchInlineArgs */
 const void *batch_kernel_ptr(int layout, int W, bool inline_desc);
+
+/* MultiValueHashTable kernels of a layout (KV32 / KV64) and window width;
+ * null pointers if not built */
+struct MvKernels {
+    const void *insert = nullptr, *count = nullptr, *values = nullptr, *unique = nullptr;
+};
+MvKernels mv_kernels(int layout, int W);
+struct MvScanKernels {
+    const void *tile_sums, *tile_offsets, *apply, *dry_status;
+};
+MvScanKernels mv_scan_kernels();
 
 /* message returned by wc_last_error() on the calling thread */
 void set_last_error(const char *msg);
