@@ -7,5 +7,6 @@
 #include "hash_set.cuh"
 #include "counting_hash_table.cuh"
 #include "bloom_filter.cuh"
+#include "multi_value_hash_table.cuh"
 
 #endif

@@ -111,6 +111,9 @@ typedef struct wc_table_info {
     unsigned char *fingerprints; /* device pointer to one byte per slot, or NULL:
                                     0 empty, 1 tombstone, else the key's
                                     fingerprint; writers of slot keys keep it */
+    unsigned long long *num_keys; /* multi-value tables: device counter of keys
+                                     holding a value (NULL for other kinds) */
+    uint64_t max_values_per_key;  /* multi-value tables */
 } wc_table_info;
 
 typedef struct wc_table wc_table;

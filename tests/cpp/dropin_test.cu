@@ -301,6 +301,108 @@ static void test_bloom()
     cudaFree(dk); cudaFree(dflag);
 }
 
+/* device per-key MultiValueHashTable methods: each group inserts one pair,
+ * then counts a key's values and reads them */
+template <class Table>
+__global__ void device_mv_insert(Table t, const typename Table::key_type *k,
+                                 const typename Table::value_type *v, uint64_t n, uint32_t *st)
+{
+    const auto g = cg::tiled_partition<Table::cg_size()>(cg::this_thread_block());
+    const uint64_t gid = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / Table::cg_size();
+    if (gid >= n) return;
+    const auto s = t.insert(k[gid], v[gid], g);
+    if (g.thread_rank() == 0) st[gid] = s.base();
+}
+
+template <class Table>
+__global__ void device_mv_read(Table t, const typename Table::key_type *k, uint64_t n,
+                               typename Table::value_type *vals, uint64_t per_key, uint64_t *nums)
+{
+    const auto g = cg::tiled_partition<Table::cg_size()>(cg::this_thread_block());
+    const uint64_t gid = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / Table::cg_size();
+    if (gid >= n) return;
+    typename Table::index_type num = 0, num2 = 0;
+    t.num_values(k[gid], num, g);
+    t.retrieve(k[gid], vals + gid * per_key, num2, g);
+    if (g.thread_rank() == 0) nums[gid] = num == num2 ? num : ~0ull;
+}
+
+static void test_multi_value()
+{
+    using T = wc::MultiValueHashTable<uint64_t, uint64_t>;
+    const uint64_t n = 3000;
+    T t(4 * n, wc::defaults::seed<uint64_t>(), 3);
+    auto keys = distinct_keys<uint64_t>(n + 100, 91);
+    std::vector<uint64_t> k(keys.begin(), keys.begin() + n);
+    uint64_t *dk = dcopy(k);
+    /* host bulk: two rounds with values r * 10^6 + i */
+    for (uint64_t r = 0; r < 2; r++) {
+        std::vector<uint64_t> v(n);
+        for (uint64_t i = 0; i < n; i++) v[i] = r * 1000000 + i;
+        uint64_t *dv = dcopy(v);
+        t.insert(dk, dv, n);
+        cudaFree(dv);
+    }
+    /* device per-key: a third round, then a fourth that hits max 3 */
+    uint32_t *dst;
+    cudaMalloc(&dst, sizeof(uint32_t) * n);
+    for (uint64_t r = 2; r < 4; r++) {
+        std::vector<uint64_t> v(n);
+        for (uint64_t i = 0; i < n; i++) v[i] = r * 1000000 + i;
+        uint64_t *dv = dcopy(v);
+        device_mv_insert<<<blocks_for(n, T::cg_size()), 256>>>(t, dk, dv, n, dst);
+        auto st = hcopy(dst, n);
+        const uint32_t want = r == 2 ? wc::Status::duplicate_key().base()
+                                     : (wc::Status::duplicate_key() + wc::Status::max_values_for_key_reached()).base();
+        CHECK(std::all_of(st.begin(), st.end(), [&](uint32_t s) { return s == want; }));
+        cudaFree(dv);
+    }
+    CHECK(t.size() == 3 * n);
+    CHECK(t.num_keys() == n);
+    /* host bulk retrieve: begin/end offsets and values in insertion order */
+    std::vector<uint64_t> q(keys.begin(), keys.end());
+    uint64_t *dq = dcopy(q), *db, *de, *dvals;
+    cudaMalloc(&db, sizeof(uint64_t) * q.size());
+    cudaMalloc(&de, sizeof(uint64_t) * q.size());
+    T::index_type num_out = 0;
+    t.retrieve(dq, q.size(), db, de, nullptr, num_out);
+    CHECK(num_out == 3 * n);
+    cudaMalloc(&dvals, sizeof(uint64_t) * num_out);
+    t.retrieve(dq, q.size(), db, de, dvals, num_out);
+    auto b = hcopy(db, q.size()), e = hcopy(de, q.size()), vals = hcopy(dvals, num_out);
+    bool ok = true;
+    for (uint64_t i = 0; i < n; i++) {
+        ok &= b[i] == 3 * i && e[i] == 3 * i + 3;
+        for (uint64_t r = 0; r < 3; r++) ok &= vals[3 * i + r] == r * 1000000 + i;
+    }
+    for (uint64_t i = n; i < q.size(); i++) ok &= e[i] == b[i];
+    CHECK(ok);
+    /* device per-key read */
+    uint64_t *dvv, *dnums;
+    cudaMalloc(&dvv, sizeof(uint64_t) * 3 * n);
+    cudaMalloc(&dnums, sizeof(uint64_t) * n);
+    device_mv_read<<<blocks_for(n, T::cg_size()), 256>>>(t, dk, n, dvv, 3, dnums);
+    auto nums = hcopy(dnums, n);
+    auto vv = hcopy(dvv, 3 * n);
+    ok = true;
+    for (uint64_t i = 0; i < n; i++) {
+        ok &= nums[i] == 3;
+        for (uint64_t r = 0; r < 3; r++) ok &= vv[3 * i + r] == r * 1000000 + i;
+    }
+    CHECK(ok);
+    /* unique keys */
+    T::index_type nk = 0;
+    uint64_t *duk;
+    cudaMalloc(&duk, sizeof(uint64_t) * n);
+    t.retrieve_all_keys(duk, nk);
+    auto uk = hcopy(duk, nk);
+    std::sort(uk.begin(), uk.end());
+    std::sort(k.begin(), k.end());
+    CHECK(nk == n && uk == k);
+    cudaFree(dk); cudaFree(dst); cudaFree(dq); cudaFree(db); cudaFree(de); cudaFree(dvals);
+    cudaFree(dvv); cudaFree(dnums); cudaFree(duk);
+}
+
 int main()
 {
     test_svht_u32();
@@ -308,6 +410,7 @@ int main()
     test_hash_set();
     test_counting();
     test_bloom();
+    test_multi_value();
     const cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         std::fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(e));

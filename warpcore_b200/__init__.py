@@ -80,6 +80,8 @@ class TableInfo(ctypes.Structure):
         ("status", ctypes.c_void_p),
         ("is_initialized", ctypes.c_int),
         ("fingerprints", ctypes.c_void_p),
+        ("num_keys", ctypes.c_void_p),
+        ("max_values_per_key", ctypes.c_uint64),
     ]
 
 

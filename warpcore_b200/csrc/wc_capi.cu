@@ -874,6 +874,8 @@ int wc_table_get_info(const wc_table *t, wc_table_info *info)
     info->status = t->status;
     info->is_initialized = t->initialized ? 1 : 0;
     info->fingerprints = t->fps;
+    info->num_keys = t->kind == 3 ? t->num_keys : nullptr;
+    info->max_values_per_key = t->max_values;
     return WC_OK;
 }
 

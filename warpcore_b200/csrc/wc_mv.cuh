@@ -19,6 +19,7 @@
 #define WC_MV_CUH
 
 #include "wc_kernels.cuh"
+#include <warpcore/detail/mv_ops.cuh>
 
 namespace warpcore {
 namespace b200 {
@@ -41,41 +42,6 @@ struct MvArgs {
     int handler;
 };
 
-/* one bucket: bit s of hits / empties = slot s holds key / is empty; the
- * functor gets (slot, LaneWords, index within the vector) for every hit in
- * slot order */
-template <class L, int W, class OnHit>
-__device__ __forceinline__ void mv_bucket(const TableView &t, uint64_t bucket,
-                                          typename L::key_t key, uint32_t &hits,
-                                          uint32_t &empties, OnHit on_hit)
-{
-    using K = typename L::key_t;
-    constexpr int SB = L::kSlotBytes;
-    constexpr int WB = W * SB;
-    constexpr int LB = WB < 16 ? WB : 16;
-    constexpr int NV = WB / LB;
-    constexpr int SPL = LB / SB;
-    const K empty = K(t.empty_key);
-    const unsigned char *const base =
-        reinterpret_cast<const unsigned char *>(t.slots) + bucket * uint64_t(WB);
-    hits = 0;
-    empties = 0;
-#pragma unroll 4
-    for (int v = 0; v < NV; ++v) {
-        const LaneWords lw = load_lane<LB>(base + v * LB);
-#pragma unroll
-        for (int s = 0; s < SPL; ++s) {
-            const K k = slot_key<L>(lw, s);
-            const int idx = v * SPL + s;
-            if (k == key) {
-                hits |= 1u << idx;
-                on_hit(idx, lw, s);
-            }
-            if (k == empty) empties |= 1u << idx;
-        }
-    }
-}
-
 __device__ __forceinline__ void mv_write_status(const MvArgs &a, uint64_t i, uint32_t st)
 {
     if (!a.status_out) return;
@@ -90,63 +56,18 @@ __global__ void __launch_bounds__(256) mv_insert_kernel(const MvArgs a)
 {
     using K = typename L::key_t;
     using V = typename L::val_t;
-    constexpr int SB = L::kSlotBytes;
-    const TableView &t = a.t;
-    const K empty = K(t.empty_key), tomb = K(t.tombstone_key);
-    unsigned char *const slots = reinterpret_cast<unsigned char *>(t.slots);
     uint32_t join = 0;
     unsigned long long new_keys = 0;
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.n; i += stride) {
-        const K key = reinterpret_cast<const K *>(a.keys)[i];
-        const V val = reinterpret_cast<const V *>(a.values)[i];
-        uint32_t st = kStNone;
-        if (key == empty || key == tomb) {
-            st = kStInvalidKey;
-            join |= st;
-        } else {
-            uint64_t b = probe_begin<K>(t, key), step = 0, wins = 0, num = 0;
-            for (;;) {
-                uint32_t hits, emp;
-                mv_bucket<L, W>(t, b, key, hits, emp, [](int, const LaneWords &, int) {});
-                num += __popc(hits);
-                if (num >= a.max_values) {
-                    st = kStDuplicateKey | kStMaxValuesReached;
-                    join |= st;
-                    break;
-                }
-                bool done = false;
-                while (emp) {
-                    const int s = __ffs(emp) - 1;
-                    unsigned char *const sp = slots + (b * W + uint64_t(s)) * SB;
-                    K old;
-                    if (claim_slot<L>(sp, empty, key, val, old)) {
-                        if (num == 0) ++new_keys;
-                        st = num ? kStDuplicateKey : kStNone;
-                        done = true;
-                        break;
-                    }
-                    if (old == key) {
-                        /* an equal key claimed this slot first: one more value */
-                        if (++num >= a.max_values) {
-                            st = kStDuplicateKey | kStMaxValuesReached;
-                            join |= st;
-                            done = true;
-                            break;
-                        }
-                    }
-                    emp &= emp - 1u;
-                }
-                if (done) break;
-                if (++wins >= a.max_windows) {
-                    st = kStProbingLengthExceeded | (num ? kStDuplicateKey : kStNone);
-                    join |= st;
-                    break;
-                }
-                if (wins == 1) step = probe_step<K>(t, key);
-                b = probe_next(t, b, step);
-            }
-        }
+        bool fresh = false;
+        const uint32_t st = mv_insert_one<L, W>(a.t, reinterpret_cast<const K *>(a.keys)[i],
+                                                reinterpret_cast<const V *>(a.values)[i],
+                                                a.max_windows, a.max_values, fresh);
+        /* the reference joins every status but the plain duplicate_key of
+         * a successful insert (:266-268) */
+        if (st != kStNone && st != kStDuplicateKey) join |= st;
+        new_keys += fresh;
         mv_write_status(a, i, st);
     }
     /* every lane of the warp arrives here (no early exits) */
@@ -154,7 +75,7 @@ __global__ void __launch_bounds__(256) mv_insert_kernel(const MvArgs a)
     const uint32_t wj = __reduce_or_sync(kFull, join);
     if ((threadIdx.x & 31) == 0) {
         if (nk) atomicAdd(a.num_keys, nk);
-        join_status(t.status, wj);
+        join_status(a.t.status, wj);
     }
 }
 
@@ -164,55 +85,28 @@ __global__ void __launch_bounds__(256) mv_find_kernel(const MvArgs a)
 {
     using K = typename L::key_t;
     using V = typename L::val_t;
-    const TableView &t = a.t;
-    const K empty = K(t.empty_key), tomb = K(t.tombstone_key);
     uint32_t join = 0;
     unsigned long long total = 0;
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.n; i += stride) {
-        const K key = reinterpret_cast<const K *>(a.keys)[i];
-        uint32_t st = kStNone;
         uint64_t num = 0;
-        if (key == empty || key == tomb) {
-            st = kStInvalidKey;
-            join |= st;
-        } else {
-            V *const out = kValues ? reinterpret_cast<V *>(a.values_out) + a.begin[i] : nullptr;
+        uint32_t st;
+        if constexpr (kValues) {
             /* values are written inside the key's own segment only; more
              * values than the counting pass saw mean the table changed in
-             * between (invalid_phase_overlap below) */
-            const uint64_t room = kValues ? a.end[i] - a.begin[i] : 0;
-            uint64_t b = probe_begin<K>(t, key), step = 0, wins = 0;
-            for (;;) {
-                uint32_t hits, emp;
-                mv_bucket<L, W>(t, b, key, hits, emp, [&](int, const LaneWords &lw, int s) {
-                    if constexpr (kValues) {
-                        if (num < room) out[num] = slot_val<L>(lw, s);
-                    }
-                    ++num;
-                });
-                if (emp || num >= a.max_values) {
-                    if (num == 0) {
-                        st = kStKeyNotFound;
-                        join |= st;
-                    }
-                    break;
-                }
-                if (++wins >= a.max_windows) {
-                    st = kStProbingLengthExceeded;
-                    join |= st;
-                    break;
-                }
-                if (wins == 1) step = probe_step<K>(t, key);
-                b = probe_next(t, b, step);
-            }
-            if constexpr (kValues) {
-                if (num != a.end[i] - a.begin[i]) {
-                    st |= kStInvalidPhaseOverlap;
-                    join |= kStInvalidPhaseOverlap;
-                }
-            }
+             * between (invalid_phase_overlap) */
+            V *const out = reinterpret_cast<V *>(a.values_out) + a.begin[i];
+            const uint64_t room = a.end[i] - a.begin[i];
+            st = mv_for_each_one<L, W>(a.t, reinterpret_cast<const K *>(a.keys)[i], a.max_windows,
+                                       a.max_values, num, [&](V v, uint64_t j) {
+                                           if (j < room) out[j] = v;
+                                       });
+            if (st != kStInvalidKey && num != room) st |= kStInvalidPhaseOverlap;
+        } else {
+            st = mv_for_each_one<L, W>(a.t, reinterpret_cast<const K *>(a.keys)[i], a.max_windows,
+                                       a.max_values, num, [](V, uint64_t) {});
         }
+        join |= st;
         if (a.counts_out) a.counts_out[i] = num;
         total += num;
         mv_write_status(a, i, st);
@@ -225,7 +119,7 @@ __global__ void __launch_bounds__(256) mv_find_kernel(const MvArgs a)
     if ((threadIdx.x & 31) == 0) {
         const unsigned long long sum = (unsigned long long)lo + ((unsigned long long)hi << 32);
         if (a.total && sum) atomicAdd(a.total, sum);
-        join_status(t.status, wj);
+        join_status(a.t.status, wj);
     }
 }
 
