@@ -15,6 +15,7 @@
 #include <warpcore/hash_set.cuh>
 #include <warpcore/counting_hash_table.cuh>
 #include <warpcore/bloom_filter.cuh>
+#include <warpcore/multi_value_hash_table.cuh>
 
 #include <cfloat>
 #include <cstdint>
@@ -164,6 +165,36 @@ int ref_bloom64_run(const uint64_t *keys, uint64_t n, const uint64_t *q, uint64_
         tm.start();
         f.retrieve(q, nq, flags);
         br = fminf(br, tm.stop());
+    }
+    *ms_insert = bi;
+    *ms_retrieve = br;
+    return int(cudaDeviceSynchronize());
+}
+
+/* MultiValueHashTable<u32,u32>: bulk insert, then the two-phase bulk
+ * retrieve (counts, scan, values; it synchronises) into caller buffers of
+ * at least the number of values */
+int ref_mv32_run(const uint32_t *keys, const uint32_t *vals, uint64_t n, const uint32_t *q,
+                 uint64_t nq, uint64_t *begin, uint64_t *end, uint32_t *values_out,
+                 uint64_t *num_out, uint64_t min_cap, int reps, float *ms_insert,
+                 float *ms_retrieve, uint64_t *capacity)
+{
+    using Table = wc::MultiValueHashTable<uint32_t, uint32_t>;
+    Table t(min_cap);
+    *capacity = t.capacity();
+    Timer tm;
+    float bi = FLT_MAX, br = FLT_MAX;
+    for (int r = 0; r < reps; ++r) {
+        t.init();
+        cudaDeviceSynchronize();
+        tm.start();
+        t.insert(keys, vals, n);
+        bi = fminf(bi, tm.stop());
+        wc::index_t num = 0;
+        tm.start();
+        t.retrieve(q, nq, (wc::index_t *)begin, (wc::index_t *)end, values_out, num);
+        br = fminf(br, tm.stop());
+        *num_out = num;
     }
     *ms_insert = bi;
     *ms_retrieve = br;

@@ -198,6 +198,30 @@ class Workload:
             self.table = wc.CountingHashTable(int(distinct / load), key_bytes=4)
             self.out = torch.empty(self.q, dtype=torch.int32, device=device)
             self.bytes_insert, self.bytes_retrieve = 4 + 32 + 32, 4 + 4 + 1 + 32
+        elif kind == "mv32":
+            # 2^(L-2) distinct keys with 4 values each, inserted as 2^L pairs
+            # in one shuffled batch; retrieve every key plus as many absent
+            distinct = n >> 2
+            self.distinct = distinct
+            keys = unique_keys32(0, 2 * distinct, seed, device)
+            idx = (torch.arange(n, device=device) % distinct)[
+                torch.randperm(n, device=device, generator=gen)]
+            self.keys = keys[:distinct][idx].contiguous()
+            self.values = uniform_values(n, 4, gen, device)
+            self.queries = keys.contiguous()
+            self.q = 2 * distinct
+            # per-key checksums of the values: sum and sum of squares (wrapping)
+            v64 = self.values.to(torch.int64) & 0xFFFFFFFF
+            self.exp_sum = torch.zeros(distinct, dtype=torch.int64, device=device).index_add_(0, idx, v64)
+            self.exp_sq = torch.zeros(distinct, dtype=torch.int64, device=device).index_add_(0, idx, v64 * v64)
+            self.table = wc.MultiValueHashTable(int(n / load), key_bytes=4)
+            self.begin = torch.empty(self.q, dtype=torch.int64, device=device)
+            self.end = torch.empty(self.q, dtype=torch.int64, device=device)
+            self.out = torch.empty(n, dtype=torch.int32, device=device)
+            # insert: pair in + one window sector read + written; retrieve:
+            # key in, offsets out, two window sectors (count and values
+            # passes), 2 values per query out on average
+            self.bytes_insert, self.bytes_retrieve = 4 + 4 + 32 + 32, 4 + 16 + 32 + 32 + 8
         elif kind == "bloom64":
             keys = unique_keys64(0, 2 * n, seed, device)
             self.keys = keys[:n].contiguous()
@@ -222,7 +246,7 @@ class Workload:
     def insert(self, stream):
         if self.sharded:
             self.table.insert(self.keys, self.values)
-        elif self.kind in ("svht32", "svht64"):
+        elif self.kind in ("svht32", "svht64", "mv32"):
             self.table.insert(self.keys, self.values, stream=stream)
         else:
             self.table.insert(self.keys, stream=stream)
@@ -230,6 +254,8 @@ class Workload:
     def retrieve(self, stream):
         if self.sharded:
             self.table.retrieve(self.queries, self.out)
+        elif self.kind == "mv32":
+            self.table.retrieve(self.queries, self.begin, self.end, self.out, stream=stream)
         else:
             self.table.retrieve(self.queries, self.out, stream=stream)
 
@@ -251,7 +277,23 @@ class Workload:
             return bool(torch.equal(got[present], self.hist[present]))
         if self.kind == "bloom64":
             return bool(out[self.n:].all())
+        if self.kind == "mv32":
+            return self.mv_ok(self.begin, self.end, out)
         return False
+
+    def mv_ok(self, begin, end, values):
+        """every key has its 4 values (per-key sum and sum of squares),
+        absent keys none"""
+        import torch
+        d = self.distinct
+        cnt = end - begin
+        if not (bool((cnt[:d] == 4).all()) and bool((cnt[d:] == 0).all())):
+            return False
+        v64 = values[: 4 * d].to(torch.int64) & 0xFFFFFFFF
+        seg = torch.repeat_interleave(torch.arange(self.q, device=v64.device), cnt)
+        s1 = torch.zeros(d, dtype=torch.int64, device=v64.device).index_add_(0, seg, v64)
+        s2 = torch.zeros(d, dtype=torch.int64, device=v64.device).index_add_(0, seg, v64 * v64)
+        return bool(torch.equal(s1, self.exp_sum)) and bool(torch.equal(s2, self.exp_sq))
 
     def verify(self):
         """size-independent properties of one fresh step"""
@@ -284,6 +326,11 @@ class Workload:
             self.retrieve(s)
             torch.cuda.synchronize()
             return bool(self.out[self.n:].all())
+        if self.kind == "mv32":
+            self.retrieve(s)
+            torch.cuda.synchronize()
+            return (self.mv_ok(self.begin, self.end, self.out) and self.table.size() == self.n
+                    and self.table.num_keys() == self.distinct)
         return False
 
 
@@ -306,6 +353,7 @@ def reference_gpu(wl, reps=5):
     torch.cuda.synchronize()
     out = torch.empty_like(wl.out)
     min_cap = int(wl.n / wl.load) if wl.kind != "counting32" else int(wl.distinct / wl.load)
+    rb = re_ = None
     if wl.kind in ("svht64", "svht32"):
         fn = lib.ref_svht64_run if wl.kind == "svht64" else lib.ref_svht32_run
         rc = fn(vp(wl.keys.data_ptr()), vp(wl.values.data_ptr()), u64(wl.n),
@@ -320,6 +368,14 @@ def reference_gpu(wl, reps=5):
         rc = lib.ref_counting32_run(vp(wl.keys.data_ptr()), u64(wl.n), vp(wl.queries.data_ptr()),
                                     u64(wl.q), vp(out.data_ptr()), u64(min_cap), ctypes.c_int(reps),
                                     ctypes.byref(ti), ctypes.byref(tr), ctypes.byref(cap))
+    elif wl.kind == "mv32":
+        rb, re_ = torch.empty_like(wl.begin), torch.empty_like(wl.end)
+        num = ctypes.c_uint64(0)
+        rc = lib.ref_mv32_run(vp(wl.keys.data_ptr()), vp(wl.values.data_ptr()), u64(wl.n),
+                              vp(wl.queries.data_ptr()), u64(wl.q), vp(rb.data_ptr()),
+                              vp(re_.data_ptr()), vp(out.data_ptr()), ctypes.byref(num),
+                              u64(min_cap), ctypes.c_int(reps), ctypes.byref(ti), ctypes.byref(tr),
+                              ctypes.byref(cap))
     elif wl.kind == "bloom64":
         rc = lib.ref_bloom64_run(vp(wl.keys.data_ptr()), u64(wl.n), vp(wl.queries.data_ptr()),
                                  u64(wl.q), vp(out.data_ptr()), u64(16 * wl.n), u64(8),
@@ -330,7 +386,7 @@ def reference_gpu(wl, reps=5):
     if rc != 0:
         return {"error": "CUDA error %d" % rc}
     # the reference's answers on the same inputs must equal ours
-    same = wl.answers_ok(out)
+    same = wl.mv_ok(rb, re_, out) if wl.kind == "mv32" else wl.answers_ok(out)
     ins_g = wl.n / (ti.value * 1e-3) / 1e9
     ret_g = wl.q / (tr.value * 1e-3) / 1e9
     return {"insert_gops": round(ins_g, 4), "retrieve_gops": round(ret_g, 4),
@@ -348,6 +404,8 @@ WORKLOAD_NAMES = {
     "hashset64": "HashSet<u64> CG16 LF{LF}: insert 2^{L} + contains 2^{L} (50% hit)",
     "counting32": "CountingHashTable<u32,u32> CG4 LF0.85: insert 2^{L} Zipf(1.1) + retrieve distinct+absent",
     "bloom64": "BloomFilter<u64,Murmur64,u64,CG8> 16 bits/key k=8: insert 2^{L} + query 2^{L1}",
+    "mv32": "MultiValueHashTable<u32,u32> CG8 LF{LF}: insert 2^{L} pairs (4 values per key, "
+            "one shuffled batch) + retrieve every key and as many absent keys",
     "served": "4096 SingleValueHashTable<u32,u32> (caps log-uniform 2^10..2^22, LF 0.85), "
               "Poisson requests (batch 2^6..2^18, 30% insert, 80% hit): continuous batching vs plain launches",
 }
@@ -528,7 +586,7 @@ def run_e2e(wl, stream, args, world):
     d2h = ho.numel() * ho.element_size()
     keys0, vals0, q0 = wl.keys, wl.values, wl.queries
     steps = max(1, min(args.steps, 3))
-    piped = hasattr(wl.table, "insert_from_host") and not wl.sharded
+    piped = hasattr(wl.table, "insert_from_host") and not wl.sharded and wl.kind != "mv32"
     if piped:
         # host buffers straight into the C ABI: chunks of 2^22 keys, copy-in
         # / kernel / copy-out overlapped; a miss gets the fill value the
@@ -736,8 +794,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="svht64", choices=sorted(WORKLOAD_NAMES))
-    ap.add_argument("--log2n", type=int, default=27)
-    ap.add_argument("--load", type=float, default=0.9)
+    ap.add_argument("--log2n", type=int, default=None,
+                    help="keys per step (2^L); default 27, or 24 pairs for mv32")
+    ap.add_argument("--load", type=float, default=None,
+                    help="target load factor; default 0.9, or 0.8 for mv32")
     ap.add_argument("--cpu-log2n", type=int, default=24)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--shard", action="store_true",
@@ -749,6 +809,10 @@ def main():
     ap.add_argument("--requests", type=int, default=8192)
     ap.add_argument("--rates", default="100000,300000,1000000")
     args = ap.parse_args()
+    if args.log2n is None:
+        args.log2n = 24 if args.workload == "mv32" else 27
+    if args.load is None:
+        args.load = 0.8 if args.workload == "mv32" else 0.9
     if args.warmup < 3:
         log("warm-up raised to 3 steps")
         args.warmup = 3

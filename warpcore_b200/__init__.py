@@ -371,8 +371,8 @@ class _Table:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib().wc_table_destroy(h)
+        if h is not None and h.value and _lib is not None:
+            _lib.wc_table_destroy(h)
             self._h = None
 
     def info(self):
