@@ -91,6 +91,35 @@ def test_cpp_dropin_program_with_fingerprints():
     assert "dropin ok" in r.stdout
 
 
+@pytest.mark.parametrize("kb", [4, 8])
+def test_near_duplicates_inserted_once(kb):
+    # every key twice, 40 positions apart: the second copy reaches its lane
+    # while the first one's claim is in flight in the same warp; it must
+    # see that claim (duplicate_key) and not take a second slot
+    n = 200_000
+    cap = 4 * n
+    t = wc.SingleValueHashTable(cap, key_bytes=kb)
+    ref = o.Table(o.SVHT, kb, kb, cap)
+    keys = o.gen_unique_keys(kb, n, 1201 + kb)
+    vals = o.gen_uniform(kb, n, 1202)
+    blk = 40
+    m = n // blk * blk
+    kk = keys[:m].reshape(-1, blk)
+    vv = vals[:m].reshape(-1, blk)
+    bk = np.concatenate([kk, kk], axis=1).ravel()
+    bv = np.concatenate([vv, vv], axis=1).ravel()
+    st = empty_dev(len(bk), 4)
+    t.insert(dev(bk), dev(bv), status_out=st)
+    want = ref.insert(bk, bv, want_status=True)
+    got = host(st)
+    a, b = np.lexsort((got, bk)), np.lexsort((want, bk))
+    assert np.array_equal(got[a], want[b])
+    assert t.size() == ref.size() == m
+    out = empty_dev(m, kb)
+    t.retrieve(dev(keys[:m]), out)
+    assert np.array_equal(host(out), vals[:m])
+
+
 @pytest.mark.parametrize("kind", ["svht32", "set32", "svht64"])
 def test_large_insert_rebuilds_fingerprints(kind):
     # a table whose fingerprints exceed half of L2 and a batch above 1/8 of

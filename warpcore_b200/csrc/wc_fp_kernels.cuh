@@ -12,7 +12,9 @@
  *     windows, and the fingerprint array (1 byte per slot, 1/16 of a u64
  *     pair table) mostly stays in L2;
  *   - a hit costs the fingerprint words plus one slot, read with an
- *     evict-first hint so that slot lines do not push fingerprints out.
+ *     evict-first hint so that slot lines do not push fingerprints out
+ *     (retrieve, erase), or from L2 without an L1 copy (inserts: a claim's
+ *     compare-and-swap lands in L2, and an equal key's lane must see it).
  *
  * Each lane owns one key and issues one memory operation per wave: a
  * fingerprint load, a candidate slot load, or a compare-and-swap claim.
@@ -41,7 +43,8 @@ namespace b200 {
 #endif
 
 /* L2 eviction priorities: fingerprint lines are loaded and stored with
- * evict_last and slot lines read with evict_first (ld.cs), so that the
+ * evict_last and slot lines read by retrieve and erase with evict_first
+ * (ld.cs), so that the
  * random slot traffic of a table larger than L2 evicts slot lines before
  * fingerprint lines (a fingerprint byte written into an evicted sector
  * costs a DRAM read to merge). */
@@ -341,8 +344,13 @@ __global__ void __launch_bounds__(256, (OP == kOpRetrieve || OP == kOpErase) ? W
             } else if (phase == kPhaseCheck) {
                 const int s = __ffs(cand) - 1;
                 unsigned char *const sp = slots + (base_slot + uint64_t(s)) * SB;
-                const LaneWords sw = load_slot_once<L>(sp);
-                if (slot_key<L>(sw, 0) == key) {
+                /* inserts read the slot where the claims' atomics land (L2):
+                 * an L1 copy may predate the claim of an equal key by
+                 * another lane, which would then be inserted twice */
+                const LaneWords sw = (OP == kOpInsert || OP == kOpCount) ? load_lane<SB>(sp)
+                                                                         : load_slot_once<L>(sp);
+                const K sk = slot_key<L>(sw, 0);
+                if (sk == key) {
                     if constexpr (OP == kOpRetrieve) {
                         st = kStNone;
                         flag = true;
@@ -368,6 +376,9 @@ __global__ void __launch_bounds__(256, (OP == kOpRetrieve || OP == kOpErase) ? W
                     }
                     pending = false;
                 } else {
+                    /* a set fingerprint over a key that reads empty is
+                     * left to the compare-and-swap, which sees the key */
+                    if ((OP == kOpInsert || OP == kOpCount) && sk == empty) emp |= 1u << s;
                     cand &= cand - 1u;
                 }
             } else if (phase == kPhasePreload) {
