@@ -16,6 +16,7 @@
 #include <warpcore/counting_hash_table.cuh>
 #include <warpcore/bloom_filter.cuh>
 #include <warpcore/multi_value_hash_table.cuh>
+#include <warpcore/multi_bucket_hash_table.cuh>
 
 #include <cfloat>
 #include <cstdint>
@@ -78,6 +79,41 @@ int run_table(const K *keys, const V *vals, uint64_t n, const K *q, uint64_t nq,
 }
 
 } // namespace
+
+/* MultiBucketHashTable<u32,u32> with AoSStore<u32, ArrayBucket<u32, B>>
+ * (the reference's multi_bucket benchmark types), B = 1, 2, 4 or 8: bulk
+ * insert, then the two-phase bulk retrieve */
+template <uint32_t B>
+static int ref_mb32(const uint32_t *keys, const uint32_t *vals, uint64_t n, const uint32_t *q,
+                    uint64_t nq, uint64_t *begin, uint64_t *end, uint32_t *values_out,
+                    uint64_t *num_out, uint64_t min_cap, int reps, float *ms_insert,
+                    float *ms_retrieve, uint64_t *capacity)
+{
+    using Table = wc::MultiBucketHashTable<
+        uint32_t, uint32_t, wc::defaults::empty_key<uint32_t>(),
+        wc::defaults::tombstone_key<uint32_t>(), wc::defaults::empty_key<uint32_t>(),
+        wc::defaults::probing_scheme_t<uint32_t, 8>,
+        wc::storage::key_value::AoSStore<uint32_t, wc::ArrayBucket<uint32_t, B>>>;
+    Table t(min_cap);
+    *capacity = t.capacity();
+    Timer tm;
+    float bi = FLT_MAX, br = FLT_MAX;
+    for (int r = 0; r < reps; ++r) {
+        t.init();
+        cudaDeviceSynchronize();
+        tm.start();
+        t.insert(keys, vals, n);
+        bi = fminf(bi, tm.stop());
+        wc::index_t num = 0;
+        tm.start();
+        t.retrieve(q, nq, (wc::index_t *)begin, (wc::index_t *)end, values_out, num);
+        br = fminf(br, tm.stop());
+        *num_out = num;
+    }
+    *ms_insert = bi;
+    *ms_retrieve = br;
+    return int(cudaDeviceSynchronize());
+}
 
 extern "C" {
 
@@ -199,6 +235,20 @@ int ref_mv32_run(const uint32_t *keys, const uint32_t *vals, uint64_t n, const u
     *ms_insert = bi;
     *ms_retrieve = br;
     return int(cudaDeviceSynchronize());
+}
+
+int ref_mb32_run(const uint32_t *keys, const uint32_t *vals, uint64_t n, const uint32_t *q,
+                 uint64_t nq, uint64_t *begin, uint64_t *end, uint32_t *values_out,
+                 uint64_t *num_out, uint64_t min_cap, uint32_t bucket, int reps, float *ms_insert,
+                 float *ms_retrieve, uint64_t *capacity)
+{
+    switch (bucket) {
+    case 1: return ref_mb32<1>(keys, vals, n, q, nq, begin, end, values_out, num_out, min_cap, reps, ms_insert, ms_retrieve, capacity);
+    case 2: return ref_mb32<2>(keys, vals, n, q, nq, begin, end, values_out, num_out, min_cap, reps, ms_insert, ms_retrieve, capacity);
+    case 4: return ref_mb32<4>(keys, vals, n, q, nq, begin, end, values_out, num_out, min_cap, reps, ms_insert, ms_retrieve, capacity);
+    case 8: return ref_mb32<8>(keys, vals, n, q, nq, begin, end, values_out, num_out, min_cap, reps, ms_insert, ms_retrieve, capacity);
+    default: return -1;
+    }
 }
 
 } // extern "C"

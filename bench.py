@@ -132,7 +132,7 @@ from warpcore_b200.datagen import (unique_keys32, unique_keys64,  # noqa: E402
 class Workload:
     """one step = init + insert(n) + retrieve(q) on resident inputs"""
 
-    def __init__(self, kind, log2n, load, rank, device, world=1, shard=False):
+    def __init__(self, kind, log2n, load, rank, device, world=1, shard=False, bucket=2):
         import torch
         import warpcore_b200 as wc
         self.kind = kind
@@ -222,6 +222,36 @@ class Workload:
             # key in, offsets out, two window sectors (count and values
             # passes), 2 values per query out on average
             self.bytes_insert, self.bytes_retrieve = 4 + 4 + 32 + 32, 4 + 16 + 32 + 32 + 8
+        elif kind == "mb32":
+            # the reference's multi_bucket benchmark: 2^L values, key of input
+            # i = i mod 2^(L-3) + 1 (8 values per key, copies 2^(L-3) apart);
+            # queries 1 .. 2^L (one in 8 present); table capacity for key
+            # load 0.8 of a B-bucket table; values uniform and non-zero
+            distinct = n >> 3
+            self.distinct = distinct
+            self.per_key = 8
+            idx = torch.arange(n, device=device) % distinct
+            self.keys = (idx + 1).to(torch.int32).contiguous()
+            self.values = uniform_values(n, 4, gen, device)
+            self.values[self.values == 0] = 1
+            self.queries = (torch.arange(n, device=device) + 1).to(torch.int32).contiguous()
+            self.q = n
+            v64 = self.values.to(torch.int64) & 0xFFFFFFFF
+            self.exp_sum = torch.zeros(distinct, dtype=torch.int64, device=device).index_add_(0, idx, v64)
+            self.exp_sq = torch.zeros(distinct, dtype=torch.int64, device=device).index_add_(0, idx, v64 * v64)
+            b = bucket
+            self.bucket = b
+            cap = int(n * (4 + 4) / (4 + 4 * b) / load)
+            self.table = wc.MultiBucketHashTable(cap, key_bytes=4, value_bytes=4, bucket_size=b)
+            self.min_cap = cap
+            self.begin = torch.empty(self.q, dtype=torch.int64, device=device)
+            self.end = torch.empty(self.q, dtype=torch.int64, device=device)
+            self.out = torch.empty(n, dtype=torch.int32, device=device)
+            # insert: pair in + the key window's sector read and written +
+            # the bucket's sector written; retrieve: key in, offsets out,
+            # the window sector in the count and value passes, one value out
+            # per query on average
+            self.bytes_insert, self.bytes_retrieve = 4 + 4 + 32 + 32, 4 + 16 + 32 + 32 + 4
         elif kind == "bloom64":
             keys = unique_keys64(0, 2 * n, seed, device)
             self.keys = keys[:n].contiguous()
@@ -246,7 +276,7 @@ class Workload:
     def insert(self, stream):
         if self.sharded:
             self.table.insert(self.keys, self.values)
-        elif self.kind in ("svht32", "svht64", "mv32"):
+        elif self.kind in ("svht32", "svht64", "mv32", "mb32"):
             self.table.insert(self.keys, self.values, stream=stream)
         else:
             self.table.insert(self.keys, stream=stream)
@@ -254,7 +284,7 @@ class Workload:
     def retrieve(self, stream):
         if self.sharded:
             self.table.retrieve(self.queries, self.out)
-        elif self.kind == "mv32":
+        elif self.kind in ("mv32", "mb32"):
             self.table.retrieve(self.queries, self.begin, self.end, self.out, stream=stream)
         else:
             self.table.retrieve(self.queries, self.out, stream=stream)
@@ -277,19 +307,20 @@ class Workload:
             return bool(torch.equal(got[present], self.hist[present]))
         if self.kind == "bloom64":
             return bool(out[self.n:].all())
-        if self.kind == "mv32":
+        if self.kind in ("mv32", "mb32"):
             return self.mv_ok(self.begin, self.end, out)
         return False
 
     def mv_ok(self, begin, end, values):
-        """every key has its 4 values (per-key sum and sum of squares),
-        absent keys none"""
+        """every key has its values (per-key count, sum and sum of
+        squares), absent keys none"""
         import torch
         d = self.distinct
+        per = getattr(self, "per_key", 4)
         cnt = end - begin
-        if not (bool((cnt[:d] == 4).all()) and bool((cnt[d:] == 0).all())):
+        if not (bool((cnt[:d] == per).all()) and bool((cnt[d:] == 0).all())):
             return False
-        v64 = values[: 4 * d].to(torch.int64) & 0xFFFFFFFF
+        v64 = values[: per * d].to(torch.int64) & 0xFFFFFFFF
         seg = torch.repeat_interleave(torch.arange(self.q, device=v64.device), cnt)
         s1 = torch.zeros(d, dtype=torch.int64, device=v64.device).index_add_(0, seg, v64)
         s2 = torch.zeros(d, dtype=torch.int64, device=v64.device).index_add_(0, seg, v64 * v64)
@@ -326,7 +357,7 @@ class Workload:
             self.retrieve(s)
             torch.cuda.synchronize()
             return bool(self.out[self.n:].all())
-        if self.kind == "mv32":
+        if self.kind in ("mv32", "mb32"):
             self.retrieve(s)
             torch.cuda.synchronize()
             return (self.mv_ok(self.begin, self.end, self.out) and self.table.size() == self.n
@@ -376,6 +407,14 @@ def reference_gpu(wl, reps=5):
                               vp(re_.data_ptr()), vp(out.data_ptr()), ctypes.byref(num),
                               u64(min_cap), ctypes.c_int(reps), ctypes.byref(ti), ctypes.byref(tr),
                               ctypes.byref(cap))
+    elif wl.kind == "mb32":
+        rb, re_ = torch.empty_like(wl.begin), torch.empty_like(wl.end)
+        num = ctypes.c_uint64(0)
+        rc = lib.ref_mb32_run(vp(wl.keys.data_ptr()), vp(wl.values.data_ptr()), u64(wl.n),
+                              vp(wl.queries.data_ptr()), u64(wl.q), vp(rb.data_ptr()),
+                              vp(re_.data_ptr()), vp(out.data_ptr()), ctypes.byref(num),
+                              u64(wl.min_cap), ctypes.c_uint32(wl.bucket), ctypes.c_int(reps),
+                              ctypes.byref(ti), ctypes.byref(tr), ctypes.byref(cap))
     elif wl.kind == "bloom64":
         rc = lib.ref_bloom64_run(vp(wl.keys.data_ptr()), u64(wl.n), vp(wl.queries.data_ptr()),
                                  u64(wl.q), vp(out.data_ptr()), u64(16 * wl.n), u64(8),
@@ -386,7 +425,7 @@ def reference_gpu(wl, reps=5):
     if rc != 0:
         return {"error": "CUDA error %d" % rc}
     # the reference's answers on the same inputs must equal ours
-    same = wl.mv_ok(rb, re_, out) if wl.kind == "mv32" else wl.answers_ok(out)
+    same = wl.mv_ok(rb, re_, out) if wl.kind in ("mv32", "mb32") else wl.answers_ok(out)
     ins_g = wl.n / (ti.value * 1e-3) / 1e9
     ret_g = wl.q / (tr.value * 1e-3) / 1e9
     return {"insert_gops": round(ins_g, 4), "retrieve_gops": round(ret_g, 4),
@@ -406,6 +445,8 @@ WORKLOAD_NAMES = {
     "bloom64": "BloomFilter<u64,Murmur64,u64,CG8> 16 bits/key k=8: insert 2^{L} + query 2^{L1}",
     "mv32": "MultiValueHashTable<u32,u32> CG8 LF{LF}: insert 2^{L} pairs (4 values per key, "
             "one shuffled batch) + retrieve every key and as many absent keys",
+    "mb32": "MultiBucketHashTable<u32,u32> CG8 bucket {B}, key LF{LF}: insert 2^{L} values "
+            "(key i mod 2^{L3} + 1, 8 per key) + retrieve keys 1..2^{L} (two-phase, offsets)",
     "served": "4096 SingleValueHashTable<u32,u32> (caps log-uniform 2^10..2^22, LF 0.85), "
               "Poisson requests (batch 2^6..2^18, 30% insert, 80% hit): continuous batching vs plain launches",
 }
@@ -443,7 +484,7 @@ def run_ours(args):
     import warpcore_b200  # noqa: F401
     warpcore_b200.lib()
 
-    wl = Workload(args.workload, args.log2n, args.load, rank, device, world,
+    wl = Workload(args.workload, args.log2n, args.load, rank, device, world, bucket=args.bucket,
                   shard=args.shard or world > 1)
     stream = torch.cuda.Stream(device=device)
     torch.cuda.synchronize()
@@ -528,7 +569,8 @@ def run_ours(args):
             "dtype": "u64" if wl.kb == 8 else "u32",
             "data": "synthetic (seeded uniform unique keys, uniform values; inputs resident in HBM)",
             "config": {
-                "workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n, L1=args.log2n + 1, LF=args.load),
+                "workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n, L1=args.log2n + 1, L3=args.log2n - 3,
+                                                         LF=args.load, B=args.bucket),
                 "capacity": int(wl.table.capacity) if hasattr(wl.table, "capacity") else None,
                 "ops_per_step": ops_step,
                 "l2": "inputs larger than L2 (no flush)" if args.log2n >= 24 else "inputs may be L2-resident",
@@ -586,7 +628,7 @@ def run_e2e(wl, stream, args, world):
     d2h = ho.numel() * ho.element_size()
     keys0, vals0, q0 = wl.keys, wl.values, wl.queries
     steps = max(1, min(args.steps, 3))
-    piped = hasattr(wl.table, "insert_from_host") and not wl.sharded and wl.kind != "mv32"
+    piped = hasattr(wl.table, "insert_from_host") and not wl.sharded and wl.kind not in ("mv32", "mb32")
     if piped:
         # host buffers straight into the C ABI: chunks of 2^22 keys, copy-in
         # / kernel / copy-out overlapped; a miss gets the fill value the
@@ -716,7 +758,8 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "u64" if args.workload not in ("svht32", "counting32") else "u32",
         "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n, L1=args.log2n + 1, LF=args.load),
+        "config": {"workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n, L1=args.log2n + 1, L3=args.log2n - 3,
+                                                         LF=args.load, B=args.bucket),
                    "sample": "2^%d keys per step on the host" % args.cpu_log2n},
         "cpu_baseline": {"value": round(value, 5), "unit": "Gops/s", "cores": threads,
                          "kind": "port",
@@ -808,11 +851,13 @@ def main():
     ap.add_argument("--tables", type=int, default=4096)
     ap.add_argument("--requests", type=int, default=8192)
     ap.add_argument("--rates", default="100000,300000,1000000")
+    ap.add_argument("--bucket", type=int, default=2,
+                    help="values per slot of the mb32 workload (1, 2, 4 or 8)")
     args = ap.parse_args()
     if args.log2n is None:
         args.log2n = 24 if args.workload == "mv32" else 27
     if args.load is None:
-        args.load = 0.8 if args.workload == "mv32" else 0.9
+        args.load = 0.8 if args.workload in ("mv32", "mb32") else 0.9
     if args.warmup < 3:
         log("warm-up raised to 3 steps")
         args.warmup = 3

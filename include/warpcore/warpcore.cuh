@@ -8,5 +8,6 @@
 #include "counting_hash_table.cuh"
 #include "bloom_filter.cuh"
 #include "multi_value_hash_table.cuh"
+#include "multi_bucket_hash_table.cuh"
 
 #endif

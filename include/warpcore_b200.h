@@ -275,6 +275,73 @@ int wc_mvht_retrieve_all_keys(wc_table *t, void *keys_out, uint64_t *num_out, wc
 int wc_mvht_num_keys(wc_table *t, wc_stream_t stream, uint64_t *out);
 
 /* ------------------------------------------------------------------ */
+/* MultiBucketHashTable<Key, Value, EmptyKey, TombstoneKey, EmptyValue,  */
+/* ProbingScheme, AoSStore<Key, ArrayBucket<Value, B>>>                  */
+/* (multi_bucket_hash_table.cuh).  A slot holds a key and a bucket of    */
+/* B values (1 <= B <= cg_size); a key's values fill its last bucket     */
+/* before the key takes another slot.  The config's key fields, probing  */
+/* and cg_size are used as for the other tables; value_bytes (4 or 8) is */
+/* independent of key_bytes.  Keys and buckets are stored as two arrays. */
+/* ------------------------------------------------------------------ */
+
+typedef struct wc_mbht wc_mbht;
+
+typedef struct wc_mbht_info {
+    uint32_t key_bytes, value_bytes, bucket_size, cg_size;
+    uint32_t probing, hasher1, hasher2;
+    uint64_t capacity;        /* key slots, reference capacity rule */
+    uint64_t value_capacity;  /* capacity * bucket_size (:1088-1093) */
+    uint64_t num_buckets;     /* capacity / cg_size */
+    uint64_t seed, empty_key, tombstone_key, empty_value, max_values_per_key;
+    uint64_t bytes_total;     /* bytes of this layout: keys, buckets, one index */
+    void *keys;               /* device: capacity keys */
+    void *values;             /* device: capacity * bucket_size values */
+    uint32_t *status;         /* device Status word */
+    unsigned long long *num_keys, *num_occupied; /* device counters */
+    int is_initialized;
+} wc_mbht_info;
+
+/* MultiBucketHashTable(min_capacity, seed, max_values_per_key, no_init)
+ * (multi_bucket_hash_table.cuh:195-217); bucket_size is ArrayBucket's B and
+ * empty_value the EmptyValue parameter (default 0) */
+int wc_mbht_create(const wc_table_config *cfg, uint32_t bucket_size, uint64_t empty_value,
+                   uint64_t min_capacity, uint64_t seed, uint64_t max_values_per_key, int no_init,
+                   wc_mbht **out);
+int wc_mbht_destroy(wc_mbht *t);
+/* init (:253-271): keys empty, bucket values empty, counters and status zero */
+int wc_mbht_init(wc_mbht *t, wc_stream_t stream);
+/* insert (:343-542): a key holding max_values_per_key values reports
+ * duplicate_key + max_values_for_key_reached; an empty value reports
+ * invalid_value; a key that held values reports duplicate_key */
+int wc_mbht_insert(wc_mbht *t, const void *keys_in, const void *values_in, uint64_t num_in,
+                   wc_stream_t stream, uint64_t probing_length, void *status_out,
+                   int status_handler, uint32_t ignore);
+/* num_values (:1013-1039): per key into num_per_key_out (device, may be
+ * NULL), their sum into *num_out (host); synchronises `stream` */
+int wc_mbht_num_values(wc_mbht *t, const void *keys_in, uint64_t num_in, uint64_t *num_out,
+                       uint64_t *num_per_key_out, wc_stream_t stream, uint64_t probing_length,
+                       void *status_out, int status_handler, uint32_t ignore);
+/* retrieve (:574-680): every key's values at values_out[begin[i] .. end[i]),
+ * in slot order along the probe sequence (insertion order); *num_out gets
+ * the total.  values_out NULL is a dry run: end_offsets_out gets the
+ * per-key counts, every status is dry_run.  Synchronises `stream`. */
+int wc_mbht_retrieve(wc_mbht *t, const void *keys_in, uint64_t num_in,
+                     uint64_t *begin_offsets_out, uint64_t *end_offsets_out, void *values_out,
+                     uint64_t *num_out, wc_stream_t stream, uint64_t probing_length,
+                     void *status_out, int status_handler, uint32_t ignore);
+/* retrieve_all_keys (:742-777): each stored key once, order unspecified;
+ * keys_out NULL gives num_keys() and joins dry_run */
+int wc_mbht_retrieve_all_keys(wc_mbht *t, void *keys_out, uint64_t *num_out, wc_stream_t stream);
+/* num_keys (:891-902), num_occupied (:904-916), size = num_values() (:1060-1082) */
+int wc_mbht_num_keys(wc_mbht *t, wc_stream_t stream, uint64_t *out);
+int wc_mbht_num_occupied(wc_mbht *t, wc_stream_t stream, uint64_t *out);
+int wc_mbht_size(wc_mbht *t, wc_stream_t stream, uint64_t *out);
+/* peek_status / pop_status (:1165-1201) */
+int wc_mbht_peek_status(wc_mbht *t, wc_stream_t stream, uint32_t *out);
+int wc_mbht_pop_status(wc_mbht *t, wc_stream_t stream, uint32_t *out);
+int wc_mbht_get_info(const wc_mbht *t, wc_mbht_info *info);
+
+/* ------------------------------------------------------------------ */
 /* BloomFilter<Key, Hasher, Slot, CGSize>                               */
 /* ------------------------------------------------------------------ */
 

@@ -64,6 +64,20 @@ def _load():
         "wco_mv_retrieve": (_u64, [_vp, _vp, _u64, _vp, _vp, _vp, _u64, _vp]),
         "wco_mv_num_keys": (_u64, [_vp]),
         "wco_mv_unique_keys": (_u64, [_vp, _vp]),
+        "wco_mb_create": (_vp, [_i, _i, _u64, _u64, _u64, _u64, _i, _i, _i, _u64, _u64, _u64,
+                                _u64]),
+        "wco_mb_destroy": (None, [_vp]),
+        "wco_mb_capacity": (_u64, [_vp]),
+        "wco_mb_init": (None, [_vp, _u64]),
+        "wco_mb_insert": (None, [_vp, _vp, _vp, _u64, _u64, _vp]),
+        "wco_mb_num_values": (_u64, [_vp, _vp, _u64, _vp, _u64, _vp]),
+        "wco_mb_retrieve": (_u64, [_vp, _vp, _u64, _vp, _vp, _vp, _u64, _vp]),
+        "wco_mb_num_keys": (_u64, [_vp]),
+        "wco_mb_num_occupied": (_u64, [_vp]),
+        "wco_mb_size": (_u64, [_vp]),
+        "wco_mb_unique_keys": (_u64, [_vp, _vp]),
+        "wco_mb_peek_status": (ctypes.c_uint32, [_vp]),
+        "wco_mb_pop_status": (ctypes.c_uint32, [_vp]),
         "wco_table_capacity": (_u64, [_vp]),
         "wco_table_init": (None, [_vp, _u64]),
         "wco_insert": (None, [_vp, _vp, _vp, _u64, _u64, _vp]),
@@ -294,6 +308,89 @@ class MVTable(Table):
         k = np.empty(max(self.capacity, 1), dtype=_kdtype(self.key_bytes))
         n = lib().wco_mv_unique_keys(self.h, _ptr(k))
         return k[:n]
+
+
+class MBTable:
+    """Sequential reference-order MultiBucketHashTable (bucket <= cg)."""
+
+    def __init__(self, key_bytes, value_bytes, min_capacity, bucket=2, seed=DEFAULT_SEED, cg=8,
+                 scheme=PROBE_DOUBLE, h1=HASH_MURMUR, h2=HASH_MURMUR, empty_key=0,
+                 tombstone_key=None, empty_value=0, max_values_per_key=None):
+        if tombstone_key is None:
+            tombstone_key = (1 << (8 * key_bytes)) - 1
+        if max_values_per_key is None:
+            max_values_per_key = 2**64 - 1
+        self.key_bytes = key_bytes
+        self.value_bytes = value_bytes
+        self.bucket = bucket
+        self.h = lib().wco_mb_create(key_bytes, value_bytes, bucket, int(min_capacity), int(seed),
+                                     cg, scheme, h1, h2, int(empty_key), int(tombstone_key),
+                                     int(empty_value), int(max_values_per_key))
+        if not self.h:
+            raise ValueError("bucket must be 1 .. cg")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().wco_mb_destroy(self.h)
+            self.h = None
+
+    @property
+    def capacity(self):
+        return lib().wco_mb_capacity(self.h)
+
+    def init(self, seed=DEFAULT_SEED):
+        lib().wco_mb_init(self.h, int(seed))
+
+    def insert(self, keys, values, probing_length=DEFAULT_PROBING_LENGTH, want_status=False):
+        keys = np.ascontiguousarray(keys)
+        values = np.ascontiguousarray(values)
+        st = np.zeros(len(keys), dtype=np.uint32) if want_status else None
+        lib().wco_mb_insert(self.h, _ptr(keys), _ptr(values), len(keys), int(probing_length),
+                            _ptr(st))
+        return st
+
+    def num_values(self, keys, probing_length=DEFAULT_PROBING_LENGTH):
+        """(total, per-key counts, statuses)"""
+        keys = np.ascontiguousarray(keys)
+        c = np.zeros(len(keys), dtype=np.uint64)
+        st = np.zeros(len(keys), dtype=np.uint32)
+        total = lib().wco_mb_num_values(self.h, _ptr(keys), len(keys), _ptr(c),
+                                        int(probing_length), _ptr(st))
+        return total, c, st
+
+    def retrieve(self, keys, dry_run=False, probing_length=DEFAULT_PROBING_LENGTH):
+        """(begin offsets, end offsets, values, statuses); a dry run gives
+        per-key counts in place of end offsets and no values"""
+        keys = np.ascontiguousarray(keys)
+        n = len(keys)
+        b = np.zeros(n, dtype=np.uint64)
+        e = np.zeros(n, dtype=np.uint64)
+        st = np.zeros(n, dtype=np.uint32)
+        total = 0 if dry_run else self.num_values(keys, probing_length)[0]
+        vals = None if dry_run else np.zeros(max(int(total), 1), dtype=_kdtype(self.value_bytes))
+        lib().wco_mb_retrieve(self.h, _ptr(keys), n, _ptr(b), _ptr(e), _ptr(vals),
+                              int(probing_length), _ptr(st))
+        return b, e, (vals[:int(total)] if vals is not None else None), st
+
+    def num_keys(self):
+        return lib().wco_mb_num_keys(self.h)
+
+    def num_occupied(self):
+        return lib().wco_mb_num_occupied(self.h)
+
+    def size(self):
+        return lib().wco_mb_size(self.h)
+
+    def unique_keys(self):
+        k = np.empty(max(self.capacity, 1), dtype=_kdtype(self.key_bytes))
+        n = lib().wco_mb_unique_keys(self.h, _ptr(k))
+        return k[:n]
+
+    def peek_status(self):
+        return lib().wco_mb_peek_status(self.h)
+
+    def pop_status(self):
+        return lib().wco_mb_pop_status(self.h)
 
 
 class Bloom:

@@ -17,6 +17,7 @@
 #include <warpcore/counting_hash_table.cuh>
 #include <warpcore/bloom_filter.cuh>
 #include <warpcore/multi_value_hash_table.cuh>
+#include <warpcore/multi_bucket_hash_table.cuh>
 #include <algorithm>
 
 #include <cstdio>
@@ -540,6 +541,98 @@ static void mv_case(const char *tag, uint64_t n, uint64_t min_cap, uint64_t ksee
     cudaFree(dq); cudaFree(db); cudaFree(de); cudaFree(dvals); cudaFree(dku); cudaFree(dst);
 }
 
+/* MultiBucketHashTable<K, V> with AoSStore<K, ArrayBucket<V, B>> (the
+ * layout of the reference's multi_bucket benchmark): five insert rounds
+ * over shrinking prefixes of the keys (each key's values arrive one per
+ * round, so their order is fixed), round 0 with an invalid key and an
+ * invalid (empty) value; then counts, a dry run, the two-phase retrieve,
+ * num_keys / num_occupied / size and the unique keys. */
+template <class K, class V, uint32_t B>
+static void mb_case(const char *tag, uint64_t n, uint64_t min_cap, uint64_t kseed,
+                    uint64_t max_values)
+{
+    using Table = wc::MultiBucketHashTable<
+        K, V, wc::defaults::empty_key<K>(), wc::defaults::tombstone_key<K>(),
+        wc::defaults::empty_key<V>(), wc::defaults::probing_scheme_t<K, 8>,
+        wc::storage::key_value::AoSStore<K, wc::ArrayBucket<V, B>>>;
+    using SH = wc::status_handlers::ReturnStatus;
+    using index_t = wc::index_t;
+    const std::string p = tag;
+    std::vector<K> all = unique_keys<K>(n + n / 4, kseed);
+    std::vector<K> keys(all.begin(), all.begin() + n);
+    Table t(min_cap, wc::defaults::seed<K>(), max_values);
+    wc::Status *dst;
+    CK(cudaMalloc(&dst, sizeof(wc::Status) * (n + n / 4)));
+    std::vector<uint32_t> st_rounds;
+    std::vector<K> keys_rounds;
+    std::vector<V> vals_rounds;
+    for (uint64_t r = 0; r < 5; r++) {
+        const uint64_t m = n - r * (n / 5);
+        std::vector<K> kr(keys.begin(), keys.begin() + m);
+        std::vector<V> vr = uniform<V>(m, kseed + 10 + r);
+        for (auto &v : vr)
+            if (v == V(0)) v = V(1);
+        if (r == 0) {
+            kr[11] = wc::defaults::tombstone_key<K>();
+            vr[7] = V(0);
+        }
+        K *dk = to_dev(kr);
+        V *dv = to_dev(vr);
+        t.template insert<SH>(dk, dv, m, 0, wc::defaults::probing_length(), dst);
+        auto st = to_host((uint32_t *)dst, m);
+        st_rounds.insert(st_rounds.end(), st.begin(), st.end());
+        keys_rounds.insert(keys_rounds.end(), kr.begin(), kr.end());
+        vals_rounds.insert(vals_rounds.end(), vr.begin(), vr.end());
+        cudaFree(dk);
+        cudaFree(dv);
+    }
+    const uint64_t num_keys = t.num_keys();
+    const uint64_t num_occupied = t.num_occupied();
+    const uint64_t size = t.size();
+    const uint32_t status1 = t.pop_status().base();
+    const uint64_t nq = all.size();
+    K *dq = to_dev(all);
+    index_t *db, *de;
+    CK(cudaMalloc(&db, sizeof(index_t) * nq));
+    CK(cudaMalloc(&de, sizeof(index_t) * nq));
+    index_t num_dry = 0;
+    t.template retrieve<SH>(dq, nq, db, de, nullptr, num_dry, 0, wc::defaults::probing_length(), dst);
+    auto counts_dry = to_host((uint64_t *)de, nq);
+    auto st_dry = to_host((uint32_t *)dst, nq);
+    const uint32_t status2 = t.pop_status().base();
+    V *dvals;
+    CK(cudaMalloc(&dvals, sizeof(V) * (num_dry ? num_dry : 1)));
+    index_t num_out = 0;
+    t.template retrieve<SH>(dq, nq, db, de, dvals, num_out, 0, wc::defaults::probing_length(), dst);
+    auto begin = to_host((uint64_t *)db, nq);
+    auto end = to_host((uint64_t *)de, nq);
+    auto values = to_host(dvals, num_out);
+    auto st_ret = to_host((uint32_t *)dst, nq);
+    const uint32_t status3 = t.pop_status().base();
+    K *dku;
+    CK(cudaMalloc(&dku, sizeof(K) * (num_occupied ? num_occupied : 1)));
+    index_t num_unique = 0;
+    t.retrieve_all_keys(dku, num_unique, 0);
+    auto uk = to_host(dku, num_unique);
+    std::sort(uk.begin(), uk.end());
+
+    dump(p + "_meta", std::vector<uint64_t>{n, min_cap, kseed, t.capacity(), B, max_values,
+                                            num_keys, num_occupied, size, status1, num_dry,
+                                            status2, num_out, status3, num_unique,
+                                            t.value_capacity()});
+    dump(p + "_insert_keys", keys_rounds);
+    dump(p + "_insert_values", vals_rounds);
+    dump(p + "_insert_status", st_rounds);
+    dump(p + "_dry_counts", counts_dry);
+    dump(p + "_dry_status", st_dry);
+    dump(p + "_begin", begin);
+    dump(p + "_end", end);
+    dump(p + "_values", values);
+    dump(p + "_retrieve_status", st_ret);
+    dump(p + "_unique_keys_sorted", uk);
+    cudaFree(dq); cudaFree(db); cudaFree(de); cudaFree(dvals); cudaFree(dku); cudaFree(dst);
+}
+
 static void run_gpu()
 {
     namespace ps = wc::probing_schemes;
@@ -608,6 +701,13 @@ static void run_gpu()
     bloom_case<uint32_t, uint64_t, 2>("bloom_u32_s64_cg2", 5000, 3, 400, 64);
     mv_case<uint32_t, uint32_t>("mv_u32u32_max3", 4000, 16000, 71, 3);
     mv_case<uint64_t, uint64_t>("mv_u64u64", 4000, 16000, 72, ~uint64_t(0));
+    mb_case<uint32_t, uint32_t, 1>("mb_u32u32_b1", 4000, 16000, 81, ~uint64_t(0));
+    mb_case<uint32_t, uint32_t, 2>("mb_u32u32_b2", 4000, 16000, 82, ~uint64_t(0));
+    mb_case<uint32_t, uint32_t, 2>("mb_u32u32_b2_max3", 4000, 16000, 83, 3);
+    mb_case<uint32_t, uint32_t, 4>("mb_u32u32_b4_max6", 4000, 8000, 84, 6);
+    mb_case<uint32_t, uint32_t, 8>("mb_u32u32_b8", 4000, 8000, 85, ~uint64_t(0));
+    mb_case<uint32_t, uint64_t, 2>("mb_u32u64_b2", 4000, 16000, 86, ~uint64_t(0));
+    mb_case<uint64_t, uint64_t, 4>("mb_u64u64_b4_max2", 4000, 16000, 87, 2);
 }
 
 int main(int argc, char **argv)

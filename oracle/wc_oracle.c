@@ -746,6 +746,319 @@ uint64_t wco_mv_unique_keys(const wco_table *t, void *keys_out)
 }
 
 /* ------------------------------------------------------------------------ */
+/* MultiBucketHashTable (multi_bucket_hash_table.cuh): every slot holds a key */
+/* and a bucket of `bucket` values; a key's values fill its last bucket       */
+/* before a new slot is claimed.  Buckets larger than the group size are not  */
+/* restated (the reference's loop over them reads value[rank] for every      */
+/* chunk, :270-274), so bucket <= cg.                                         */
+/* ------------------------------------------------------------------------ */
+
+struct wco_mb {
+    int key_bytes, value_bytes, scheme, h1, h2;
+    uint64_t capacity, cg, bucket, seed, empty, tomb, empty_value, max_values;
+    uint64_t *keys;
+    uint64_t *vals; /* capacity * bucket */
+    uint64_t num_keys, num_occupied;
+    uint32_t status;
+};
+
+wco_mb *wco_mb_create(int key_bytes, int value_bytes, uint64_t bucket, uint64_t min_capacity,
+                      uint64_t seed, uint64_t cg, int scheme, int h1, int h2, uint64_t empty_key,
+                      uint64_t tombstone_key, uint64_t empty_value, uint64_t max_values_per_key)
+{
+    if (bucket == 0 || bucket > cg) return NULL;
+    wco_mb *t = (wco_mb *)calloc(1, sizeof(wco_mb));
+    t->key_bytes = key_bytes;
+    t->value_bytes = value_bytes;
+    t->scheme = scheme; t->h1 = h1; t->h2 = h2;
+    t->cg = cg;
+    t->bucket = bucket;
+    t->capacity = wco_valid_capacity(min_capacity, cg);
+    t->empty = empty_key & kmask(key_bytes);
+    t->tomb = tombstone_key & kmask(key_bytes);
+    t->empty_value = empty_value & kmask(value_bytes);
+    t->max_values = max_values_per_key;
+    t->keys = (uint64_t *)malloc((t->capacity ? t->capacity : 1) * 8);
+    t->vals = (uint64_t *)malloc((t->capacity ? t->capacity : 1) * bucket * 8);
+    wco_mb_init(t, seed);
+    return t;
+}
+
+void wco_mb_destroy(wco_mb *t)
+{
+    if (!t) return;
+    free(t->keys);
+    free(t->vals);
+    free(t);
+}
+
+uint64_t wco_mb_capacity(const wco_mb *t) { return t->capacity; }
+
+/* init (:253-271): keys := empty, every bucket value := empty value,
+ * counters zero */
+void wco_mb_init(wco_mb *t, uint64_t seed)
+{
+    t->seed = seed & kmask(t->key_bytes);
+    for (uint64_t i = 0; i < t->capacity; i++) t->keys[i] = t->empty;
+    for (uint64_t i = 0; i < t->capacity * t->bucket; i++) t->vals[i] = t->empty_value;
+    t->num_keys = 0;
+    t->num_occupied = 0;
+    t->status = 0;
+}
+
+static int mb_valid_key(const wco_mb *t, uint64_t k) { return k != t->empty && k != t->tomb; }
+
+/* insert_into_bucket (:262-330), one thread after another: lane 0 and the
+ * lanes past the bucket count as full ("first bucket value always written
+ * after key insert"), the others hold value[lane]; the count so far grows
+ * by the full ones; the first empty lane takes the value. */
+static int mb_insert_into_bucket(wco_mb *t, uint64_t slot, uint64_t value, uint64_t num_values,
+                                 uint32_t *st)
+{
+    const uint64_t B = t->bucket;
+    uint64_t *const b = t->vals + slot * B;
+    uint64_t empties = 0;
+    for (uint64_t r = 1; r < B; r++)
+        if (b[r] == t->empty_value) empties |= 1ull << r;
+    num_values += B - (uint64_t)__builtin_popcountll(empties);
+    if (num_values >= t->max_values) {
+        *st = WCO_ST_DUPLICATE_KEY | WCO_ST_MAX_VALUES_REACHED;
+        t->status |= *st;
+        return 1;
+    }
+    if (empties) {
+        b[__builtin_ctzll(empties)] = value;
+        *st = num_values > 0 ? WCO_ST_DUPLICATE_KEY : WCO_ST_NONE;
+        return 1;
+    }
+    return 0;
+}
+
+/* insert (:343-517): along the probe sequence, note the last slot that
+ * holds the key and count bucket_size per such slot; once the count
+ * reaches max_values_per_key, only the last bucket can take the value.  In
+ * the first window with an empty slot, fill the last bucket if it has room,
+ * else claim the empty slot with the value in its bucket's first place. */
+static uint32_t mb_insert_one(wco_mb *t, uint64_t key, uint64_t value, uint64_t probing_length)
+{
+    const uint64_t B = t->bucket;
+    if (!mb_valid_key(t, key)) {
+        t->status |= WCO_ST_INVALID_KEY;
+        return WCO_ST_INVALID_KEY;
+    }
+    if (value == t->empty_value) {
+        t->status |= WCO_ST_INVALID_VALUE;
+        return WCO_ST_INVALID_VALUE;
+    }
+    probe_t p;
+    probe_begin(&p, t->scheme, t->h1, t->h2, t->key_bytes, t->cg, t->capacity, key, t->seed,
+                probing_length);
+    uint64_t num = 0, guard = t->capacity / t->cg + 1;
+    int64_t last = -1;
+    uint32_t st;
+    do {
+        int64_t hit_last = -1;
+        uint64_t hits = 0, empties = 0;
+        for (uint64_t r = 0; r < t->cg; r++) {
+            const uint64_t k = t->keys[p.pos[r]];
+            if (k == key) { hits++; hit_last = (int64_t)r; }
+            if (k == t->empty) empties |= 1ull << r;
+        }
+        if (hits) last = (int64_t)p.pos[hit_last];
+        num += B * hits;
+        if (num >= t->max_values) {
+            if (B == 1) {
+                st = WCO_ST_DUPLICATE_KEY | WCO_ST_MAX_VALUES_REACHED;
+                t->status |= st;
+                return st;
+            }
+            st = WCO_ST_UNKNOWN_ERROR;
+            mb_insert_into_bucket(t, (uint64_t)last, value, num - B, &st);
+            return st;
+        }
+        if (empties) {
+            if (B > 1 && last >= 0 && mb_insert_into_bucket(t, (uint64_t)last, value, num - B, &st))
+                return st;
+            const uint64_t slot = p.pos[__builtin_ctzll(empties)];
+            t->keys[slot] = key;
+            t->vals[slot * B] = value;
+            t->num_occupied++;
+            if (num == 0) t->num_keys++;
+            return num > 0 ? WCO_ST_DUPLICATE_KEY : WCO_ST_NONE;
+        }
+    } while (--guard && probe_next(&p));
+    if (B > 1 && last >= 0 && mb_insert_into_bucket(t, (uint64_t)last, value, num - B, &st))
+        return st;
+    st = WCO_ST_PROBING_LENGTH_EXCEEDED | (num > 0 ? WCO_ST_DUPLICATE_KEY : 0);
+    t->status |= st;
+    return st;
+}
+
+void wco_mb_insert(wco_mb *t, const void *keys, const void *values, uint64_t n,
+                   uint64_t probing_length, uint32_t *status_out)
+{
+    for (uint64_t i = 0; i < n; i++) {
+        const uint32_t st = mb_insert_one(t, load_elem(keys, t->key_bytes, i),
+                                          load_elem(values, t->value_bytes, i), probing_length);
+        if (status_out) status_out[i] = st;
+    }
+}
+
+/* for_each (:786-846): windows of the probe sequence (probing length capped
+ * at the capacity); a hit slot's non-empty values get the indices
+ * num + bucket * (hits before it in the window) + place; the count grows by
+ * bucket per hit less the empty places of the window's last hit; stop at a
+ * window with an empty key or once the count reaches max_values_per_key. */
+static uint32_t mb_for_each(wco_mb *t, uint64_t key, uint64_t probing_length, void *out,
+                            uint64_t room, uint64_t *num_out)
+{
+    const uint64_t B = t->bucket;
+    if (!mb_valid_key(t, key)) {
+        *num_out = 0;
+        t->status |= WCO_ST_INVALID_KEY;
+        return WCO_ST_INVALID_KEY;
+    }
+    probe_t p;
+    const uint64_t pl = probing_length < t->capacity ? probing_length : t->capacity;
+    probe_begin(&p, t->scheme, t->h1, t->h2, t->key_bytes, t->cg, t->capacity, key, t->seed, pl);
+    uint64_t num = 0, guard = t->capacity / t->cg + 1;
+    do {
+        uint64_t h = 0, last_empty = 0;
+        int any_empty = 0;
+        for (uint64_t r = 0; r < t->cg; r++) {
+            const uint64_t k = t->keys[p.pos[r]];
+            if (k == key) {
+                const uint64_t j = num + B * h;
+                uint64_t e = 0;
+                for (uint64_t b = 0; b < B; b++) {
+                    const uint64_t v = t->vals[p.pos[r] * B + b];
+                    if (v != t->empty_value) {
+                        if (out && j + b < room) store_elem(out, t->value_bytes, j + b, v);
+                    } else {
+                        e++;
+                    }
+                }
+                last_empty = e;
+                h++;
+            }
+            any_empty |= k == t->empty;
+        }
+        num += B * h - last_empty;
+        if (any_empty || num >= t->max_values) {
+            *num_out = num;
+            if (num == 0) {
+                t->status |= WCO_ST_KEY_NOT_FOUND;
+                return WCO_ST_KEY_NOT_FOUND;
+            }
+            return WCO_ST_NONE;
+        }
+    } while (--guard && probe_next(&p));
+    *num_out = num;
+    t->status |= WCO_ST_PROBING_LENGTH_EXCEEDED;
+    return WCO_ST_PROBING_LENGTH_EXCEEDED;
+}
+
+/* bulk num_values (:1013-1039, gpu_engine.cuh:466-504) */
+uint64_t wco_mb_num_values(wco_mb *t, const void *keys, uint64_t n, uint64_t *counts_out,
+                           uint64_t probing_length, uint32_t *status_out)
+{
+    uint64_t total = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t num = 0;
+        const uint32_t st = mb_for_each(t, load_elem(keys, t->key_bytes, i), probing_length,
+                                        NULL, 0, &num);
+        if (counts_out) counts_out[i] = num;
+        total += num;
+        if (status_out) status_out[i] = st;
+    }
+    return total;
+}
+
+/* bulk retrieve (:574-680): counts, inclusive scan into end offsets, begin
+ * offsets one behind, then each key's values at its begin offset; with
+ * values_out NULL a dry run (per-key counts in end_out, status dry_run).
+ * The reference writes values without a bound; here index >= the key's
+ * count is not written (the counts come from the same walk). */
+uint64_t wco_mb_retrieve(wco_mb *t, const void *keys, uint64_t n, uint64_t *begin_out,
+                         uint64_t *end_out, void *values_out, uint64_t probing_length,
+                         uint32_t *status_out)
+{
+    const uint64_t total = wco_mb_num_values(t, keys, n, end_out, probing_length, NULL);
+    if (!values_out) {
+        for (uint64_t i = 0; i < n && status_out; i++) status_out[i] = WCO_ST_DRY_RUN;
+        t->status |= WCO_ST_DRY_RUN;
+        return total;
+    }
+    uint64_t s = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        begin_out[i] = s;
+        s += end_out[i];
+        end_out[i] = s;
+    }
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t num = 0;
+        char *dst = (char *)values_out + begin_out[i] * (uint64_t)t->value_bytes;
+        const uint32_t st = mb_for_each(t, load_elem(keys, t->key_bytes, i), probing_length, dst,
+                                        end_out[i] - begin_out[i], &num);
+        if (status_out) status_out[i] = st;
+    }
+    return total;
+}
+
+uint64_t wco_mb_num_keys(const wco_mb *t) { return t->num_keys; }
+uint64_t wco_mb_num_occupied(const wco_mb *t) { return t->num_occupied; }
+
+/* size (:1060-1082, gpu_engine.cuh:419-464): non-empty values of slots
+ * with a valid key */
+uint64_t wco_mb_size(const wco_mb *t)
+{
+    uint64_t n = 0;
+    for (uint64_t i = 0; i < t->capacity; i++) {
+        if (!mb_valid_key(t, t->keys[i])) continue;
+        for (uint64_t b = 0; b < t->bucket; b++) n += t->vals[i * t->bucket + b] != t->empty_value;
+    }
+    return n;
+}
+
+/* retrieve_all_keys (:742-777, gpu_engine.cuh:51-93): a slot's key is
+ * output when that slot is the lowest lane of the first window holding
+ * the key; slot order */
+uint64_t wco_mb_unique_keys(const wco_mb *t, void *keys_out)
+{
+    uint64_t n = 0;
+    for (uint64_t gid = 0; gid < t->capacity; gid++) {
+        const uint64_t key = t->keys[gid];
+        if (!mb_valid_key(t, key)) continue;
+        probe_t p;
+        probe_begin(&p, t->scheme, t->h1, t->h2, t->key_bytes, t->cg, t->capacity, key, t->seed,
+                    t->capacity);
+        uint64_t guard = t->capacity / t->cg + 1;
+        do {
+            int64_t leader = -1;
+            for (uint64_t r = 0; r < t->cg && leader < 0; r++)
+                if (t->keys[p.pos[r]] == key) leader = (int64_t)p.pos[r];
+            if (leader >= 0) {
+                if ((uint64_t)leader == gid) {
+                    if (keys_out) store_elem(keys_out, t->key_bytes, n, key);
+                    n++;
+                }
+                break;
+            }
+        } while (--guard && probe_next(&p));
+    }
+    return n;
+}
+
+uint32_t wco_mb_peek_status(const wco_mb *t) { return t->status; }
+
+uint32_t wco_mb_pop_status(wco_mb *t)
+{
+    const uint32_t s = t->status;
+    t->status = 0;
+    return s;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Bloom filter (bloom_filter.cuh:78-93 sizes, :168-192 insert,
  * :216-237 retrieve, :342-408 fpr)                                          */
 /* ------------------------------------------------------------------------ */

@@ -127,6 +127,28 @@ uint64_t wco_mv_retrieve(wco_table *t, const void *keys, uint64_t n, uint64_t *b
 uint64_t wco_mv_num_keys(const wco_table *t);
 uint64_t wco_mv_unique_keys(const wco_table *t, void *keys_out);
 
+/* MultiBucketHashTable (multi_bucket_hash_table.cuh); bucket <= cg */
+typedef struct wco_mb wco_mb;
+wco_mb *wco_mb_create(int key_bytes, int value_bytes, uint64_t bucket, uint64_t min_capacity,
+                      uint64_t seed, uint64_t cg, int scheme, int h1, int h2, uint64_t empty_key,
+                      uint64_t tombstone_key, uint64_t empty_value, uint64_t max_values_per_key);
+void wco_mb_destroy(wco_mb *t);
+uint64_t wco_mb_capacity(const wco_mb *t);
+void wco_mb_init(wco_mb *t, uint64_t seed);
+void wco_mb_insert(wco_mb *t, const void *keys, const void *values, uint64_t n,
+                   uint64_t probing_length, uint32_t *status_out);
+uint64_t wco_mb_num_values(wco_mb *t, const void *keys, uint64_t n, uint64_t *counts_out,
+                           uint64_t probing_length, uint32_t *status_out);
+uint64_t wco_mb_retrieve(wco_mb *t, const void *keys, uint64_t n, uint64_t *begin_out,
+                         uint64_t *end_out, void *values_out, uint64_t probing_length,
+                         uint32_t *status_out);
+uint64_t wco_mb_num_keys(const wco_mb *t);
+uint64_t wco_mb_num_occupied(const wco_mb *t);
+uint64_t wco_mb_size(const wco_mb *t);
+uint64_t wco_mb_unique_keys(const wco_mb *t, void *keys_out);
+uint32_t wco_mb_peek_status(const wco_mb *t);
+uint32_t wco_mb_pop_status(wco_mb *t);
+
 typedef struct wco_bloom wco_bloom;
 wco_bloom *wco_bloom_create(int key_bytes, int slot_bytes, uint64_t cg,
                             int hasher, uint64_t num_bits, uint64_t k,

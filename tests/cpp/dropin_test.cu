@@ -403,6 +403,98 @@ static void test_multi_value()
     cudaFree(dvv); cudaFree(dnums); cudaFree(duk);
 }
 
+/* MultiBucketHashTable<u32, u64> with buckets of 2 (the reference example's
+ * types): host and device inserts, max_values_per_key, offsets and values
+ * in insertion order, device reads, for_each_value / for_each_bucket with
+ * device lambdas, unique keys */
+static void test_multi_bucket()
+{
+    using T = wc::MultiBucketHashTable<uint32_t, uint64_t>;
+    static_assert(T::bucket_size() == 2, "default bucket of two values");
+    const uint64_t n = 3000;
+    T t(4 * n, wc::defaults::seed<uint32_t>(), 5);
+    auto keys = distinct_keys<uint32_t>(n + 100, 93);
+    std::vector<uint32_t> k(keys.begin(), keys.begin() + n);
+    uint32_t *dk = dcopy(k);
+    auto value = [](uint64_t r, uint64_t i) { return r * 1000000 + i + 1; };
+    for (uint64_t r = 0; r < 2; r++) {
+        std::vector<uint64_t> v(n);
+        for (uint64_t i = 0; i < n; i++) v[i] = value(r, i);
+        uint64_t *dv = dcopy(v);
+        t.insert(dk, dv, n);
+        cudaFree(dv);
+    }
+    uint32_t *dst;
+    cudaMalloc(&dst, sizeof(uint32_t) * n);
+    for (uint64_t r = 2; r < 6; r++) {
+        std::vector<uint64_t> v(n);
+        for (uint64_t i = 0; i < n; i++) v[i] = value(r, i);
+        uint64_t *dv = dcopy(v);
+        device_mv_insert<<<blocks_for(n, T::cg_size()), 256>>>(t, dk, dv, n, dst);
+        auto st = hcopy(dst, n);
+        const uint32_t want = r < 5 ? wc::Status::duplicate_key().base()
+                                    : (wc::Status::duplicate_key() + wc::Status::max_values_for_key_reached()).base();
+        CHECK(std::all_of(st.begin(), st.end(), [&](uint32_t s) { return s == want; }));
+        cudaFree(dv);
+    }
+    CHECK(t.size() == 5 * n);
+    CHECK(t.num_keys() == n);
+    CHECK(t.num_occupied() == 3 * n);
+    CHECK(t.value_capacity() == 2 * t.capacity());
+    std::vector<uint32_t> q(keys.begin(), keys.end());
+    uint32_t *dq = dcopy(q);
+    uint64_t *db, *de, *dvals;
+    cudaMalloc(&db, sizeof(uint64_t) * q.size());
+    cudaMalloc(&de, sizeof(uint64_t) * q.size());
+    T::index_type num_out = 0;
+    t.retrieve(dq, q.size(), db, de, nullptr, num_out);
+    CHECK(num_out == 5 * n);
+    cudaMalloc(&dvals, sizeof(uint64_t) * num_out);
+    t.retrieve(dq, q.size(), db, de, dvals, num_out);
+    auto b = hcopy(db, q.size()), e = hcopy(de, q.size()), vals = hcopy(dvals, num_out);
+    bool ok = true;
+    for (uint64_t i = 0; i < n; i++) {
+        ok &= b[i] == 5 * i && e[i] == 5 * i + 5;
+        for (uint64_t r = 0; r < 5; r++) ok &= vals[5 * i + r] == value(r, i);
+    }
+    for (uint64_t i = n; i < q.size(); i++) ok &= e[i] == b[i];
+    CHECK(ok);
+    uint64_t *dvv, *dnums;
+    cudaMalloc(&dvv, sizeof(uint64_t) * 5 * n);
+    cudaMalloc(&dnums, sizeof(uint64_t) * n);
+    device_mv_read<<<blocks_for(n, T::cg_size()), 256>>>(t, dk, n, dvv, 5, dnums);
+    auto nums = hcopy(dnums, n);
+    auto vv = hcopy(dvv, 5 * n);
+    ok = true;
+    for (uint64_t i = 0; i < n; i++) {
+        ok &= nums[i] == 5;
+        for (uint64_t r = 0; r < 5; r++) ok &= vv[5 * i + r] == value(r, i);
+    }
+    CHECK(ok);
+    /* for_each_value: every stored value once; for_each_bucket: every slot */
+    unsigned long long *dsum;
+    cudaMalloc(&dsum, 2 * sizeof(unsigned long long));
+    cudaMemset(dsum, 0, 2 * sizeof(unsigned long long));
+    t.for_each_value([=] __device__(uint32_t, uint64_t v) { atomicAdd(dsum, (unsigned long long)v); });
+    t.for_each_bucket([=] __device__(uint32_t, const T::bucket_type &) { atomicAdd(dsum + 1, 1ull); });
+    auto sums = hcopy(dsum, 2);
+    unsigned long long want_sum = 0;
+    for (uint64_t i = 0; i < n; i++)
+        for (uint64_t r = 0; r < 5; r++) want_sum += value(r, i);
+    CHECK(sums[0] == want_sum);
+    CHECK(sums[1] == 3 * n);
+    T::index_type nk = 0;
+    uint32_t *duk;
+    cudaMalloc(&duk, sizeof(uint32_t) * n);
+    t.retrieve_all_keys(duk, nk);
+    auto uk = hcopy(duk, nk);
+    std::sort(uk.begin(), uk.end());
+    std::sort(k.begin(), k.end());
+    CHECK(nk == n && uk == k);
+    cudaFree(dk); cudaFree(dst); cudaFree(dq); cudaFree(db); cudaFree(de); cudaFree(dvals);
+    cudaFree(dvv); cudaFree(dnums); cudaFree(dsum); cudaFree(duk);
+}
+
 int main()
 {
     test_svht_u32();
@@ -411,6 +503,7 @@ int main()
     test_counting();
     test_bloom();
     test_multi_value();
+    test_multi_bucket();
     const cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         std::fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(e));

@@ -148,3 +148,55 @@ def mv_scenario(F, tag, kb, make_table):
     uk = np.sort(t.unique_keys())
     assert uk.size == num_unique
     assert np.array_equal(uk, F[tag + "_unique_keys_sorted"])
+
+
+MB_CASES = [("mb_u32u32_b1", 4, 4), ("mb_u32u32_b2", 4, 4), ("mb_u32u32_b2_max3", 4, 4),
+            ("mb_u32u32_b4_max6", 4, 4), ("mb_u32u32_b8", 4, 4), ("mb_u32u64_b2", 4, 8),
+            ("mb_u64u64_b4_max2", 8, 8)]
+
+
+def mb_scenario(F, tag, kb, vb, make_table):
+    """make_table(min_cap, bucket, max_values_per_key) -> object with insert /
+    num_keys / num_occupied / size / pop_status / retrieve(keys, dry_run) /
+    unique_keys like oracle.MBTable"""
+    (n, min_cap, kseed, cap, bucket, max_values, num_keys, num_occupied, size, s1, num_dry, s2,
+     num_out, s3, num_unique, value_capacity) = F[tag + "_meta"].tolist()
+    allk = o.gen_unique_keys(kb, n + n // 4, kseed)
+    keys = allk[:n]
+    t = make_table(min_cap, bucket, max_values)
+    assert t.capacity == cap
+    assert t.capacity * bucket == value_capacity
+    st_all, keys_all, vals_all = [], [], []
+    for r in range(5):
+        m = n - r * (n // 5)
+        k = keys[:m].copy()
+        v = o.gen_uniform(vb, m, kseed + 10 + r)
+        v[v == 0] = 1
+        if r == 0:
+            k[11] = (1 << (8 * kb)) - 1      # the tombstone key: invalid_key
+            v[7] = 0                         # the empty value: invalid_value
+        st_all.append(t.insert(k, v, want_status=True))
+        keys_all.append(k)
+        vals_all.append(v)
+    assert np.array_equal(np.concatenate(keys_all), F[tag + "_insert_keys"])
+    assert np.array_equal(np.concatenate(vals_all), F[tag + "_insert_values"])
+    assert np.array_equal(np.concatenate(st_all), F[tag + "_insert_status"])
+    assert t.num_keys() == num_keys
+    assert t.num_occupied() == num_occupied
+    assert t.size() == size
+    assert t.pop_status() == s1
+    _, counts, _, st = t.retrieve(allk, dry_run=True)
+    assert int(counts.sum()) == num_dry
+    assert np.array_equal(counts, F[tag + "_dry_counts"])
+    assert np.array_equal(st, F[tag + "_dry_status"])
+    assert t.pop_status() == s2
+    b, e, v, st = t.retrieve(allk)
+    assert np.array_equal(b, F[tag + "_begin"])
+    assert np.array_equal(e, F[tag + "_end"])
+    assert v.size == num_out
+    assert np.array_equal(v, F[tag + "_values"])
+    assert np.array_equal(st, F[tag + "_retrieve_status"])
+    assert t.pop_status() == s3
+    uk = np.sort(t.unique_keys())
+    assert uk.size == num_unique
+    assert np.array_equal(uk, F[tag + "_unique_keys_sorted"])

@@ -62,3 +62,9 @@ def test_bloom(tag):
 @pytest.mark.parametrize("tag,kb", gs.MV_CASES)
 def test_multi_value(tag, kb):
     gs.mv_scenario(F, tag, kb, lambda cap, mx: o.MVTable(kb, kb, cap, max_values_per_key=mx))
+
+
+@pytest.mark.parametrize("tag,kb,vb", gs.MB_CASES)
+def test_multi_bucket(tag, kb, vb):
+    gs.mb_scenario(F, tag, kb, vb, lambda cap, bucket, mx: o.MBTable(
+        kb, vb, cap, bucket=bucket, max_values_per_key=mx))

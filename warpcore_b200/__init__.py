@@ -20,6 +20,7 @@ from ._status import Status  # noqa: F401
 
 __all__ = [
     "Status", "SingleValueHashTable", "HashSet", "CountingHashTable", "MultiValueHashTable",
+    "MultiBucketHashTable",
     "BloomFilter", "lib", "valid_capacity", "WarpcoreError", "set_l2_persistence",
     "HostPipe", "set_fingerprint_policy", "set_fingerprint_ops", "launch_count", "FINGERPRINTS_AUTO", "FINGERPRINTS_ALWAYS",
     "FINGERPRINTS_NEVER",
@@ -56,6 +57,33 @@ class TableConfig(ctypes.Structure):
         ("hasher1", ctypes.c_uint32),
         ("hasher2", ctypes.c_uint32),
         ("cg_size", ctypes.c_uint32),
+    ]
+
+
+class MbInfo(ctypes.Structure):
+    _fields_ = [
+        ("key_bytes", ctypes.c_uint32),
+        ("value_bytes", ctypes.c_uint32),
+        ("bucket_size", ctypes.c_uint32),
+        ("cg_size", ctypes.c_uint32),
+        ("probing", ctypes.c_uint32),
+        ("hasher1", ctypes.c_uint32),
+        ("hasher2", ctypes.c_uint32),
+        ("capacity", ctypes.c_uint64),
+        ("value_capacity", ctypes.c_uint64),
+        ("num_buckets", ctypes.c_uint64),
+        ("seed", ctypes.c_uint64),
+        ("empty_key", ctypes.c_uint64),
+        ("tombstone_key", ctypes.c_uint64),
+        ("empty_value", ctypes.c_uint64),
+        ("max_values_per_key", ctypes.c_uint64),
+        ("bytes_total", ctypes.c_uint64),
+        ("keys", ctypes.c_void_p),
+        ("values", ctypes.c_void_p),
+        ("status", ctypes.c_void_p),
+        ("num_keys", ctypes.c_void_p),
+        ("num_occupied", ctypes.c_void_p),
+        ("is_initialized", ctypes.c_int),
     ]
 
 
@@ -223,6 +251,20 @@ SIGNATURES = {
                               _i, _u32]),
     "wc_mvht_retrieve_all_keys": (_i, [_vp, _vp, ctypes.POINTER(_u64), _vp]),
     "wc_mvht_num_keys": (_i, [_vp, _vp, ctypes.POINTER(_u64)]),
+    "wc_mbht_create": (_i, [ctypes.POINTER(TableConfig), _u32, _u64, _u64, _u64, _u64, _i, _pp]),
+    "wc_mbht_destroy": (_i, [_vp]),
+    "wc_mbht_init": (_i, [_vp, _vp]),
+    "wc_mbht_insert": (_i, [_vp, _vp, _vp, _u64, _vp, _u64, _vp, _i, _u32]),
+    "wc_mbht_num_values": (_i, [_vp, _vp, _u64, ctypes.POINTER(_u64), _vp, _vp, _u64, _vp, _i, _u32]),
+    "wc_mbht_retrieve": (_i, [_vp, _vp, _u64, _vp, _vp, _vp, ctypes.POINTER(_u64), _vp, _u64, _vp,
+                              _i, _u32]),
+    "wc_mbht_retrieve_all_keys": (_i, [_vp, _vp, ctypes.POINTER(_u64), _vp]),
+    "wc_mbht_num_keys": (_i, [_vp, _vp, ctypes.POINTER(_u64)]),
+    "wc_mbht_num_occupied": (_i, [_vp, _vp, ctypes.POINTER(_u64)]),
+    "wc_mbht_size": (_i, [_vp, _vp, ctypes.POINTER(_u64)]),
+    "wc_mbht_peek_status": (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32)]),
+    "wc_mbht_pop_status": (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32)]),
+    "wc_mbht_get_info": (_i, [_vp, ctypes.POINTER(MbInfo)]),
     "wc_table_l2_window": (_i, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(ctypes.c_float)]),
     "wc_tune_set": (_i, [_u32, _i, _u32, _u32, _u32, _u32]),
     "wc_tune_reset": (_i, []),
@@ -594,6 +636,154 @@ class MultiValueHashTable(_Table):
     def num_keys(self, stream=None):
         out = _u64(0)
         _check(lib().wc_mvht_num_keys(self._h, _stream(stream), ctypes.byref(out)))
+        return int(out.value)
+
+
+class MultiBucketHashTable:
+    """warpcore::MultiBucketHashTable (multi_bucket_hash_table.cuh:88-110):
+    a slot holds a key and a bucket of `bucket_size` values (ArrayBucket's
+    B, 1 .. cg_size); a key's values fill its last bucket before it takes
+    another slot.  The empty value (default 0) marks a free place and cannot
+    be stored.  retrieve returns each key's values in insertion order with
+    begin/end offsets."""
+
+    def __init__(self, min_capacity, seed=DEFAULT_SEED, max_values_per_key=2**64 - 1,
+                 no_init=False, key_bytes=4, value_bytes=None, bucket_size=2, empty_value=0,
+                 empty_key=None, tombstone_key=None, probing=None, hasher1=None, hasher2=None,
+                 cg_size=None):
+        value_bytes = key_bytes if value_bytes is None else value_bytes
+        cfg = _table_config(lib().wc_svht_default_config, key_bytes, key_bytes, empty_key,
+                            tombstone_key, probing, hasher1, hasher2, cg_size)
+        cfg.value_bytes = value_bytes
+        h = ctypes.c_void_p()
+        _check(lib().wc_mbht_create(ctypes.byref(cfg), int(bucket_size), int(empty_value),
+                                    int(min_capacity), int(seed), int(max_values_per_key),
+                                    int(bool(no_init)), ctypes.byref(h)))
+        self._h = h
+        self._cfg = cfg
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.wc_mbht_destroy(h)
+            self._h = None
+
+    def info(self):
+        inf = MbInfo()
+        _check(lib().wc_mbht_get_info(self._h, ctypes.byref(inf)))
+        return inf
+
+    @property
+    def key_bytes(self):
+        return self._cfg.key_bytes
+
+    @property
+    def value_bytes(self):
+        return self._cfg.value_bytes
+
+    @property
+    def capacity(self):
+        return self.info().capacity
+
+    @property
+    def value_capacity(self):
+        return self.info().value_capacity
+
+    def bucket_size(self):
+        return self.info().bucket_size
+
+    def bytes_total(self):
+        return self.info().bytes_total
+
+    def init(self, stream=None):
+        _check(lib().wc_mbht_init(self._h, _stream(stream)))
+
+    def insert(self, keys_in, values_in, num_in=None, stream=None,
+               probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+               status_handler=None, ignore=0):
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        _check_width(values_in, self.value_bytes, "values_in")
+        h = _handler(status_out, status_handler)
+        _check(lib().wc_mbht_insert(self._h, _ptr(keys_in), _ptr(values_in),
+                                    _numel(keys_in, num_in), _stream(stream),
+                                    int(probing_length), _ptr(status_out), h, int(ignore)))
+
+    def num_values(self, keys_in=None, num_per_key_out=None, num_in=None, stream=None,
+                   probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+                   status_handler=None, ignore=0):
+        """values per key (uint64 tensor, optional) and their sum; with no
+        keys, the number of values in the table (size)"""
+        if keys_in is None:
+            return self.size(stream)
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        h = _handler(status_out, status_handler)
+        out = _u64(0)
+        _check(lib().wc_mbht_num_values(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                        ctypes.byref(out), _ptr(num_per_key_out),
+                                        _stream(stream), int(probing_length), _ptr(status_out),
+                                        h, int(ignore)))
+        return int(out.value)
+
+    def retrieve(self, keys_in, begin_offsets_out, end_offsets_out, values_out=None,
+                 num_in=None, stream=None, probing_length=DEFAULT_PROBING_LENGTH,
+                 status_out=None, status_handler=None, ignore=0):
+        """values_out None: dry run (end_offsets_out gets the counts);
+        returns the total number of values"""
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        if values_out is not None:
+            _check_width(values_out, self.value_bytes, "values_out")
+        h = _handler(status_out, status_handler)
+        out = _u64(0)
+        _check(lib().wc_mbht_retrieve(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                      _ptr(begin_offsets_out), _ptr(end_offsets_out),
+                                      _ptr(values_out), ctypes.byref(out), _stream(stream),
+                                      int(probing_length), _ptr(status_out), h, int(ignore)))
+        return int(out.value)
+
+    def retrieve_all_keys(self, keys_out=None, stream=None):
+        """each stored key once; keys_out None: only the count"""
+        out = _u64(0)
+        _check(lib().wc_mbht_retrieve_all_keys(self._h, _ptr(keys_out), ctypes.byref(out),
+                                               _stream(stream)))
+        return int(out.value)
+
+    def _counter(self, fn, stream):
+        out = _u64(0)
+        _check(fn(self._h, _stream(stream), ctypes.byref(out)))
+        return int(out.value)
+
+    def num_keys(self, stream=None):
+        return self._counter(lib().wc_mbht_num_keys, stream)
+
+    def num_occupied(self, stream=None):
+        return self._counter(lib().wc_mbht_num_occupied, stream)
+
+    def size(self, stream=None):
+        return self._counter(lib().wc_mbht_size, stream)
+
+    def key_load_factor(self, stream=None):
+        return self.num_occupied(stream) / self.capacity
+
+    def value_load_factor(self, stream=None):
+        return self.size(stream) / self.value_capacity
+
+    def storage_density(self, stream=None):
+        payload = self.num_keys(stream) * self.key_bytes + self.size(stream) * self.value_bytes
+        return payload / self.bytes_total()
+
+    def relative_storage_density(self, stream=None):
+        values = self.size(stream) * self.value_bytes
+        payload = self.num_keys(stream) * self.key_bytes + values
+        return payload / (self.num_occupied(stream) * self.key_bytes + values)
+
+    def peek_status(self, stream=None):
+        out = ctypes.c_uint32(0)
+        _check(lib().wc_mbht_peek_status(self._h, _stream(stream), ctypes.byref(out)))
+        return int(out.value)
+
+    def pop_status(self, stream=None):
+        out = ctypes.c_uint32(0)
+        _check(lib().wc_mbht_pop_status(self._h, _stream(stream), ctypes.byref(out)))
         return int(out.value)
 
 

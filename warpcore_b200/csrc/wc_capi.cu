@@ -325,6 +325,25 @@ constexpr int kBlock = 256;
 
 void warpcore::b200::set_last_error(const char *msg) { g_last_error = msg; }
 
+int warpcore::b200::host_fail(int code, const char *msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+int warpcore::b200::host_cuda_fail(cudaError_t e, const char *what) { return cuda_fail(e, what); }
+
+unsigned warpcore::b200::host_grid(const void *kernel, int block, uint64_t items,
+                                   uint64_t per_block)
+{
+    return grid_for(kernel, block, items, per_block);
+}
+
+uint64_t warpcore::b200::host_valid_capacity(uint64_t min_capacity, uint64_t cg)
+{
+    return valid_capacity(min_capacity, cg);
+}
+
 static std::atomic<unsigned long long> g_launches{0};
 void warpcore::b200::note_launches(uint32_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
@@ -970,7 +989,10 @@ int mv_scan(wc_table *t, uint64_t *begin, uint64_t *end, uint64_t n, cudaStream_
     WC_CUDA(cudaLaunchKernel(k.tile_sums, dim3(unsigned(ntiles)), dim3(kScanThreads), a1, 0, s));
     void *a2[] = {&ts, &nt};
     WC_CUDA(cudaLaunchKernel(k.tile_offsets, dim3(1), dim3(kScanThreads), a2, 0, s));
-    void *a3[] = {&e, &b, &nn, &ts};
+    /* end == begin + 1: the scan writes end only, begin[0] is zero */
+    int write_begin = e == b + 1 ? 0 : 1;
+    if (!write_begin) WC_CUDA(cudaMemsetAsync(b, 0, sizeof(unsigned long long), s));
+    void *a3[] = {&e, &b, &nn, &ts, &write_begin};
     WC_CUDA(cudaLaunchKernel(k.apply, dim3(unsigned(ntiles)), dim3(kScanThreads), a3, 0, s));
     note_launches(3);
     return WC_OK;

@@ -52,6 +52,14 @@ MvScanKernels mv_scan_kernels();
 /* message returned by wc_last_error() on the calling thread */
 void set_last_error(const char *msg);
 
+/* host helpers of wc_capi.cu for the other translation units: set the
+ * error message and return `code`; map a CUDA error to a WC_ERR code;
+ * launch geometry (at most one wave of resident blocks); the capacity rule */
+int host_fail(int code, const char *msg);
+int host_cuda_fail(cudaError_t e, const char *what);
+unsigned host_grid(const void *kernel, int block, uint64_t items, uint64_t per_block);
+uint64_t host_valid_capacity(uint64_t min_capacity, uint64_t cg);
+
 /* kernels this library launched (wc_launch_count) */
 void note_launches(uint32_t n);
 

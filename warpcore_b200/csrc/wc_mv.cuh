@@ -237,12 +237,16 @@ __global__ void __launch_bounds__(kScanThreads) scan_tile_offsets_kernel(unsigne
     }
 }
 
-/* counts (in end) -> end = inclusive prefix sums, begin = end - count */
+/* counts (in end) -> end = inclusive prefix sums, begin = end - count.
+ * write_begin 0 leaves begin alone: the caller passed end == begin + 1 (the
+ * reference's offsets_out, offsets_out + 1 idiom), where begin[i + 1] is
+ * end[i] already and writing it would race with the block reading it. */
 template <int kUnused = 0>
 __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(unsigned long long *end,
                                                                   unsigned long long *begin,
                                                                   uint64_t n,
-                                                                  const unsigned long long *tile_offsets)
+                                                                  const unsigned long long *tile_offsets,
+                                                                  int write_begin)
 {
     const uint64_t t0 = uint64_t(blockIdx.x) * kScanTile;
     unsigned long long c[kScanItems];
@@ -260,7 +264,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(unsigned long 
     for (int j = 0; j < kScanItems; ++j) {
         const uint64_t i = t0 + uint64_t(threadIdx.x) * kScanItems + j;
         if (i < n) {
-            begin[i] = run;
+            if (write_begin) begin[i] = run;
             run += c[j];
             end[i] = run;
         }
