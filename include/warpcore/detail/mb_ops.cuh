@@ -40,8 +40,22 @@ struct MbView {
     unsigned long long *num_occupied;/* claimed slots */
 };
 
+/* kW / kB: the window width (cg_size) and bucket size when known at
+ * compile time, 0 to take them from the view.  The bulk kernels are built
+ * for CG 8 with buckets of 1, 2, 4 and 8 and for any shape at run time. */
+template <int kW>
+__device__ __forceinline__ uint32_t mb_w(const MbView &m)
+{
+    return kW ? uint32_t(kW) : m.t.cg_size;
+}
+template <int kB>
+__device__ __forceinline__ uint32_t mb_b(const MbView &m)
+{
+    return kB ? uint32_t(kB) : m.bucket;
+}
+
 /* one window of keys: bit s of hits / empties = key s equals `key` / is empty */
-template <class K>
+template <class K, int kW>
 __device__ __forceinline__ void mb_window(const K *kw, uint32_t W, K key, K empty, uint32_t &hits,
                                           uint32_t &empties)
 {
@@ -49,7 +63,8 @@ __device__ __forceinline__ void mb_window(const K *kw, uint32_t W, K key, K empt
     empties = 0;
     const uint32_t bytes = W * uint32_t(sizeof(K));
     if (bytes >= 16) {
-        for (uint32_t v = 0; v < bytes / 16; ++v) {
+#pragma unroll
+        for (uint32_t v = 0; v < (kW ? kW * sizeof(K) / 16 : bytes / 16); ++v) {
             const uint4 q = __ldcg(reinterpret_cast<const uint4 *>(kw) + v);
             if constexpr (sizeof(K) == 4) {
                 const uint32_t s = v * 4;
@@ -73,6 +88,41 @@ __device__ __forceinline__ void mb_window(const K *kw, uint32_t W, K key, K empt
     }
 }
 
+/* bit r of the result: place r of a bucket holds the empty value.  With a
+ * compile-time bucket of 8, 16 or 32 bytes (or more, in 16-byte pieces)
+ * the places come in vector loads. */
+template <class V, int kB>
+__device__ __forceinline__ uint32_t mb_bucket_empties(const V *b, uint32_t B, V ev, V *vals_out)
+{
+    uint32_t e = 0;
+    if constexpr (kB > 0 && (kB * sizeof(V)) % 8 == 0 && ((kB * sizeof(V)) & (kB * sizeof(V) - 1)) == 0) {
+        constexpr int bytes = kB * int(sizeof(V));
+        V v[kB];
+        if constexpr (bytes == 8) {
+            const uint2 q = __ldcg(reinterpret_cast<const uint2 *>(b));
+            memcpy(v, &q, 8);
+        } else {
+#pragma unroll
+            for (int c = 0; c < bytes / 16; ++c) {
+                const uint4 q = __ldcg(reinterpret_cast<const uint4 *>(b) + c);
+                memcpy(reinterpret_cast<char *>(v) + 16 * c, &q, 16);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < kB; ++r) {
+            if (vals_out) vals_out[r] = v[r];
+            e |= uint32_t(v[r] == ev) << r;
+        }
+    } else {
+        for (uint32_t r = 0; r < B; ++r) {
+            const V x = __ldcg(b + r);
+            if (vals_out) vals_out[r] = x;
+            e |= uint32_t(x == ev) << r;
+        }
+    }
+    return e;
+}
+
 template <class V>
 __device__ __forceinline__ V mb_cas(V *p, V expect, V desired)
 {
@@ -88,16 +138,15 @@ __device__ __forceinline__ V mb_cas(V *p, V expect, V desired)
  * written right after the slot's claim); the count grows by the full
  * places; the value goes to the first free place that a compare-and-swap
  * wins.  Returns true when the insert is decided (stored, or capped). */
-template <class K, class V>
+template <class K, class V, int kB>
 __device__ bool mb_into_bucket(const MbView &m, uint64_t slot, V value, uint64_t num_values,
                                uint32_t &st)
 {
-    V *const b = reinterpret_cast<V *>(m.vals) + slot * m.bucket;
+    const uint32_t B = mb_b<kB>(m);
+    V *const b = reinterpret_cast<V *>(m.vals) + slot * B;
     const V ev = V(m.empty_value);
-    uint32_t empties = 0;
-    for (uint32_t r = 1; r < m.bucket; ++r)
-        if (__ldcg(b + r) == ev) empties |= 1u << r;
-    num_values += m.bucket - uint32_t(__popc(empties));
+    uint32_t empties = mb_bucket_empties<V, kB>(b, B, ev, nullptr) & ~1u;
+    num_values += B - uint32_t(__popc(empties));
     if (num_values >= m.max_values) {
         st = kStDuplicateKey | kStMaxValuesReached;
         return true;
@@ -121,12 +170,12 @@ __device__ bool mb_into_bucket(const MbView &m, uint64_t slot, V value, uint64_t
  * `fresh` tell whether a slot was claimed and whether it was the key's
  * first.  The caller joins every status but none and the plain
  * duplicate_key of a stored value into the table status. */
-template <class K, class V>
+template <class K, class V, int kW = 0, int kB = 0>
 __device__ uint32_t mb_insert_one(const MbView &m, K key, V value, uint64_t max_windows,
                                   bool &claimed, bool &fresh)
 {
     const TableView &t = m.t;
-    const uint32_t W = t.cg_size, B = m.bucket;
+    const uint32_t W = mb_w<kW>(m), B = mb_b<kB>(m);
     const K empty = K(t.empty_key), tomb = K(t.tombstone_key);
     K *const keys = reinterpret_cast<K *>(t.slots);
     claimed = false;
@@ -138,16 +187,16 @@ __device__ uint32_t mb_insert_one(const MbView &m, K key, V value, uint64_t max_
     uint32_t st = kStUnknownError;
     for (uint64_t w = 0; w < max_windows; ++w) {
         uint32_t hits, emp;
-        mb_window<K>(keys + b * W, W, key, empty, hits, emp);
+        mb_window<K, kW>(keys + b * W, W, key, empty, hits, emp);
         if (hits) last = b * W + uint64_t(31 - __clz(hits));
         num += uint64_t(B) * uint64_t(__popc(hits));
         if (num >= m.max_values) {
             if (B == 1) return kStDuplicateKey | kStMaxValuesReached;
-            mb_into_bucket<K, V>(m, last, value, num - B, st);
+            mb_into_bucket<K, V, kB>(m, last, value, num - B, st);
             return st;
         }
         while (emp) {
-            if (B > 1 && last != ~0ull && mb_into_bucket<K, V>(m, last, value, num - B, st))
+            if (B > 1 && last != ~0ull && mb_into_bucket<K, V, kB>(m, last, value, num - B, st))
                 return st;
             const int s = __ffs(emp) - 1;
             const uint64_t slot = b * W + uint64_t(s);
@@ -169,19 +218,21 @@ __device__ uint32_t mb_insert_one(const MbView &m, K key, V value, uint64_t max_
         if (w == 0) step = probe_step<K>(t, key);
         b = probe_next(t, b, step);
     }
-    if (B > 1 && last != ~0ull && mb_into_bucket<K, V>(m, last, value, num - B, st)) return st;
+    if (B > 1 && last != ~0ull && mb_into_bucket<K, V, kB>(m, last, value, num - B, st)) return st;
     return kStProbingLengthExceeded | (num > 0 ? kStDuplicateKey : kStNone);
 }
 
-/* for_each over one key's values (:786-846): f(value, index); returns the
- * status (none, key_not_found, probing_length_exceeded, invalid_key) and
- * the count in num */
-template <class K, class V, class F>
+/* for_each over one key's values (:786-846): f(value, index) when kValues;
+ * returns the status (none, key_not_found, probing_length_exceeded,
+ * invalid_key) and the count in num.  The count takes bucket values per
+ * hit slot less the empty places of each window's last hit slot, so a
+ * count-only walk reads that one bucket per window. */
+template <class K, class V, int kW = 0, int kB = 0, bool kValues = true, class F>
 __device__ uint32_t mb_for_each_one(const MbView &m, K key, uint64_t max_windows, uint64_t &num,
                                     F f)
 {
     const TableView &t = m.t;
-    const uint32_t W = t.cg_size, B = m.bucket;
+    const uint32_t W = mb_w<kW>(m), B = mb_b<kB>(m);
     const K empty = K(t.empty_key), tomb = K(t.tombstone_key);
     const K *const keys = reinterpret_cast<const K *>(t.slots);
     const V *const vals = reinterpret_cast<const V *>(m.vals);
@@ -191,21 +242,24 @@ __device__ uint32_t mb_for_each_one(const MbView &m, K key, uint64_t max_windows
     uint64_t b = probe_begin<K>(t, key), step = 0;
     for (uint64_t w = 0; w < max_windows; ++w) {
         uint32_t hits, emp;
-        mb_window<K>(keys + b * W, W, key, empty, hits, emp);
-        uint64_t h = 0, last_empty = 0;
-        for (uint32_t x = hits; x; x &= x - 1u) {
-            const uint64_t slot = b * W + uint64_t(__ffs(x) - 1);
-            const uint64_t j = num + uint64_t(B) * h;
-            uint64_t e = 0;
-            for (uint32_t r = 0; r < B; ++r) {
-                const V v = __ldcg(vals + slot * B + r);
-                if (v != ev) f(v, j + r);
-                else ++e;
+        mb_window<K, kW>(keys + b * W, W, key, empty, hits, emp);
+        if (hits) {
+            const int last = 31 - __clz(hits);
+            if constexpr (kValues) {
+                uint64_t j = num;
+                for (uint32_t x = hits; x; x &= x - 1u) {
+                    const uint64_t slot = b * W + uint64_t(__ffs(x) - 1);
+                    V v[kB ? kB : 32];
+                    const uint32_t e = mb_bucket_empties<V, kB>(vals + slot * B, B, ev, v);
+                    for (uint32_t r = 0; r < (kB ? uint32_t(kB) : B); ++r)
+                        if (!((e >> r) & 1u)) f(v[r], j + r);
+                    j += B;
+                }
             }
-            last_empty = e;
-            ++h;
+            const uint32_t le = __popc(mb_bucket_empties<V, kB>(
+                vals + (b * W + uint64_t(last)) * B, B, ev, nullptr));
+            num += uint64_t(B) * uint64_t(__popc(hits)) - le;
         }
-        num += uint64_t(B) * h - last_empty;
         if (emp || num >= m.max_values) return num ? kStNone : kStKeyNotFound;
         if (w == 0) step = probe_step<K>(t, key);
         b = probe_next(t, b, step);

@@ -59,7 +59,7 @@ __global__ void mb_for_each_bucket_kernel(Func f, b200::MbView m, std::uint64_t 
     f(k, b);
 }
 
-template <class Func, class K, class V>
+template <class Func, class K, class V, int kW, int kB>
 __global__ void mb_for_each_keys_kernel(Func f, b200::MbView m, const K *keys, std::uint64_t n,
                                         std::uint64_t max_windows, void *status_out, int handler,
                                         std::uint32_t bool_mask)
@@ -68,7 +68,7 @@ __global__ void mb_for_each_keys_kernel(Func f, b200::MbView m, const K *keys, s
     if (i >= n) return;
     const K key = keys[i];
     std::uint64_t num = 0;
-    const std::uint32_t st = b200::mb_for_each_one<K, V>(
+    const std::uint32_t st = b200::mb_for_each_one<K, V, kW, kB>(
         m, key, max_windows, num, [&](V v, std::uint64_t j) { f(key, v, j); });
     if (st) b200::join_status(m.t.status, st);
     if (status_out && handler == b200::kHandlerStatus)
@@ -168,7 +168,7 @@ class MultiBucketHashTable {
         std::uint32_t st = 0;
         if (group.thread_rank() == 0) {
             bool claimed = false, fresh = false;
-            st = b200::mb_insert_one<K, V>(
+            st = b200::mb_insert_one<K, V, int(cg_size()), int(bucket_size())>(
                 view_, K(key_in), V(value_in),
                 b200::max_windows(probing_length, cg_size(), view_.t.num_buckets), claimed, fresh);
             if (claimed) atomicAdd(view_.num_occupied, 1ull);
@@ -202,7 +202,7 @@ class MultiBucketHashTable {
         std::uint64_t num = 0;
         if (group.thread_rank() == 0) {
             const std::uint64_t pl = probing_length < capacity_ ? probing_length : capacity_;
-            st = b200::mb_for_each_one<K, V>(
+            st = b200::mb_for_each_one<K, V, int(cg_size()), int(bucket_size())>(
                 view_, K(key_in), b200::max_windows(pl, cg_size(), view_.t.num_buckets), num,
                 [&](V v, std::uint64_t j) { f(key_in, value_type(v), j); });
             if (st) b200::join_status(view_.t.status, st);
@@ -320,7 +320,8 @@ class MultiBucketHashTable {
         if (!is_initialized_ || num_in == 0) return;
         const std::uint64_t pl = probing_length < capacity_ ? probing_length : capacity_;
         const unsigned grid = unsigned((num_in + 255) / 256);
-        detail::mb_for_each_keys_kernel<Func, K, V><<<grid, 256, smem_bytes, stream>>>(
+        detail::mb_for_each_keys_kernel<Func, K, V, int(cg_size()), int(bucket_size())>
+            <<<grid, 256, smem_bytes, stream>>>(
             f, view_, reinterpret_cast<const K *>(keys_in), num_in,
             b200::max_windows(pl, cg_size(), view_.t.num_buckets), (void *)status_out,
             StatusHandler::kId, (~std::uint32_t(StatusHandler::kIgnore)) ^ 0xFFFu);

@@ -86,7 +86,7 @@ __device__ __forceinline__ void mb_flush(const MbView &m, uint32_t join, unsigne
     }
 }
 
-template <class K, class V>
+template <class K, class V, int kW, int kB>
 __global__ void __launch_bounds__(256, 4) mb_insert_kernel(const MbArgs a)
 {
     uint32_t join = 0;
@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(256, 4) mb_insert_kernel(const MbArgs a)
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.n; i += stride) {
         bool c = false, f = false;
-        const uint32_t st = mb_insert_one<K, V>(a.m, reinterpret_cast<const K *>(a.keys)[i],
+        const uint32_t st = mb_insert_one<K, V, kW, kB>(a.m, reinterpret_cast<const K *>(a.keys)[i],
                                                 reinterpret_cast<const V *>(a.values)[i],
                                                 a.max_windows, c, f);
         /* every status but a stored value's none / duplicate_key is joined */
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(256, 4) mb_insert_kernel(const MbArgs a)
 }
 
 /* num_values (kValues false) or retrieve of each key's values */
-template <class K, class V, bool kValues>
+template <class K, class V, int kW, int kB, bool kValues>
 __global__ void __launch_bounds__(256, 4) mb_find_kernel(const MbArgs a)
 {
     uint32_t join = 0;
@@ -122,12 +122,12 @@ __global__ void __launch_bounds__(256, 4) mb_find_kernel(const MbArgs a)
              * than the counting pass saw means the table changed in between */
             V *const out = reinterpret_cast<V *>(a.values_out) + a.begin[i];
             const uint64_t room = a.end[i] - a.begin[i];
-            st = mb_for_each_one<K, V>(a.m, key, a.max_windows, num, [&](V v, uint64_t j) {
+            st = mb_for_each_one<K, V, kW, kB, true>(a.m, key, a.max_windows, num, [&](V v, uint64_t j) {
                 if (j < room) out[j] = v;
             });
             if (st != kStInvalidKey && num != room) st |= kStInvalidPhaseOverlap;
         } else {
-            st = mb_for_each_one<K, V>(a.m, key, a.max_windows, num, [](V, uint64_t) {});
+            st = mb_for_each_one<K, V, kW, kB, false>(a.m, key, a.max_windows, num, [](V, uint64_t) {});
         }
         join |= st;
         if (a.counts_out) a.counts_out[i] = num;
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(256) mb_unique_keys_kernel(const MbView m, uin
                 uint64_t b = probe_begin<K>(t, key), step = 0;
                 for (uint64_t w = 0; w < t.num_buckets; ++w) {
                     uint32_t hits, emp;
-                    mb_window<K>(keys + b * t.cg_size, t.cg_size, key, empty, hits, emp);
+                    mb_window<K, 0>(keys + b * t.cg_size, t.cg_size, key, empty, hits, emp);
                     if (hits) {
                         emit = b * t.cg_size + uint64_t(__ffs(hits) - 1) == gid;
                         break;
@@ -209,23 +209,41 @@ struct MbKernels {
     const void *insert, *count, *values, *unique, *size;
 };
 
-template <class K, class V>
+template <class K, class V, int kW, int kB>
 MbKernels mb_kernels_of()
 {
-    return {reinterpret_cast<const void *>(mb_insert_kernel<K, V>),
-            reinterpret_cast<const void *>(mb_find_kernel<K, V, false>),
-            reinterpret_cast<const void *>(mb_find_kernel<K, V, true>),
+    return {reinterpret_cast<const void *>(mb_insert_kernel<K, V, kW, kB>),
+            reinterpret_cast<const void *>(mb_find_kernel<K, V, kW, kB, false>),
+            reinterpret_cast<const void *>(mb_find_kernel<K, V, kW, kB, true>),
             reinterpret_cast<const void *>(mb_unique_keys_kernel<K>),
             reinterpret_cast<const void *>(mb_size_kernel<K, V>)};
+}
+
+/* CG 8 (the reference's default) with buckets of 1, 2, 4 or 8 runs kernels
+ * built for that shape; every other shape runs the run-time ones */
+template <class K, class V>
+MbKernels mb_kernels_kv(uint32_t cg, uint32_t bucket)
+{
+    if (cg == 8) {
+        switch (bucket) {
+        case 1: return mb_kernels_of<K, V, 8, 1>();
+        case 2: return mb_kernels_of<K, V, 8, 2>();
+        case 4: return mb_kernels_of<K, V, 8, 4>();
+        case 8: return mb_kernels_of<K, V, 8, 8>();
+        default: break;
+        }
+    }
+    return mb_kernels_of<K, V, 0, 0>();
 }
 
 MbKernels mb_kernels(const wc_mbht *t)
 {
     using U32 = unsigned int;
     using U64 = unsigned long long;
+    const uint32_t cg = t->cfg.cg_size, b = t->bucket;
     if (t->cfg.key_bytes == 4)
-        return t->cfg.value_bytes == 4 ? mb_kernels_of<U32, U32>() : mb_kernels_of<U32, U64>();
-    return t->cfg.value_bytes == 4 ? mb_kernels_of<U64, U32>() : mb_kernels_of<U64, U64>();
+        return t->cfg.value_bytes == 4 ? mb_kernels_kv<U32, U32>(cg, b) : mb_kernels_kv<U32, U64>(cg, b);
+    return t->cfg.value_bytes == 4 ? mb_kernels_kv<U64, U32>(cg, b) : mb_kernels_kv<U64, U64>(cg, b);
 }
 
 MbView view_of(const wc_mbht *t)
