@@ -17,6 +17,7 @@
 #include <warpcore/bloom_filter.cuh>
 #include <warpcore/multi_value_hash_table.cuh>
 #include <warpcore/multi_bucket_hash_table.cuh>
+#include <warpcore/bucket_list_hash_table.cuh>
 
 #include <cfloat>
 #include <cstdint>
@@ -249,6 +250,41 @@ int ref_mb32_run(const uint32_t *keys, const uint32_t *vals, uint64_t n, const u
     case 8: return ref_mb32<8>(keys, vals, n, q, nq, begin, end, values_out, num_out, min_cap, reps, ms_insert, ms_retrieve, capacity);
     default: return -1;
     }
+}
+
+/* BucketListHashTable<u32, u32> over BucketListStore<u32, 29, 18, 15> (the
+ * reference's bucket_list benchmark types), grow factor 1.1, first bucket
+ * 1: bulk insert (n a multiple of 128, the insert kernel's groups per
+ * block), then the two-phase bulk retrieve */
+int ref_bl32_run(const uint32_t *keys, const uint32_t *vals, uint64_t n, const uint32_t *q,
+                 uint64_t nq, uint64_t *begin, uint64_t *end, uint32_t *values_out,
+                 uint64_t *num_out, uint64_t key_cap, uint64_t value_cap, int reps,
+                 float *ms_insert, float *ms_retrieve, uint64_t *capacity)
+{
+    if (n % 128) return -1;
+    using Store = wc::storage::multi_value::BucketListStore<uint32_t, 29, 18, 15>;
+    using Table = wc::BucketListHashTable<uint32_t, uint32_t, wc::defaults::empty_key<uint32_t>(),
+                                          wc::defaults::tombstone_key<uint32_t>(), Store,
+                                          wc::defaults::probing_scheme_t<uint32_t, 8>>;
+    Table t(key_cap, value_cap, wc::defaults::seed<uint32_t>(), 1.1f, 1);
+    *capacity = t.key_capacity();
+    Timer tm;
+    float bi = FLT_MAX, br = FLT_MAX;
+    for (int r = 0; r < reps; ++r) {
+        t.init();
+        cudaDeviceSynchronize();
+        tm.start();
+        t.insert(keys, vals, n);
+        bi = fminf(bi, tm.stop());
+        wc::index_t num = 0;
+        tm.start();
+        t.retrieve(q, nq, (wc::index_t *)begin, (wc::index_t *)end, values_out, num);
+        br = fminf(br, tm.stop());
+        *num_out = num;
+    }
+    *ms_insert = bi;
+    *ms_retrieve = br;
+    return int(cudaDeviceSynchronize());
 }
 
 } // extern "C"

@@ -252,6 +252,34 @@ class Workload:
             # the window sector in the count and value passes, one value out
             # per query on average
             self.bytes_insert, self.bytes_retrieve = 4 + 4 + 32 + 32, 4 + 16 + 32 + 32 + 4
+        elif kind == "bl32":
+            # the reference's bucket_list benchmark: 2^L values, key of input
+            # i = i mod 2^(L-3) + 1 (8 values per key); key table for load 0.9
+            # of the distinct keys, value pool for load 0.5 of the values;
+            # store bits 29 / 18 / 15, grow factor 1.1, first bucket 1
+            distinct = n >> 3
+            self.distinct = distinct
+            self.per_key = 8
+            idx = torch.arange(n, device=device) % distinct
+            self.keys = (idx + 1).to(torch.int32).contiguous()
+            self.values = uniform_values(n, 4, gen, device)
+            self.queries = (torch.arange(n, device=device) + 1).to(torch.int32).contiguous()
+            self.q = n
+            v64 = self.values.to(torch.int64) & 0xFFFFFFFF
+            self.exp_sum = torch.zeros(distinct, dtype=torch.int64, device=device).index_add_(0, idx, v64)
+            self.exp_sq = torch.zeros(distinct, dtype=torch.int64, device=device).index_add_(0, idx, v64 * v64)
+            self.key_cap, self.value_cap = int(distinct / 0.9), int(n / 0.5)
+            self.table = wc.BucketListHashTable(self.key_cap, self.value_cap, key_bytes=4,
+                                                value_bytes=4, grow_factor=1.1, min_bucket_size=1,
+                                                bits=(29, 18, 15))
+            self.begin = torch.empty(self.q, dtype=torch.int64, device=device)
+            self.end = torch.empty(self.q, dtype=torch.int64, device=device)
+            self.out = torch.empty(n, dtype=torch.int32, device=device)
+            # insert: pair in + the key window's sector + the handle's sector
+            # + the pool sector written; retrieve: key in, offsets out, key
+            # window and handle sectors in the count and value passes, one
+            # value out per query on average
+            self.bytes_insert, self.bytes_retrieve = 4 + 4 + 32 + 32 + 32, 4 + 16 + 4 * 32 + 4
         elif kind == "bloom64":
             keys = unique_keys64(0, 2 * n, seed, device)
             self.keys = keys[:n].contiguous()
@@ -276,7 +304,7 @@ class Workload:
     def insert(self, stream):
         if self.sharded:
             self.table.insert(self.keys, self.values)
-        elif self.kind in ("svht32", "svht64", "mv32", "mb32"):
+        elif self.kind in ("svht32", "svht64", "mv32", "mb32", "bl32"):
             self.table.insert(self.keys, self.values, stream=stream)
         else:
             self.table.insert(self.keys, stream=stream)
@@ -284,7 +312,7 @@ class Workload:
     def retrieve(self, stream):
         if self.sharded:
             self.table.retrieve(self.queries, self.out)
-        elif self.kind in ("mv32", "mb32"):
+        elif self.kind in ("mv32", "mb32", "bl32"):
             self.table.retrieve(self.queries, self.begin, self.end, self.out, stream=stream)
         else:
             self.table.retrieve(self.queries, self.out, stream=stream)
@@ -307,7 +335,7 @@ class Workload:
             return bool(torch.equal(got[present], self.hist[present]))
         if self.kind == "bloom64":
             return bool(out[self.n:].all())
-        if self.kind in ("mv32", "mb32"):
+        if self.kind in ("mv32", "mb32", "bl32"):
             return self.mv_ok(self.begin, self.end, out)
         return False
 
@@ -357,10 +385,11 @@ class Workload:
             self.retrieve(s)
             torch.cuda.synchronize()
             return bool(self.out[self.n:].all())
-        if self.kind in ("mv32", "mb32"):
+        if self.kind in ("mv32", "mb32", "bl32"):
             self.retrieve(s)
             torch.cuda.synchronize()
-            return (self.mv_ok(self.begin, self.end, self.out) and self.table.size() == self.n
+            size = self.table.num_values() if self.kind == "bl32" else self.table.size()
+            return (self.mv_ok(self.begin, self.end, self.out) and size == self.n
                     and self.table.num_keys() == self.distinct)
         return False
 
@@ -415,6 +444,14 @@ def reference_gpu(wl, reps=5):
                               vp(re_.data_ptr()), vp(out.data_ptr()), ctypes.byref(num),
                               u64(wl.min_cap), ctypes.c_uint32(wl.bucket), ctypes.c_int(reps),
                               ctypes.byref(ti), ctypes.byref(tr), ctypes.byref(cap))
+    elif wl.kind == "bl32":
+        rb, re_ = torch.empty_like(wl.begin), torch.empty_like(wl.end)
+        num = ctypes.c_uint64(0)
+        rc = lib.ref_bl32_run(vp(wl.keys.data_ptr()), vp(wl.values.data_ptr()), u64(wl.n),
+                              vp(wl.queries.data_ptr()), u64(wl.q), vp(rb.data_ptr()),
+                              vp(re_.data_ptr()), vp(out.data_ptr()), ctypes.byref(num),
+                              u64(wl.key_cap), u64(wl.value_cap), ctypes.c_int(reps),
+                              ctypes.byref(ti), ctypes.byref(tr), ctypes.byref(cap))
     elif wl.kind == "bloom64":
         rc = lib.ref_bloom64_run(vp(wl.keys.data_ptr()), u64(wl.n), vp(wl.queries.data_ptr()),
                                  u64(wl.q), vp(out.data_ptr()), u64(16 * wl.n), u64(8),
@@ -425,7 +462,7 @@ def reference_gpu(wl, reps=5):
     if rc != 0:
         return {"error": "CUDA error %d" % rc}
     # the reference's answers on the same inputs must equal ours
-    same = wl.mv_ok(rb, re_, out) if wl.kind in ("mv32", "mb32") else wl.answers_ok(out)
+    same = wl.mv_ok(rb, re_, out) if wl.kind in ("mv32", "mb32", "bl32") else wl.answers_ok(out)
     ins_g = wl.n / (ti.value * 1e-3) / 1e9
     ret_g = wl.q / (tr.value * 1e-3) / 1e9
     return {"insert_gops": round(ins_g, 4), "retrieve_gops": round(ret_g, 4),
@@ -447,6 +484,9 @@ WORKLOAD_NAMES = {
             "one shuffled batch) + retrieve every key and as many absent keys",
     "mb32": "MultiBucketHashTable<u32,u32> CG8 bucket {B}, key LF{LF}: insert 2^{L} values "
             "(key i mod 2^{L3} + 1, 8 per key) + retrieve keys 1..2^{L} (two-phase, offsets)",
+    "bl32": "BucketListHashTable<u32,u32> CG8 BucketListStore<29,18,15> grow 1.1: insert 2^{L} "
+            "values (key i mod 2^{L3} + 1, 8 per key; key LF 0.9, pool LF 0.5) + retrieve keys "
+            "1..2^{L} (two-phase, offsets)",
     "served": "4096 SingleValueHashTable<u32,u32> (caps log-uniform 2^10..2^22, LF 0.85), "
               "Poisson requests (batch 2^6..2^18, 30% insert, 80% hit): continuous batching vs plain launches",
 }
@@ -628,7 +668,7 @@ def run_e2e(wl, stream, args, world):
     d2h = ho.numel() * ho.element_size()
     keys0, vals0, q0 = wl.keys, wl.values, wl.queries
     steps = max(1, min(args.steps, 3))
-    piped = hasattr(wl.table, "insert_from_host") and not wl.sharded and wl.kind not in ("mv32", "mb32")
+    piped = hasattr(wl.table, "insert_from_host") and not wl.sharded and wl.kind not in ("mv32", "mb32", "bl32")
     if piped:
         # host buffers straight into the C ABI: chunks of 2^22 keys, copy-in
         # / kernel / copy-out overlapped; a miss gets the fill value the

@@ -49,6 +49,7 @@ struct true_permutation_hasher {};
 struct probing_scheme {};
 struct cycle_free_probing_scheme {};
 struct key_value_storage {};
+struct dynamic_value_storage {};
 struct status_handler {};
 } // namespace tags
 
@@ -310,14 +311,56 @@ class QuadraticProbing {
 
 namespace storage {
 namespace key_value {
-/* the AoS slot store (storage.cuh:438-645) is the only layout */
+/* the AoS slot store (storage.cuh:438-645): {key, value} slots */
 template <class Key, class Value>
 struct AoSStore {
     using key_type = Key;
     using value_type = Value;
     using tag = tags::key_value_storage;
 };
+/* SoAStore (storage.cuh:218-432): accepted wherever AoSStore is.  It names
+ * the same key and value types; the tables choose their own layout in HBM
+ * (single-value tables keep {key, value} slots so that one compare-and-swap
+ * publishes both; the multi-bucket and bucket-list tables keep keys apart
+ * from values), so answers do not depend on this parameter. */
+template <class Key, class Value>
+struct SoAStore {
+    using key_type = Key;
+    using value_type = Value;
+    using tag = tags::key_value_storage;
+};
 } // namespace key_value
+namespace multi_value {
+/* BucketListStore<Value, BucketIndexBits, ValueCounterBits, BucketSizeBits>
+ * (storage.cuh:890-1454): names the value type and the bit widths of the
+ * bucket-list handles; the store itself lives in the library */
+template <class Value, index_t BucketIndexBits = 32, index_t ValueCounterBits = 20,
+          index_t BucketSizeBits = 10>
+struct BucketListStore {
+    static_assert(BucketIndexBits + ValueCounterBits + BucketSizeBits + 2 <= 64,
+                  "Too many bits for bucket index and value counter and bucket size.");
+    using value_type = Value;
+    using index_type = index_t;
+    using tag = tags::dynamic_value_storage;
+    struct handle_type {
+        __host__ __device__ static constexpr index_t max_bucket_index() noexcept
+        {
+            return (index_t{1} << BucketIndexBits) - 1;
+        }
+        __host__ __device__ static constexpr index_t max_value_count() noexcept
+        {
+            return (index_t{1} << ValueCounterBits) - 1;
+        }
+        __host__ __device__ static constexpr index_t max_bucket_size() noexcept
+        {
+            return (index_t{1} << BucketSizeBits) - 1;
+        }
+    };
+    __host__ __device__ static constexpr index_t bucket_index_bits() noexcept { return BucketIndexBits; }
+    __host__ __device__ static constexpr index_t value_counter_bits() noexcept { return ValueCounterBits; }
+    __host__ __device__ static constexpr index_t bucket_size_bits() noexcept { return BucketSizeBits; }
+};
+} // namespace multi_value
 } // namespace storage
 
 /* defaults.cuh:9-44 */
@@ -337,6 +380,8 @@ using probing_scheme_t = probing_schemes::DoubleHashing<hasher_t<Key>, hasher_t<
 using status_handler_t = status_handlers::ReturnNothing;
 template <class Key, class Value>
 using table_storage_t = storage::key_value::AoSStore<Key, Value>;
+template <class Value>
+using value_storage_t = storage::multi_value::BucketListStore<Value>;
 } // namespace defaults
 
 namespace detail {

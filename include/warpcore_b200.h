@@ -275,6 +275,83 @@ int wc_mvht_retrieve_all_keys(wc_table *t, void *keys_out, uint64_t *num_out, wc
 int wc_mvht_num_keys(wc_table *t, wc_stream_t stream, uint64_t *out);
 
 /* ------------------------------------------------------------------ */
+/* BucketListHashTable<Key, Value, EmptyKey, TombstoneKey,               */
+/* BucketListStore<Value, IndexBits, CounterBits, SizeBits>, Probing>    */
+/* (bucket_list_hash_table.cuh, storage.cuh:651-1454).  A key table maps */
+/* each key to a list of value buckets in a pool of value_capacity       */
+/* elements: the first bucket holds min_bucket_size values, each later   */
+/* one a header and ceil(previous size * grow_factor) values, at most    */
+/* max_bucket_size.  The bit widths bound the pool (2^index_bits - 1),   */
+/* the values per key (2^counter_bits - 1) and the bucket size           */
+/* (2^size_bits - 1); the reference's defaults are 32 / 20 / 10.         */
+/* ------------------------------------------------------------------ */
+
+typedef struct wc_blht wc_blht;
+
+typedef struct wc_blht_info {
+    uint32_t key_bytes, value_bytes, cg_size, probing, hasher1, hasher2;
+    uint32_t index_bits, counter_bits, size_bits;
+    float grow_factor;
+    uint64_t key_capacity;    /* key slots, reference capacity rule */
+    uint64_t value_capacity;  /* pool elements */
+    uint64_t num_buckets;     /* key_capacity / cg_size */
+    uint64_t seed, empty_key, tombstone_key;
+    uint64_t min_bucket_size, max_bucket_size, max_values_per_key;
+    uint64_t bytes_total;     /* keys, handles, pool, the pool counter */
+    void *keys;               /* device: key_capacity keys */
+    unsigned long long *handles; /* device: one list handle per key slot */
+    unsigned long long *pool; /* device: value_capacity values or bucket headers */
+    unsigned long long *next_free; /* device: pool elements handed out */
+    uint32_t *status;         /* device Status word */
+    int is_initialized;
+} wc_blht_info;
+
+/* BucketListHashTable(key_capacity, value_capacity, seed, grow_factor,
+ * min_bucket_size, max_bucket_size, max_values_per_key, no_init)
+ * (bucket_list_hash_table.cuh:106-121) with BucketListStore's bit widths;
+ * a configuration the store refuses (storage.cuh:990-1014) is
+ * WC_ERR_INVALID_ARGUMENT.  max_values_per_key is capped at
+ * 2^counter_bits - 1. */
+int wc_blht_create(const wc_table_config *cfg, uint64_t key_capacity, uint64_t value_capacity,
+                   uint64_t seed, float grow_factor, uint64_t min_bucket_size,
+                   uint64_t max_bucket_size, uint64_t max_values_per_key, uint32_t index_bits,
+                   uint32_t counter_bits, uint32_t size_bits, int no_init, wc_blht **out);
+int wc_blht_destroy(wc_blht *t);
+/* init(seed) (:160-176): keys empty, every list empty, pool counter zero */
+int wc_blht_init(wc_blht *t, uint64_t seed, wc_stream_t stream);
+/* insert (:235-326): the key's status from the key table (none,
+ * duplicate_key, probing_length_exceeded, invalid_key) plus the append's
+ * (max_values_for_key_reached, out_of_memory when the pool is used up).
+ * Every key gets a status; the reference writes none for a key that found
+ * no slot. */
+int wc_blht_insert(wc_blht *t, const void *keys_in, const void *values_in, uint64_t num_in,
+                   wc_stream_t stream, uint64_t probing_length, void *status_out,
+                   int status_handler, uint32_t ignore);
+/* num_values (:776-800): list lengths per key and their sum (synchronises) */
+int wc_blht_num_values(wc_blht *t, const void *keys_in, uint64_t num_in, uint64_t *num_out,
+                       uint64_t *num_per_key_out, wc_stream_t stream, uint64_t probing_length,
+                       void *status_out, int status_handler, uint32_t ignore);
+/* retrieve (:375-466): every key's list at values_out[begin[i] .. end[i]),
+ * newest bucket first; values_out NULL is a dry run (per-key counts in
+ * end_offsets_out, status dry_run).  Synchronises `stream`. */
+int wc_blht_retrieve(wc_blht *t, const void *keys_in, uint64_t num_in,
+                     uint64_t *begin_offsets_out, uint64_t *end_offsets_out, void *values_out,
+                     uint64_t *num_out, wc_stream_t stream, uint64_t probing_length,
+                     void *status_out, int status_handler, uint32_t ignore);
+/* retrieve_all_keys (:574-605): every stored key, order unspecified;
+ * keys_out NULL gives the count */
+int wc_blht_retrieve_all_keys(wc_blht *t, void *keys_out, uint64_t *num_out, wc_stream_t stream);
+/* num_keys (:719-726), num_values() (:797-818: the sum of all list
+ * lengths), the pool elements handed out (value_load_factor = used /
+ * value_capacity, storage.cuh:1369-1396) */
+int wc_blht_num_keys(wc_blht *t, wc_stream_t stream, uint64_t *out);
+int wc_blht_total_values(wc_blht *t, wc_stream_t stream, uint64_t *out);
+int wc_blht_pool_used(wc_blht *t, wc_stream_t stream, uint64_t *out);
+int wc_blht_peek_status(wc_blht *t, wc_stream_t stream, uint32_t *out);
+int wc_blht_pop_status(wc_blht *t, wc_stream_t stream, uint32_t *out);
+int wc_blht_get_info(const wc_blht *t, wc_blht_info *info);
+
+/* ------------------------------------------------------------------ */
 /* MultiBucketHashTable<Key, Value, EmptyKey, TombstoneKey, EmptyValue,  */
 /* ProbingScheme, AoSStore<Key, ArrayBucket<Value, B>>>                  */
 /* (multi_bucket_hash_table.cuh).  A slot holds a key and a bucket of    */

@@ -64,6 +64,20 @@ def _load():
         "wco_mv_retrieve": (_u64, [_vp, _vp, _u64, _vp, _vp, _vp, _u64, _vp]),
         "wco_mv_num_keys": (_u64, [_vp]),
         "wco_mv_unique_keys": (_u64, [_vp, _vp]),
+        "wco_bl_create": (_vp, [_i, _i, _u64, _u64, _u64, ctypes.c_float, _u64, _u64, _u64, _u64,
+                                _u64, _u64, _u64]),
+        "wco_bl_destroy": (None, [_vp]),
+        "wco_bl_init": (None, [_vp, _u64]),
+        "wco_bl_key_capacity": (_u64, [_vp]),
+        "wco_bl_insert": (None, [_vp, _vp, _vp, _u64, _u64, _vp]),
+        "wco_bl_num_values": (_u64, [_vp, _vp, _u64, _vp, _u64, _vp]),
+        "wco_bl_retrieve": (_u64, [_vp, _vp, _u64, _vp, _vp, _vp, _u64, _vp]),
+        "wco_bl_num_keys": (_u64, [_vp]),
+        "wco_bl_total_values": (_u64, [_vp]),
+        "wco_bl_next_free": (_u64, [_vp]),
+        "wco_bl_all_keys": (_u64, [_vp, _vp]),
+        "wco_bl_peek_status": (ctypes.c_uint32, [_vp]),
+        "wco_bl_pop_status": (ctypes.c_uint32, [_vp]),
         "wco_mb_create": (_vp, [_i, _i, _u64, _u64, _u64, _u64, _i, _i, _i, _u64, _u64, _u64,
                                 _u64]),
         "wco_mb_destroy": (None, [_vp]),
@@ -308,6 +322,93 @@ class MVTable(Table):
         k = np.empty(max(self.capacity, 1), dtype=_kdtype(self.key_bytes))
         n = lib().wco_mv_unique_keys(self.h, _ptr(k))
         return k[:n]
+
+
+class BLTable:
+    """Sequential reference-order BucketListHashTable (BucketListStore with
+    index / counter / size bits; default 32 / 20 / 10)."""
+
+    def __init__(self, key_bytes, value_bytes, key_capacity, value_capacity, seed=DEFAULT_SEED,
+                 grow_factor=1.1, min_bucket_size=1, max_bucket_size=None,
+                 max_values_per_key=None, bits=(32, 20, 10), cg=8):
+        ib, cb, sb = bits
+        if max_bucket_size is None:
+            max_bucket_size = (1 << sb) - 1
+        if max_values_per_key is None:
+            max_values_per_key = (1 << cb) - 1
+        self.key_bytes = key_bytes
+        self.value_bytes = value_bytes
+        self.value_capacity = value_capacity
+        self.h = lib().wco_bl_create(key_bytes, value_bytes, int(key_capacity),
+                                     int(value_capacity), int(seed), float(grow_factor),
+                                     int(min_bucket_size), int(max_bucket_size),
+                                     int(max_values_per_key), ib, cb, sb, cg)
+        if not self.h:
+            raise ValueError("invalid bucket list configuration")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().wco_bl_destroy(self.h)
+            self.h = None
+
+    @property
+    def key_capacity(self):
+        return lib().wco_bl_key_capacity(self.h)
+
+    def init(self, seed=DEFAULT_SEED):
+        lib().wco_bl_init(self.h, int(seed))
+
+    def insert(self, keys, values, probing_length=DEFAULT_PROBING_LENGTH, want_status=False,
+               status_fill=0):
+        """statuses of keys that found no slot keep `status_fill`"""
+        keys = np.ascontiguousarray(keys)
+        values = np.ascontiguousarray(values)
+        st = np.full(len(keys), status_fill, dtype=np.uint32) if want_status else None
+        lib().wco_bl_insert(self.h, _ptr(keys), _ptr(values), len(keys), int(probing_length),
+                            _ptr(st))
+        return st
+
+    def num_values(self, keys, probing_length=DEFAULT_PROBING_LENGTH):
+        keys = np.ascontiguousarray(keys)
+        c = np.zeros(len(keys), dtype=np.uint64)
+        st = np.zeros(len(keys), dtype=np.uint32)
+        total = lib().wco_bl_num_values(self.h, _ptr(keys), len(keys), _ptr(c),
+                                        int(probing_length), _ptr(st))
+        return total, c, st
+
+    def retrieve(self, keys, dry_run=False, probing_length=DEFAULT_PROBING_LENGTH, fill=0):
+        """(begin, end, values, statuses); a list whose pool ran out is not
+        read, so its part of the values keeps `fill`"""
+        keys = np.ascontiguousarray(keys)
+        n = len(keys)
+        b = np.zeros(n, dtype=np.uint64)
+        e = np.zeros(n, dtype=np.uint64)
+        st = np.zeros(n, dtype=np.uint32)
+        total = 0 if dry_run else self.num_values(keys, probing_length)[0]
+        vals = None if dry_run else np.full(max(int(total), 1), fill, dtype=_kdtype(self.value_bytes))
+        lib().wco_bl_retrieve(self.h, _ptr(keys), n, _ptr(b), _ptr(e), _ptr(vals),
+                              int(probing_length), _ptr(st))
+        return b, e, (vals[:int(total)] if vals is not None else None), st
+
+    def num_keys(self):
+        return lib().wco_bl_num_keys(self.h)
+
+    def total_values(self):
+        return lib().wco_bl_total_values(self.h)
+
+    def next_free(self):
+        return lib().wco_bl_next_free(self.h)
+
+    def all_keys(self):
+        k = np.empty(max(self.key_capacity, 1), dtype=_kdtype(self.key_bytes))
+        n = lib().wco_bl_all_keys(self.h, _ptr(k))
+        return k[:n]
+
+    def peek_status(self):
+        return lib().wco_bl_peek_status(self.h)
+
+    def pop_status(self):
+        return lib().wco_bl_pop_status(self.h)
 
 
 class MBTable:

@@ -18,6 +18,7 @@
 #include <warpcore/bloom_filter.cuh>
 #include <warpcore/multi_value_hash_table.cuh>
 #include <warpcore/multi_bucket_hash_table.cuh>
+#include <warpcore/bucket_list_hash_table.cuh>
 #include <algorithm>
 
 #include <cstdio>
@@ -633,6 +634,120 @@ static void mb_case(const char *tag, uint64_t n, uint64_t min_cap, uint64_t ksee
     cudaFree(dq); cudaFree(db); cudaFree(de); cudaFree(dvals); cudaFree(dku); cudaFree(dst);
 }
 
+/* BucketListHashTable<K, V> over BucketListStore<V, IB, CB, SB>: eight
+ * insert rounds over shrinking prefixes of n keys (one value per key per
+ * round, so each key's list is built in a fixed order; every batch a
+ * multiple of 128 keys, the bulk insert's groups per block), round 0 with an
+ * invalid key; then counts, a dry run, the two-phase retrieve, num_keys,
+ * num_values, the value load factor and all keys.  exhaust_after >= 0 sizes
+ * the value pool to what the oracle's rounds 0 .. exhaust_after use, so
+ * every later bucket allocation fails (out_of_memory) whatever the order.
+ * The status buffer starts at 0xffffffff: the reference writes no status
+ * for a key that found no slot. */
+template <class K, class V, uint64_t IB, uint64_t CB, uint64_t SB>
+static void bl_case(const char *tag, uint64_t n, uint64_t key_cap, uint64_t value_cap,
+                    float grow, uint64_t min_b, uint64_t max_b, uint64_t max_values,
+                    uint64_t kseed, int exhaust_after)
+{
+    using Store = wc::storage::multi_value::BucketListStore<V, IB, CB, SB>;
+    using Table = wc::BucketListHashTable<K, V, wc::defaults::empty_key<K>(),
+                                          wc::defaults::tombstone_key<K>(), Store,
+                                          wc::defaults::probing_scheme_t<K, 8>>;
+    using SH = wc::status_handlers::ReturnStatus;
+    using index_t = wc::index_t;
+    const std::string p = tag;
+    std::vector<K> all = unique_keys<K>(n + n / 4, kseed);
+    std::vector<K> keys(all.begin(), all.begin() + n);
+    std::vector<std::vector<K>> rk;
+    std::vector<std::vector<V>> rv;
+    for (uint64_t r = 0; r < 8; r++) {
+        const uint64_t m = n - r * (n / 8);
+        std::vector<K> kr(keys.begin(), keys.begin() + m);
+        std::vector<V> vr = uniform<V>(m, kseed + 10 + r);
+        if (r == 0) kr[11] = wc::defaults::tombstone_key<K>();
+        rk.push_back(kr);
+        rv.push_back(vr);
+    }
+    if (exhaust_after >= 0) {
+        wco_bl *o = wco_bl_create(sizeof(K), sizeof(V), key_cap, uint64_t(1) << 22, 0x5ad0ded,
+                                  grow, min_b, max_b, max_values, IB, CB, SB, 8);
+        for (int r = 0; r <= exhaust_after; r++)
+            wco_bl_insert(o, rk[r].data(), rv[r].data(), rk[r].size(), ~0ull - 1024, nullptr);
+        value_cap = wco_bl_next_free(o);
+        wco_bl_destroy(o);
+    }
+    Table t(key_cap, value_cap, wc::defaults::seed<K>(), grow, min_b, max_b, max_values);
+    wc::Status *dst;
+    CK(cudaMalloc(&dst, sizeof(wc::Status) * (n + n / 4)));
+    std::vector<uint32_t> st_rounds;
+    std::vector<K> keys_rounds;
+    std::vector<V> vals_rounds;
+    for (uint64_t r = 0; r < 8; r++) {
+        const uint64_t m = rk[r].size();
+        K *dk = to_dev(rk[r]);
+        V *dv = to_dev(rv[r]);
+        CK(cudaMemset(dst, 0xff, sizeof(wc::Status) * m));
+        t.template insert<SH>(dk, dv, m, 0, wc::defaults::probing_length(), dst);
+        auto st = to_host((uint32_t *)dst, m);
+        st_rounds.insert(st_rounds.end(), st.begin(), st.end());
+        keys_rounds.insert(keys_rounds.end(), rk[r].begin(), rk[r].end());
+        vals_rounds.insert(vals_rounds.end(), rv[r].begin(), rv[r].end());
+        cudaFree(dk);
+        cudaFree(dv);
+    }
+    const uint64_t num_keys = t.num_keys();
+    const uint64_t num_values = t.num_values();
+    const float vlf = t.value_load_factor();
+    uint32_t vlf_bits;
+    std::memcpy(&vlf_bits, &vlf, 4);
+    const uint32_t status1 = t.pop_status().base();
+    const uint64_t nq = all.size();
+    K *dq = to_dev(all);
+    index_t *db, *de;
+    CK(cudaMalloc(&db, sizeof(index_t) * nq));
+    CK(cudaMalloc(&de, sizeof(index_t) * nq));
+    index_t num_dry = 0;
+    t.template retrieve<SH>(dq, nq, db, de, nullptr, num_dry, 0, wc::defaults::probing_length(), dst);
+    auto counts_dry = to_host((uint64_t *)de, nq);
+    auto st_dry = to_host((uint32_t *)dst, nq);
+    const uint32_t status2 = t.pop_status().base();
+    V *dvals;
+    CK(cudaMalloc(&dvals, sizeof(V) * (num_dry ? num_dry : 1)));
+    /* a list whose pool ran out is not read (storage.cuh:1304): its part of
+     * the output keeps this fill */
+    CK(cudaMemset(dvals, 0xff, sizeof(V) * (num_dry ? num_dry : 1)));
+    index_t num_out = 0;
+    t.template retrieve<SH>(dq, nq, db, de, dvals, num_out, 0, wc::defaults::probing_length(), dst);
+    auto begin = to_host((uint64_t *)db, nq);
+    auto end = to_host((uint64_t *)de, nq);
+    auto values = to_host(dvals, num_out);
+    auto st_ret = to_host((uint32_t *)dst, nq);
+    const uint32_t status3 = t.pop_status().base();
+    K *dku;
+    CK(cudaMalloc(&dku, sizeof(K) * (num_keys ? num_keys : 1)));
+    index_t num_all = 0;
+    t.retrieve_all_keys(dku, num_all, 0);
+    auto ak = to_host(dku, num_all);
+    std::sort(ak.begin(), ak.end());
+
+    dump(p + "_meta", std::vector<uint64_t>{n, key_cap, value_cap, t.key_capacity(),
+                                            t.value_capacity(), uint64_t(grow * 1000.0f + 0.5f),
+                                            min_b, max_b, max_values, IB, CB, SB, num_keys,
+                                            num_values, vlf_bits, status1, num_dry, status2,
+                                            num_out, status3, num_all, kseed});
+    dump(p + "_insert_keys", keys_rounds);
+    dump(p + "_insert_values", vals_rounds);
+    dump(p + "_insert_status", st_rounds);
+    dump(p + "_dry_counts", counts_dry);
+    dump(p + "_dry_status", st_dry);
+    dump(p + "_begin", begin);
+    dump(p + "_end", end);
+    dump(p + "_values", values);
+    dump(p + "_retrieve_status", st_ret);
+    dump(p + "_all_keys_sorted", ak);
+    cudaFree(dq); cudaFree(db); cudaFree(de); cudaFree(dvals); cudaFree(dku); cudaFree(dst);
+}
+
 static void run_gpu()
 {
     namespace ps = wc::probing_schemes;
@@ -708,6 +823,16 @@ static void run_gpu()
     mb_case<uint32_t, uint32_t, 8>("mb_u32u32_b8", 4000, 8000, 85, ~uint64_t(0));
     mb_case<uint32_t, uint64_t, 2>("mb_u32u64_b2", 4000, 16000, 86, ~uint64_t(0));
     mb_case<uint64_t, uint64_t, 4>("mb_u64u64_b4_max2", 4000, 16000, 87, 2);
+    bl_case<uint32_t, uint32_t, 32, 20, 10>("bl_u32u32", 4096, 5120, 65536, 1.1f, 1, 1023,
+                                            (1u << 20) - 1, 91, -1);
+    bl_case<uint32_t, uint32_t, 29, 18, 15>("bl_u32u32_bench_bits_max6", 4096, 5120, 65536, 1.1f, 1,
+                                            (1u << 15) - 1, 6, 92, -1);
+    bl_case<uint32_t, uint32_t, 32, 20, 10>("bl_u32u32_min2_grow15_max4", 4096, 5120, 65536, 1.5f,
+                                            2, 4, (1u << 20) - 1, 93, -1);
+    bl_case<uint64_t, uint64_t, 32, 20, 10>("bl_u64u64", 4096, 5120, 65536, 1.1f, 1, 1023,
+                                            (1u << 20) - 1, 94, -1);
+    bl_case<uint32_t, uint32_t, 32, 20, 10>("bl_u32u32_oom", 4096, 5120, 0, 1.1f, 1, 1023,
+                                            (1u << 20) - 1, 95, 2);
 }
 
 int main(int argc, char **argv)

@@ -746,6 +746,329 @@ uint64_t wco_mv_unique_keys(const wco_table *t, void *keys_out)
 }
 
 /* ------------------------------------------------------------------------ */
+/* BucketListHashTable (bucket_list_hash_table.cuh) over BucketListStore      */
+/* (storage.cuh:651-1454): a single-value table maps each key to a handle of  */
+/* a list of value buckets in a shared pool.  The first bucket holds          */
+/* min_bucket_size values and no header; every later bucket starts with a    */
+/* header {previous bucket, size} and grows by grow_factor (float, ceilf) up  */
+/* to max_bucket_size.  Handles pack {state, bucket index, count, values in   */
+/* the newest bucket} in index_bits / counter_bits / size_bits (+2 state).    */
+/* ------------------------------------------------------------------------ */
+
+enum { BL_UNINIT = 0, BL_INIT = 1, BL_BLOCKING = 2, BL_FULL = 3 };
+
+struct wco_bl {
+    wco_table *keys;               /* SVHT<K, handle> (values hold packed handles) */
+    int value_bytes;
+    uint64_t capacity;             /* pool elements */
+    uint64_t ib, cb, sb;           /* bucket index, counter, bucket size bits */
+    float grow;
+    uint64_t min_bucket, max_bucket, max_values;
+    uint64_t next_free;
+    uint64_t *pool_val, *pool_prev, *pool_size;
+};
+
+static uint64_t bl_head(const wco_bl *b) { return (1ull << b->ib) - 1; }
+
+static uint64_t bl_pack(const wco_bl *b, int state, uint64_t index, uint64_t count, uint64_t tail)
+{
+    return (uint64_t)state | (index << 2) | (count << (2 + b->ib)) | (tail << (2 + b->ib + b->cb));
+}
+
+static void bl_unpack(const wco_bl *b, uint64_t h, int *state, uint64_t *index, uint64_t *count,
+                      uint64_t *tail)
+{
+    *state = (int)(h & 3);
+    *index = (h >> 2) & ((1ull << b->ib) - 1);
+    *count = (h >> (2 + b->ib)) & ((1ull << b->cb) - 1);
+    *tail = (h >> (2 + b->ib + b->cb)) & ((1ull << b->sb) - 1);
+}
+
+/* BucketListHashTable(key_capacity, value_capacity, seed, grow_factor,
+ * min_bucket_size, max_bucket_size, max_values_per_key) (:106-121) with
+ * BucketListStore<Value, index_bits, counter_bits, size_bits>.  NULL when
+ * the store's configuration check (storage.cuh:990-1014) fails. */
+wco_bl *wco_bl_create(int key_bytes, int value_bytes, uint64_t key_capacity,
+                      uint64_t value_capacity, uint64_t seed, float grow_factor,
+                      uint64_t min_bucket_size, uint64_t max_bucket_size,
+                      uint64_t max_values_per_key, uint64_t index_bits, uint64_t counter_bits,
+                      uint64_t size_bits, uint64_t cg)
+{
+    if (index_bits + counter_bits + size_bits + 2 > 64) return NULL;
+    wco_bl *b = (wco_bl *)calloc(1, sizeof(wco_bl));
+    b->ib = index_bits; b->cb = counter_bits; b->sb = size_bits;
+    const uint64_t max_bucket_ok = (1ull << size_bits) - 1;
+    if (!(value_capacity < bl_head(b) && grow_factor >= 1.0f && min_bucket_size >= 1 &&
+          max_bucket_size >= min_bucket_size && max_bucket_size <= max_bucket_ok)) {
+        free(b);
+        return NULL;
+    }
+    b->value_bytes = value_bytes;
+    b->capacity = value_capacity;
+    b->grow = grow_factor;
+    b->min_bucket = min_bucket_size;
+    b->max_bucket = max_bucket_size;
+    const uint64_t max_count = (1ull << counter_bits) - 1;
+    b->max_values = max_values_per_key < max_count ? max_values_per_key : max_count;
+    b->keys = wco_table_create(WCO_SVHT, key_bytes, 8, key_capacity, seed, cg, WCO_PROBE_DOUBLE,
+                               WCO_HASH_MURMUR, WCO_HASH_MURMUR, 0, ~0ull, ~0ull);
+    b->pool_val = (uint64_t *)calloc(value_capacity ? value_capacity : 1, 8);
+    b->pool_prev = (uint64_t *)calloc(value_capacity ? value_capacity : 1, 8);
+    b->pool_size = (uint64_t *)calloc(value_capacity ? value_capacity : 1, 8);
+    wco_bl_init(b, seed);
+    return b;
+}
+
+void wco_bl_destroy(wco_bl *b)
+{
+    if (!b) return;
+    wco_table_destroy(b->keys);
+    free(b->pool_val);
+    free(b->pool_prev);
+    free(b->pool_size);
+    free(b);
+}
+
+/* init (:160-176; storage.cuh:1068-1098): keys empty, every handle
+ * uninitialized, pool headers {head, min_bucket_size}, next free 0 */
+void wco_bl_init(wco_bl *b, uint64_t seed)
+{
+    wco_table_init(b->keys, seed);
+    const uint64_t u = bl_pack(b, BL_UNINIT, bl_head(b), 0, 0);
+    for (uint64_t i = 0; i < b->keys->capacity; i++) b->keys->values[i] = u;
+    for (uint64_t i = 0; i < b->capacity; i++) {
+        b->pool_prev[i] = bl_head(b);
+        b->pool_size[i] = b->min_bucket;
+        b->pool_val[i] = 0;
+    }
+    b->next_free = 0;
+}
+
+uint64_t wco_bl_key_capacity(const wco_bl *b) { return b->keys->capacity; }
+
+/* append (storage.cuh:1108-1285), one call after another */
+static uint32_t bl_append(wco_bl *b, uint64_t *handle, uint64_t value)
+{
+    int state;
+    uint64_t index, count, tail;
+    bl_unpack(b, *handle, &state, &index, &count, &tail);
+    if (state == BL_UNINIT) {
+        const uint64_t alloc = b->next_free;
+        b->next_free += b->min_bucket;
+        if (alloc + b->min_bucket <= b->capacity) {
+            b->pool_val[alloc] = value;
+            *handle = bl_pack(b, BL_INIT, alloc, 1, 1);
+            return WCO_ST_NONE;
+        }
+        *handle = bl_pack(b, BL_FULL, bl_head(b), 0, 0);
+        return WCO_ST_OUT_OF_MEMORY;
+    }
+    if (state == BL_FULL) return WCO_ST_OUT_OF_MEMORY;
+    if (count == b->max_values) return WCO_ST_MAX_VALUES_REACHED;
+    const uint64_t cur_size = count <= b->min_bucket ? b->min_bucket : b->pool_size[index];
+    if (tail == cur_size) {
+        float grown = ceilf((float)cur_size * b->grow);
+        float cap = (float)b->max_bucket;
+        const uint64_t new_size = (uint64_t)(cap < grown ? cap : grown);
+        const uint64_t alloc = b->next_free;
+        b->next_free += new_size + 1;
+        if (alloc + new_size + 1 <= b->capacity) {
+            b->pool_val[alloc + 1] = value;
+            b->pool_prev[alloc] = index;
+            b->pool_size[alloc] = new_size;
+            *handle = bl_pack(b, BL_INIT, alloc, count + 1, 1);
+            return WCO_ST_NONE;
+        }
+        *handle = bl_pack(b, BL_FULL, index, count, tail);
+        return WCO_ST_OUT_OF_MEMORY;
+    }
+    const uint64_t j = count + 1 <= b->min_bucket ? tail : tail + 1;
+    b->pool_val[index + j] = value;
+    *handle = bl_pack(b, BL_INIT, index, count + 1, tail + 1);
+    return WCO_ST_NONE;
+}
+
+/* bulk insert (:235-326): key through the single-value table's insert
+ * (none / duplicate_key / probing_length_exceeded / invalid_key), then the
+ * append unless the key already holds max_values_per_key values; the
+ * status is the sum of both and append errors are joined.  Like the
+ * reference kernel (:300-322), no status is written for a key that found
+ * no slot (invalid key, probing length exceeded). */
+void wco_bl_insert(wco_bl *b, const void *keys, const void *values, uint64_t n,
+                   uint64_t probing_length, uint32_t *status_out)
+{
+    for (uint64_t i = 0; i < n; i++) {
+        uint32_t st = WCO_ST_UNKNOWN_ERROR;
+        const int64_t slot = insert_impl(b->keys, load_elem(keys, b->keys->key_bytes, i),
+                                         probing_length, &st);
+        if (slot >= 0) {
+            uint64_t *h = &b->keys->values[slot];
+            int state;
+            uint64_t index, count, tail;
+            bl_unpack(b, *h, &state, &index, &count, &tail);
+            uint32_t ast;
+            if (count >= b->max_values) ast = WCO_ST_MAX_VALUES_REACHED;
+            else ast = bl_append(b, h, load_elem(values, b->value_bytes, i));
+            if (ast) join(b->keys, ast);
+            st |= ast;
+            if (status_out) status_out[i] = st;
+        }
+    }
+}
+
+/* the single-value table's retrieve of the handle (single_value_hash_table.cuh:268-307) */
+static uint32_t bl_find(wco_bl *b, uint64_t key, uint64_t pl, uint64_t *handle)
+{
+    wco_table *t = b->keys;
+    if (!valid_key(t, key)) {
+        join(t, WCO_ST_INVALID_KEY);
+        return WCO_ST_INVALID_KEY;
+    }
+    probe_t p;
+    probe_begin(&p, t->scheme, t->h1, t->h2, t->key_bytes, t->cg, t->capacity, key, t->seed, pl);
+    uint64_t guard = t->capacity / t->cg + 1;
+    do {
+        int any_empty = 0;
+        for (uint64_t r = 0; r < t->cg; r++) {
+            if (t->keys[p.pos[r]] == key) {
+                *handle = t->values[p.pos[r]];
+                return WCO_ST_NONE;
+            }
+            any_empty |= t->keys[p.pos[r]] == t->empty;
+        }
+        if (any_empty) {
+            join(t, WCO_ST_KEY_NOT_FOUND);
+            return WCO_ST_KEY_NOT_FOUND;
+        }
+    } while (--guard && probe_next(&p));
+    join(t, WCO_ST_PROBING_LENGTH_EXCEEDED);
+    return WCO_ST_PROBING_LENGTH_EXCEEDED;
+}
+
+/* for_each over a list (storage.cuh:1292-1343): the newest bucket's values
+ * first, then every older bucket from its first place; out[index] */
+static void bl_walk(const wco_bl *b, uint64_t h, void *out, uint64_t room)
+{
+    int state;
+    uint64_t index, count, tail;
+    bl_unpack(b, h, &state, &index, &count, &tail);
+    if (state != BL_INIT || index == bl_head(b)) return;
+    uint64_t ptr = index;
+    uint64_t off = count <= b->min_bucket ? 0 : 1;
+    uint64_t g = 0;
+    for (uint64_t l = 0; l < tail; l++, g++)
+        if (out && g < room) store_elem(out, b->value_bytes, g, b->pool_val[ptr + l + off]);
+    while (g < count) {
+        ptr = b->pool_prev[ptr];
+        const int last = g >= count - b->min_bucket;
+        const uint64_t size = last ? b->min_bucket : b->pool_size[ptr];
+        off = last ? 0 : 1;
+        for (uint64_t l = 0; l < size && g < count; l++, g++)
+            if (out && g < room) store_elem(out, b->value_bytes, g, b->pool_val[ptr + l + off]);
+    }
+}
+
+/* bulk num_values (:762-789, gpu_engine.cuh:466-504): the handle's count */
+uint64_t wco_bl_num_values(wco_bl *b, const void *keys, uint64_t n, uint64_t *counts_out,
+                           uint64_t probing_length, uint32_t *status_out)
+{
+    uint64_t total = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t h = 0, num = 0;
+        const uint32_t st = bl_find(b, load_elem(keys, b->keys->key_bytes, i), probing_length, &h);
+        if (st == WCO_ST_NONE) {
+            int state;
+            uint64_t index, tail;
+            bl_unpack(b, h, &state, &index, &num, &tail);
+        }
+        if (counts_out) counts_out[i] = num;
+        total += num;
+        if (status_out) status_out[i] = st;
+    }
+    return total;
+}
+
+/* bulk retrieve (:375-466, gpu_engine.cuh:305-346): counts, scan, then each
+ * key's list at its begin offset; a count that differs from the first
+ * pass's is invalid_phase_overlap.  values_out NULL is a dry run. */
+uint64_t wco_bl_retrieve(wco_bl *b, const void *keys, uint64_t n, uint64_t *begin_out,
+                         uint64_t *end_out, void *values_out, uint64_t probing_length,
+                         uint32_t *status_out)
+{
+    const uint64_t total = wco_bl_num_values(b, keys, n, end_out, probing_length, NULL);
+    if (!values_out) {
+        for (uint64_t i = 0; i < n && status_out; i++) status_out[i] = WCO_ST_DRY_RUN;
+        join(b->keys, WCO_ST_DRY_RUN);
+        return total;
+    }
+    uint64_t s = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        begin_out[i] = s;
+        s += end_out[i];
+        end_out[i] = s;
+    }
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t h = 0, num = 0;
+        uint32_t st = bl_find(b, load_elem(keys, b->keys->key_bytes, i), probing_length, &h);
+        if (st == WCO_ST_NONE) {
+            int state;
+            uint64_t index, tail;
+            bl_unpack(b, h, &state, &index, &num, &tail);
+            char *dst = (char *)values_out + begin_out[i] * (uint64_t)b->value_bytes;
+            bl_walk(b, h, dst, end_out[i] - begin_out[i]);
+        }
+        if (num != end_out[i] - begin_out[i]) {
+            join(b->keys, WCO_ST_INVALID_PHASE_OVERLAP);
+            st |= WCO_ST_INVALID_PHASE_OVERLAP;
+        }
+        if (status_out) status_out[i] = st;
+    }
+    return total;
+}
+
+/* num_keys = the key table's size (:719-726); num_values = the sum of all
+ * handle counts (:797-818); the pool's next free index (load factor,
+ * storage.cuh:1369-1396) */
+uint64_t wco_bl_num_keys(const wco_bl *b) { return wco_size(b->keys); }
+
+uint64_t wco_bl_total_values(const wco_bl *b)
+{
+    uint64_t n = 0;
+    for (uint64_t i = 0; i < b->keys->capacity; i++) {
+        if (!valid_key(b->keys, b->keys->keys[i])) continue;
+        int state;
+        uint64_t index, count, tail;
+        bl_unpack(b, b->keys->values[i], &state, &index, &count, &tail);
+        n += count;
+    }
+    return n;
+}
+
+uint64_t wco_bl_next_free(const wco_bl *b) { return b->next_free; }
+
+/* retrieve_all_keys (:574-605): every valid key of the key table */
+uint64_t wco_bl_all_keys(const wco_bl *b, void *keys_out)
+{
+    uint64_t n = 0;
+    for (uint64_t i = 0; i < b->keys->capacity; i++) {
+        const uint64_t k = b->keys->keys[i];
+        if (!valid_key(b->keys, k)) continue;
+        if (keys_out) store_elem(keys_out, b->keys->key_bytes, n, k);
+        n++;
+    }
+    return n;
+}
+
+uint32_t wco_bl_peek_status(const wco_bl *b) { return b->keys->status; }
+
+uint32_t wco_bl_pop_status(wco_bl *b)
+{
+    const uint32_t s = b->keys->status;
+    b->keys->status = 0;
+    return s;
+}
+
+/* ------------------------------------------------------------------------ */
 /* MultiBucketHashTable (multi_bucket_hash_table.cuh): every slot holds a key */
 /* and a bucket of `bucket` values; a key's values fill its last bucket       */
 /* before a new slot is claimed.  Buckets larger than the group size are not  */

@@ -127,6 +127,32 @@ uint64_t wco_mv_retrieve(wco_table *t, const void *keys, uint64_t n, uint64_t *b
 uint64_t wco_mv_num_keys(const wco_table *t);
 uint64_t wco_mv_unique_keys(const wco_table *t, void *keys_out);
 
+/* BucketListHashTable (bucket_list_hash_table.cuh) with
+ * BucketListStore<Value, index_bits, counter_bits, size_bits>; CG cg,
+ * MurmurHash double hashing, default sentinels */
+typedef struct wco_bl wco_bl;
+wco_bl *wco_bl_create(int key_bytes, int value_bytes, uint64_t key_capacity,
+                      uint64_t value_capacity, uint64_t seed, float grow_factor,
+                      uint64_t min_bucket_size, uint64_t max_bucket_size,
+                      uint64_t max_values_per_key, uint64_t index_bits, uint64_t counter_bits,
+                      uint64_t size_bits, uint64_t cg);
+void wco_bl_destroy(wco_bl *b);
+void wco_bl_init(wco_bl *b, uint64_t seed);
+uint64_t wco_bl_key_capacity(const wco_bl *b);
+void wco_bl_insert(wco_bl *b, const void *keys, const void *values, uint64_t n,
+                   uint64_t probing_length, uint32_t *status_out);
+uint64_t wco_bl_num_values(wco_bl *b, const void *keys, uint64_t n, uint64_t *counts_out,
+                           uint64_t probing_length, uint32_t *status_out);
+uint64_t wco_bl_retrieve(wco_bl *b, const void *keys, uint64_t n, uint64_t *begin_out,
+                         uint64_t *end_out, void *values_out, uint64_t probing_length,
+                         uint32_t *status_out);
+uint64_t wco_bl_num_keys(const wco_bl *b);
+uint64_t wco_bl_total_values(const wco_bl *b);
+uint64_t wco_bl_next_free(const wco_bl *b);
+uint64_t wco_bl_all_keys(const wco_bl *b, void *keys_out);
+uint32_t wco_bl_peek_status(const wco_bl *b);
+uint32_t wco_bl_pop_status(wco_bl *b);
+
 /* MultiBucketHashTable (multi_bucket_hash_table.cuh); bucket <= cg */
 typedef struct wco_mb wco_mb;
 wco_mb *wco_mb_create(int key_bytes, int value_bytes, uint64_t bucket, uint64_t min_capacity,

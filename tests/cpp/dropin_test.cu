@@ -7,6 +7,7 @@
 #include <warpcore/warpcore.cuh>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <numeric>
@@ -495,6 +496,140 @@ static void test_multi_bucket()
     cudaFree(dvv); cudaFree(dnums); cudaFree(dsum); cudaFree(duk);
 }
 
+template <class Table>
+__global__ void device_bl_insert(Table t, const typename Table::key_type *k,
+                                 const typename Table::value_type *v, uint64_t n, uint32_t *st)
+{
+    const auto g = cg::tiled_partition<Table::cg_size()>(cg::this_thread_block());
+    const uint64_t gid = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / Table::cg_size();
+    if (gid >= n) return;
+    const auto s = t.insert(k[gid], v[gid], g);
+    if (g.thread_rank() == 0) st[gid] = s.base();
+}
+
+template <class Table>
+__global__ void device_bl_read(Table t, const typename Table::key_type *k, uint64_t n,
+                               typename Table::value_type *vals, uint64_t per_key, uint64_t *nums,
+                               unsigned long long *sums)
+{
+    const auto g = cg::tiled_partition<Table::cg_size()>(cg::this_thread_block());
+    const uint64_t gid = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / Table::cg_size();
+    if (gid >= n) return;
+    typename Table::index_type num = 0, num2 = 0;
+    t.num_values(k[gid], num, g);
+    t.retrieve(k[gid], vals + gid * per_key, num2, g);
+    t.for_each([=](const typename Table::value_type &v, typename Table::index_type) {
+        atomicAdd(sums, (unsigned long long)v);
+    }, k[gid], g);
+    if (g.thread_rank() == 0) nums[gid] = num == num2 ? num : ~0ull;
+}
+
+/* list order of values appended 0 .. c-1 (storage.cuh:1292-1343): buckets of
+ * min, then ceil(previous * grow) up to max; newest bucket first */
+static std::vector<uint64_t> list_order(uint64_t c, uint64_t min_b, float grow, uint64_t max_b)
+{
+    std::vector<std::pair<uint64_t, uint64_t>> buckets; /* [first, size) */
+    uint64_t first = 0, size = min_b;
+    while (first < c) {
+        buckets.push_back({first, size});
+        first += size;
+        const float g = std::ceil(float(size) * grow);
+        size = uint64_t(float(max_b) < g ? float(max_b) : g);
+    }
+    std::vector<uint64_t> out;
+    for (auto it = buckets.rbegin(); it != buckets.rend(); ++it)
+        for (uint64_t j = it->first; j < it->first + it->second && j < c; ++j) out.push_back(j);
+    return out;
+}
+
+/* BucketListHashTable<u32, u32> (the reference example's types): host and
+ * device inserts, lists in bucket order, device reads and for_each,
+ * max_values_per_key, unique keys, load factors */
+static void test_bucket_list()
+{
+    using T = wc::BucketListHashTable<uint32_t, uint32_t>;
+    const uint64_t n = 3000, rounds = 7;
+    T t(2 * n, 40 * n, wc::defaults::seed<uint32_t>(), 1.1f, 1, T::max_bucket_size(), 6);
+    auto keys = distinct_keys<uint32_t>(n + 100, 97);
+    std::vector<uint32_t> k(keys.begin(), keys.begin() + n);
+    uint32_t *dk = dcopy(k);
+    auto value = [](uint64_t r, uint64_t i) { return uint32_t(r * 100000 + i + 1); };
+    uint32_t *dst;
+    cudaMalloc(&dst, sizeof(uint32_t) * n);
+    for (uint64_t r = 0; r < rounds; r++) {
+        std::vector<uint32_t> v(n);
+        for (uint64_t i = 0; i < n; i++) v[i] = value(r, i);
+        uint32_t *dv = dcopy(v);
+        if (r < 3) {
+            t.insert<wc::status_handlers::ReturnStatus>(dk, dv, n, 0, wc::defaults::probing_length(),
+                                                        reinterpret_cast<wc::Status *>(dst));
+        } else {
+            device_bl_insert<<<blocks_for(n, T::cg_size()), 256>>>(t, dk, dv, n, dst);
+        }
+        auto st = hcopy(dst, n);
+        const uint32_t want = r == 0 ? 0u
+                              : r < 6 ? wc::Status::duplicate_key().base()
+                                      : (wc::Status::duplicate_key() + wc::Status::max_values_for_key_reached()).base();
+        CHECK(std::all_of(st.begin(), st.end(), [&](uint32_t s) { return s == want; }));
+        cudaFree(dv);
+    }
+    CHECK(t.num_keys() == n);
+    CHECK(t.num_values() == 6 * n);
+    std::vector<uint32_t> q(keys.begin(), keys.end());
+    uint32_t *dq = dcopy(q), *dvals;
+    uint64_t *db, *de;
+    cudaMalloc(&db, sizeof(uint64_t) * q.size());
+    cudaMalloc(&de, sizeof(uint64_t) * q.size());
+    T::index_type num_out = 0;
+    t.retrieve(dq, q.size(), db, de, nullptr, num_out);
+    CHECK(num_out == 6 * n);
+    cudaMalloc(&dvals, sizeof(uint32_t) * num_out);
+    t.retrieve(dq, q.size(), db, de, dvals, num_out);
+    auto b = hcopy(db, q.size()), e = hcopy(de, q.size());
+    auto vals = hcopy(dvals, num_out);
+    const auto order = list_order(6, 1, 1.1f, T::max_bucket_size());
+    bool ok = true;
+    for (uint64_t i = 0; i < n; i++) {
+        ok &= b[i] == 6 * i && e[i] == 6 * i + 6;
+        for (uint64_t j = 0; j < 6; j++) ok &= vals[6 * i + j] == value(order[j], i);
+    }
+    for (uint64_t i = n; i < q.size(); i++) ok &= e[i] == b[i];
+    CHECK(ok);
+    uint32_t *dvv;
+    uint64_t *dnums;
+    unsigned long long *dsum;
+    cudaMalloc(&dvv, sizeof(uint32_t) * 6 * n);
+    cudaMalloc(&dnums, sizeof(uint64_t) * n);
+    cudaMalloc(&dsum, sizeof(unsigned long long));
+    cudaMemset(dsum, 0, sizeof(unsigned long long));
+    device_bl_read<<<blocks_for(n, T::cg_size()), 256>>>(t, dk, n, dvv, 6, dnums, dsum);
+    auto nums = hcopy(dnums, n);
+    auto vv = hcopy(dvv, 6 * n);
+    auto sum = hcopy(dsum, 1);
+    unsigned long long want_sum = 0;
+    ok = true;
+    for (uint64_t i = 0; i < n; i++) {
+        ok &= nums[i] == 6;
+        for (uint64_t j = 0; j < 6; j++) {
+            ok &= vv[6 * i + j] == value(order[j], i);
+            want_sum += value(j, i);
+        }
+    }
+    CHECK(ok);
+    CHECK(sum[0] == want_sum);
+    T::index_type nk = 0;
+    uint32_t *duk;
+    cudaMalloc(&duk, sizeof(uint32_t) * n);
+    t.retrieve_all_keys(duk, nk);
+    auto uk = hcopy(duk, nk);
+    std::sort(uk.begin(), uk.end());
+    std::sort(k.begin(), k.end());
+    CHECK(nk == n && uk == k);
+    CHECK(t.key_load_factor() > 0.f && t.value_load_factor() > 0.f && t.storage_density() > 0.f);
+    cudaFree(dk); cudaFree(dst); cudaFree(dq); cudaFree(db); cudaFree(de); cudaFree(dvals);
+    cudaFree(dvv); cudaFree(dnums); cudaFree(dsum); cudaFree(duk);
+}
+
 int main()
 {
     test_svht_u32();
@@ -504,6 +639,7 @@ int main()
     test_bloom();
     test_multi_value();
     test_multi_bucket();
+    test_bucket_list();
     const cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         std::fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(e));

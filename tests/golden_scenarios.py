@@ -200,3 +200,69 @@ def mb_scenario(F, tag, kb, vb, make_table):
     uk = np.sort(t.unique_keys())
     assert uk.size == num_unique
     assert np.array_equal(uk, F[tag + "_unique_keys_sorted"])
+
+
+BL_CASES = [("bl_u32u32", 4, 4), ("bl_u32u32_bench_bits_max6", 4, 4),
+            ("bl_u32u32_min2_grow15_max4", 4, 4), ("bl_u64u64", 8, 8), ("bl_u32u32_oom", 4, 4)]
+
+UNWRITTEN = 0xFFFFFFFF
+
+
+def bl_scenario(F, tag, kb, vb, make_table):
+    """make_table(key_cap, value_cap, grow, min_b, max_b, max_values, bits) ->
+    object with insert(keys, values, want_status, status_fill) /
+    num_keys / total_values / next_free / pop_status / retrieve(keys,
+    dry_run) / all_keys like oracle.BLTable.  The reference writes no
+    status for a key that found no slot (UNWRITTEN in the fixture); there
+    the table may leave the fill or report the key's own status."""
+    (n, key_cap, value_cap, key_capacity, value_capacity, grow_milli, min_b, max_b, max_values,
+     ib, cb, sb, num_keys, num_values, vlf_bits, s1, num_dry, s2, num_out, s3, num_all,
+     kseed) = F[tag + "_meta"].tolist()
+    allk = o.gen_unique_keys(kb, n + n // 4, kseed)
+    keys = allk[:n]
+    t = make_table(key_cap, value_cap, grow_milli / 1000.0, min_b, max_b, max_values, (ib, cb, sb))
+    assert t.key_capacity == key_capacity
+    st_all, keys_all, vals_all = [], [], []
+    for r in range(8):
+        m = n - r * (n // 8)
+        k = keys[:m].copy()
+        v = o.gen_uniform(vb, m, kseed + 10 + r)
+        if r == 0:
+            k[11] = (1 << (8 * kb)) - 1      # the tombstone key: no slot
+        st_all.append(t.insert(k, v, want_status=True, status_fill=UNWRITTEN))
+        keys_all.append(k)
+        vals_all.append(v)
+    assert np.array_equal(np.concatenate(keys_all), F[tag + "_insert_keys"])
+    assert np.array_equal(np.concatenate(vals_all), F[tag + "_insert_values"])
+    got, want = np.concatenate(st_all), F[tag + "_insert_status"]
+    written = want != UNWRITTEN
+    assert np.array_equal(got[written], want[written])
+    assert np.all((got[~written] == UNWRITTEN) | (got[~written] == o.ST_INVALID_KEY))
+    assert t.num_keys() == num_keys
+    assert t.total_values() == num_values
+    vlf = np.float32(t.next_free()) / np.float32(value_capacity)
+    assert vlf.view(np.uint32) == vlf_bits
+    assert t.pop_status() == s1
+    _, counts, _, st = t.retrieve(allk, dry_run=True)
+    assert int(counts.sum()) == num_dry
+    assert np.array_equal(counts, F[tag + "_dry_counts"])
+    assert np.array_equal(st, F[tag + "_dry_status"])
+    assert t.pop_status() == s2
+    # the output starts all-ones: a list whose pool ran out is not read, so
+    # its part keeps the fill here; in the reference run it keeps the fill
+    # too, except at the front of the buffer, which the reference lends to
+    # its offset scan as temporary storage (bucket_list_hash_table.cuh:437-443)
+    fill = (1 << (8 * vb)) - 1
+    b, e, v, st = t.retrieve(allk, fill=fill)
+    assert np.array_equal(b, F[tag + "_begin"])
+    assert np.array_equal(e, F[tag + "_end"])
+    assert v.size == num_out
+    gv = F[tag + "_values"]
+    read = v != fill
+    assert np.array_equal(v[read], gv[read])
+    assert np.all((gv[~read] == fill) | (np.nonzero(~read)[0] * vb < 4096))
+    assert np.array_equal(st, F[tag + "_retrieve_status"])
+    assert t.pop_status() == s3
+    ak = np.sort(t.all_keys())
+    assert ak.size == num_all
+    assert np.array_equal(ak, F[tag + "_all_keys_sorted"])

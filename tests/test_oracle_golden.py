@@ -68,3 +68,11 @@ def test_multi_value(tag, kb):
 def test_multi_bucket(tag, kb, vb):
     gs.mb_scenario(F, tag, kb, vb, lambda cap, bucket, mx: o.MBTable(
         kb, vb, cap, bucket=bucket, max_values_per_key=mx))
+
+
+@pytest.mark.parametrize("tag,kb,vb", gs.BL_CASES)
+def test_bucket_list(tag, kb, vb):
+    def make(key_cap, value_cap, grow, min_b, max_b, mx, bits):
+        return o.BLTable(kb, vb, key_cap, value_cap, grow_factor=grow, min_bucket_size=min_b,
+                         max_bucket_size=max_b, max_values_per_key=mx, bits=bits)
+    gs.bl_scenario(F, tag, kb, vb, make)

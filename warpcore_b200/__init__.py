@@ -20,7 +20,7 @@ from ._status import Status  # noqa: F401
 
 __all__ = [
     "Status", "SingleValueHashTable", "HashSet", "CountingHashTable", "MultiValueHashTable",
-    "MultiBucketHashTable",
+    "MultiBucketHashTable", "BucketListHashTable",
     "BloomFilter", "lib", "valid_capacity", "WarpcoreError", "set_l2_persistence",
     "HostPipe", "set_fingerprint_policy", "set_fingerprint_ops", "launch_count", "FINGERPRINTS_AUTO", "FINGERPRINTS_ALWAYS",
     "FINGERPRINTS_NEVER",
@@ -57,6 +57,37 @@ class TableConfig(ctypes.Structure):
         ("hasher1", ctypes.c_uint32),
         ("hasher2", ctypes.c_uint32),
         ("cg_size", ctypes.c_uint32),
+    ]
+
+
+class BlInfo(ctypes.Structure):
+    _fields_ = [
+        ("key_bytes", ctypes.c_uint32),
+        ("value_bytes", ctypes.c_uint32),
+        ("cg_size", ctypes.c_uint32),
+        ("probing", ctypes.c_uint32),
+        ("hasher1", ctypes.c_uint32),
+        ("hasher2", ctypes.c_uint32),
+        ("index_bits", ctypes.c_uint32),
+        ("counter_bits", ctypes.c_uint32),
+        ("size_bits", ctypes.c_uint32),
+        ("grow_factor", ctypes.c_float),
+        ("key_capacity", ctypes.c_uint64),
+        ("value_capacity", ctypes.c_uint64),
+        ("num_buckets", ctypes.c_uint64),
+        ("seed", ctypes.c_uint64),
+        ("empty_key", ctypes.c_uint64),
+        ("tombstone_key", ctypes.c_uint64),
+        ("min_bucket_size", ctypes.c_uint64),
+        ("max_bucket_size", ctypes.c_uint64),
+        ("max_values_per_key", ctypes.c_uint64),
+        ("bytes_total", ctypes.c_uint64),
+        ("keys", ctypes.c_void_p),
+        ("handles", ctypes.c_void_p),
+        ("pool", ctypes.c_void_p),
+        ("next_free", ctypes.c_void_p),
+        ("status", ctypes.c_void_p),
+        ("is_initialized", ctypes.c_int),
     ]
 
 
@@ -251,6 +282,21 @@ SIGNATURES = {
                               _i, _u32]),
     "wc_mvht_retrieve_all_keys": (_i, [_vp, _vp, ctypes.POINTER(_u64), _vp]),
     "wc_mvht_num_keys": (_i, [_vp, _vp, ctypes.POINTER(_u64)]),
+    "wc_blht_create": (_i, [ctypes.POINTER(TableConfig), _u64, _u64, _u64, ctypes.c_float, _u64,
+                            _u64, _u64, _u32, _u32, _u32, _i, _pp]),
+    "wc_blht_destroy": (_i, [_vp]),
+    "wc_blht_init": (_i, [_vp, _u64, _vp]),
+    "wc_blht_insert": (_i, [_vp, _vp, _vp, _u64, _vp, _u64, _vp, _i, _u32]),
+    "wc_blht_num_values": (_i, [_vp, _vp, _u64, ctypes.POINTER(_u64), _vp, _vp, _u64, _vp, _i, _u32]),
+    "wc_blht_retrieve": (_i, [_vp, _vp, _u64, _vp, _vp, _vp, ctypes.POINTER(_u64), _vp, _u64, _vp,
+                              _i, _u32]),
+    "wc_blht_retrieve_all_keys": (_i, [_vp, _vp, ctypes.POINTER(_u64), _vp]),
+    "wc_blht_num_keys": (_i, [_vp, _vp, ctypes.POINTER(_u64)]),
+    "wc_blht_total_values": (_i, [_vp, _vp, ctypes.POINTER(_u64)]),
+    "wc_blht_pool_used": (_i, [_vp, _vp, ctypes.POINTER(_u64)]),
+    "wc_blht_peek_status": (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32)]),
+    "wc_blht_pop_status": (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32)]),
+    "wc_blht_get_info": (_i, [_vp, ctypes.POINTER(BlInfo)]),
     "wc_mbht_create": (_i, [ctypes.POINTER(TableConfig), _u32, _u64, _u64, _u64, _u64, _i, _pp]),
     "wc_mbht_destroy": (_i, [_vp]),
     "wc_mbht_init": (_i, [_vp, _vp]),
@@ -636,6 +682,147 @@ class MultiValueHashTable(_Table):
     def num_keys(self, stream=None):
         out = _u64(0)
         _check(lib().wc_mvht_num_keys(self._h, _stream(stream), ctypes.byref(out)))
+        return int(out.value)
+
+
+class BucketListHashTable:
+    """warpcore::BucketListHashTable (bucket_list_hash_table.cuh:17-121) over
+    BucketListStore<Value, index_bits, counter_bits, size_bits>: each key
+    holds a list of value buckets in a pool of `value_capacity` elements;
+    the first bucket has `min_bucket_size` values, each later one
+    ceil(previous * grow_factor), at most `max_bucket_size`.  retrieve
+    returns each key's values newest bucket first, with begin/end offsets."""
+
+    def __init__(self, key_capacity, value_capacity, seed=DEFAULT_SEED, grow_factor=1.1,
+                 min_bucket_size=1, max_bucket_size=None, max_values_per_key=None,
+                 no_init=False, key_bytes=4, value_bytes=None, bits=(32, 20, 10),
+                 empty_key=None, tombstone_key=None, probing=None, hasher1=None, hasher2=None,
+                 cg_size=None):
+        value_bytes = key_bytes if value_bytes is None else value_bytes
+        ib, cb, sb = bits
+        if max_bucket_size is None:
+            max_bucket_size = (1 << sb) - 1
+        if max_values_per_key is None:
+            max_values_per_key = (1 << cb) - 1
+        cfg = _table_config(lib().wc_svht_default_config, key_bytes, key_bytes, empty_key,
+                            tombstone_key, probing, hasher1, hasher2, cg_size)
+        cfg.value_bytes = value_bytes
+        h = ctypes.c_void_p()
+        _check(lib().wc_blht_create(ctypes.byref(cfg), int(key_capacity), int(value_capacity),
+                                    int(seed), float(grow_factor), int(min_bucket_size),
+                                    int(max_bucket_size), int(max_values_per_key), int(ib), int(cb),
+                                    int(sb), int(bool(no_init)), ctypes.byref(h)))
+        self._h = h
+        self._cfg = cfg
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.wc_blht_destroy(h)
+            self._h = None
+
+    def info(self):
+        inf = BlInfo()
+        _check(lib().wc_blht_get_info(self._h, ctypes.byref(inf)))
+        return inf
+
+    @property
+    def key_bytes(self):
+        return self._cfg.key_bytes
+
+    @property
+    def value_bytes(self):
+        return self._cfg.value_bytes
+
+    @property
+    def key_capacity(self):
+        return self.info().key_capacity
+
+    @property
+    def value_capacity(self):
+        return self.info().value_capacity
+
+    def bytes_total(self):
+        return self.info().bytes_total
+
+    def init(self, seed=None, stream=None):
+        s = self.info().seed if seed is None else seed
+        _check(lib().wc_blht_init(self._h, int(s), _stream(stream)))
+
+    def insert(self, keys_in, values_in, num_in=None, stream=None,
+               probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+               status_handler=None, ignore=0):
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        _check_width(values_in, self.value_bytes, "values_in")
+        h = _handler(status_out, status_handler)
+        _check(lib().wc_blht_insert(self._h, _ptr(keys_in), _ptr(values_in),
+                                    _numel(keys_in, num_in), _stream(stream),
+                                    int(probing_length), _ptr(status_out), h, int(ignore)))
+
+    def num_values(self, keys_in=None, num_per_key_out=None, num_in=None, stream=None,
+                   probing_length=DEFAULT_PROBING_LENGTH, status_out=None,
+                   status_handler=None, ignore=0):
+        """list lengths per key (uint64 tensor, optional) and their sum; with
+        no keys, the number of values in the table"""
+        if keys_in is None:
+            return self._counter(lib().wc_blht_total_values, stream)
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        h = _handler(status_out, status_handler)
+        out = _u64(0)
+        _check(lib().wc_blht_num_values(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                        ctypes.byref(out), _ptr(num_per_key_out),
+                                        _stream(stream), int(probing_length), _ptr(status_out),
+                                        h, int(ignore)))
+        return int(out.value)
+
+    def retrieve(self, keys_in, begin_offsets_out, end_offsets_out, values_out=None,
+                 num_in=None, stream=None, probing_length=DEFAULT_PROBING_LENGTH,
+                 status_out=None, status_handler=None, ignore=0):
+        """values_out None: dry run (end_offsets_out gets the counts);
+        returns the total number of values"""
+        _check_width(keys_in, self.key_bytes, "keys_in")
+        if values_out is not None:
+            _check_width(values_out, self.value_bytes, "values_out")
+        h = _handler(status_out, status_handler)
+        out = _u64(0)
+        _check(lib().wc_blht_retrieve(self._h, _ptr(keys_in), _numel(keys_in, num_in),
+                                      _ptr(begin_offsets_out), _ptr(end_offsets_out),
+                                      _ptr(values_out), ctypes.byref(out), _stream(stream),
+                                      int(probing_length), _ptr(status_out), h, int(ignore)))
+        return int(out.value)
+
+    def retrieve_all_keys(self, keys_out=None, stream=None):
+        out = _u64(0)
+        _check(lib().wc_blht_retrieve_all_keys(self._h, _ptr(keys_out), ctypes.byref(out),
+                                               _stream(stream)))
+        return int(out.value)
+
+    def _counter(self, fn, stream):
+        out = _u64(0)
+        _check(fn(self._h, _stream(stream), ctypes.byref(out)))
+        return int(out.value)
+
+    def num_keys(self, stream=None):
+        return self._counter(lib().wc_blht_num_keys, stream)
+
+    def pool_used(self, stream=None):
+        """pool elements handed out (values and bucket headers)"""
+        return self._counter(lib().wc_blht_pool_used, stream)
+
+    def key_load_factor(self, stream=None):
+        return self.num_keys(stream) / self.key_capacity
+
+    def value_load_factor(self, stream=None):
+        return self.pool_used(stream) / self.value_capacity
+
+    def peek_status(self, stream=None):
+        out = ctypes.c_uint32(0)
+        _check(lib().wc_blht_peek_status(self._h, _stream(stream), ctypes.byref(out)))
+        return int(out.value)
+
+    def pop_status(self, stream=None):
+        out = ctypes.c_uint32(0)
+        _check(lib().wc_blht_pop_status(self._h, _stream(stream), ctypes.byref(out)))
         return int(out.value)
 
 
