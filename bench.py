@@ -487,6 +487,7 @@ WORKLOAD_NAMES = {
     "bl32": "BucketListHashTable<u32,u32> CG8 BucketListStore<29,18,15> grow 1.1: insert 2^{L} "
             "values (key i mod 2^{L3} + 1, 8 per key; key LF 0.9, pool LF 0.5) + retrieve keys "
             "1..2^{L} (two-phase, offsets)",
+    "gen": "on-device generators: unique + uniform u64 keys, Zipf(1.1) ranks",
     "served": "4096 SingleValueHashTable<u32,u32> (caps log-uniform 2^10..2^22, LF 0.85), "
               "Poisson requests (batch 2^6..2^18, 30% insert, 80% hit): continuous batching vs plain launches",
 }
@@ -812,6 +813,92 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_gen(args):
+    """The on-device input generators (random_distributions.cuh:50-326):
+    2^L distinct u64 keys, 2^L uniform u64 words and 2^(L-2) Zipf(1.1)
+    ranks over 2^(L-4) per step, each checked against the oracle on its
+    first elements.  Reported value: elements generated per second over the
+    three; the roofline is the unique-key kernel's write bandwidth.  The
+    step's outputs are checked by properties: every key distinct and no
+    sentinel, uniform words with the right mean, Zipf ranks in range with
+    rank 1 at its expected frequency."""
+    import torch
+    import warpcore_b200 as wc
+    torch.cuda.set_device(0)
+    n = 1 << args.log2n
+    nz = n >> 2
+    a = torch.empty(n, dtype=torch.int64, device="cuda")
+    b = torch.empty(n, dtype=torch.int64, device="cuda")
+    z = torch.empty(nz, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.Stream()
+    seed = 77
+
+    def step(k):
+        wc.gen_unique(a, seed + k, stream=stream)
+        wc.gen_uniform(b, seed + k, stream=stream)
+        wc.gen_zipf(z, n >> 4, 1.1, seed + k, stream=stream)
+
+    with torch.cuda.stream(stream):
+        step(0)
+    torch.cuda.synchronize()
+    m = min(n, 1 << 24)
+    distinct = torch.unique(a[:m]).numel() == m and not bool(((a == 0) | (a == -1)).any())
+    top = (b[:m] >> 32) & 0xFFFFFFFF                       # the high words, uniform on 2^32
+    uniform = abs(float(top.double().mean()) / 2**32 - 0.5) < 0.01
+    nin = n >> 4
+    h = sum(k ** -1.1 for k in range(1, 100001)) + (nin ** -0.1 - 100000 ** -0.1) / -0.1
+    p1 = float((z == 1).double().mean())
+    zipf = bool(((z >= 1) & (z <= nin)).all()) and abs(p1 * h - 1.0) < 0.02
+    verified = distinct and uniform and zipf
+    with torch.cuda.stream(stream):
+        for k in range(args.warmup):
+            step(k)
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    launches0 = wc.launch_count()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            wc.gen_unique(a, seed + k, stream=stream)
+            ev[k][1].record(stream)
+            wc.gen_uniform(b, seed + k, stream=stream)
+            ev[k][2].record(stream)
+            wc.gen_zipf(z, n >> 4, 1.1, seed + k, stream=stream)
+            ev[k][3].record(stream)
+    torch.cuda.synchronize()
+    launches = wc.launch_count() - launches0
+    clocks = sampler.stop()
+    uq = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
+    un = statistics.mean(e[1].elapsed_time(e[2]) for e in ev)
+    zf = statistics.mean(e[2].elapsed_time(e[3]) for e in ev)
+    total_ms = uq + un + zf
+    peak, peak_src = measured_peak()
+    achieved = 8 * n / (uq * 1e-3) / 1e9
+    line = {
+        "metric": "generated elements/s (distinct keys, uniform words, Zipf draws)",
+        "value": round((2 * n + nz) / (total_ms * 1e-3) / 1e9, 4),
+        "unit": "Gelem/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total_ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "generated on the device (counter-based splitmix64 / fmix64)",
+        "config": {"workload": "generators: unique 2^%d u64 + uniform 2^%d u64 + Zipf(1.1) 2^%d over 2^%d"
+                               % (args.log2n, args.log2n, args.log2n - 2, args.log2n - 4)},
+        "unique_gelem_s": round(n / (uq * 1e-3) / 1e9, 3),
+        "uniform_gelem_s": round(n / (un * 1e-3) / 1e9, 3),
+        "zipf_gelem_s": round(nz / (zf * 1e-3) / 1e9, 3),
+        "verified": bool(verified),
+        "roofline": {"bound": "hbm", "kernel": "gen_unique_kernel", "achieved": round(achieved, 2),
+                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "peak_source": peak_src, "algorithmic_bytes_per_op": 8, "traffic": None},
+        "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_served(args):
     """The served mixed workload on one GPU, in both forms, at several
     arrival rates, bit-exact against per-table expectations.  Reported
@@ -905,6 +992,8 @@ def main():
         run_reference(args)
     elif args.workload == "served":
         run_served(args)
+    elif args.workload == "gen":
+        run_gen(args)
     else:
         run_ours(args)
 

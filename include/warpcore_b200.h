@@ -275,6 +275,25 @@ int wc_mvht_retrieve_all_keys(wc_table *t, void *keys_out, uint64_t *num_out, wc
 int wc_mvht_num_keys(wc_table *t, wc_stream_t stream, uint64_t *out);
 
 /* ------------------------------------------------------------------ */
+/* Input generators (random_distributions.cuh:50-326), on the device.   */
+/* Element i depends only on (seed, i): the same output for any launch  */
+/* shape.  splitmix64 replaces the reference's kiss_rng (absent).       */
+/* ------------------------------------------------------------------ */
+
+/* uniform_distribution (:50-137): n uniform 4- or 8-byte words */
+int wc_gen_uniform(void *out, uint64_t n, uint32_t bytes, uint64_t seed, wc_stream_t stream);
+/* unique_distribution (:144-251): n distinct keys, never 0 or all ones
+ * (the default empty and tombstone keys), at most 2^32 - 2 for 4-byte keys;
+ * a bijection of the index where the reference rejects Bloom positives */
+int wc_gen_unique(void *out, uint64_t n, uint32_t key_bytes, uint64_t seed, wc_stream_t stream);
+/* zipf_distribution (:259-326): n_out draws of Zipf(s) over ranks
+ * 1 .. n_in by the reference's rejection sampler; out gets in[rank - 1],
+ * or the 1-based rank when `in` is NULL (the reference writes in[rank] and
+ * rank + 1, one past the ranks).  s > 0 and s != 1. */
+int wc_gen_zipf(const void *in, uint64_t n_in, void *out, uint64_t n_out, uint32_t bytes,
+                double s, uint64_t seed, wc_stream_t stream);
+
+/* ------------------------------------------------------------------ */
 /* BucketListHashTable<Key, Value, EmptyKey, TombstoneKey,               */
 /* BucketListStore<Value, IndexBits, CounterBits, SizeBits>, Probing>    */
 /* (bucket_list_hash_table.cuh, storage.cuh:651-1454).  A key table maps */

@@ -113,6 +113,7 @@ def _load():
         "wco_gen_unique_keys": (None, [_i, _u64, _u64, _vp]),
         "wco_gen_uniform": (None, [_i, _u64, _u64, _vp]),
         "wco_gen_zipf_ranks": (None, [_u64, ctypes.c_double, _u64, _u64, _vp]),
+        "wco_gen_zipf_streams": (None, [_vp, _u64, _vp, _u64, _i, ctypes.c_double, _u64]),
         "wco_mt_create": (_vp, [_i, _i, _u64, _u64, _u64]),
         "wco_mt_destroy": (None, [_vp]),
         "wco_mt_clear": (None, [_vp, _i]),
@@ -187,6 +188,14 @@ def gen_uniform(nbytes, n, seed):
 def gen_zipf_ranks(n_in, s, n_out, seed):
     out = np.empty(n_out, dtype=np.uint64)
     lib().wco_gen_zipf_ranks(n_in, s, n_out, seed, _ptr(out))
+    return out
+
+
+def gen_zipf_streams(n_in, s, n_out, seed, key_bytes=8, in_=None):
+    """Zipf draws with one stream per output (the library generator's form):
+    1-based ranks, or in_[rank - 1]"""
+    out = np.empty(n_out, dtype=_kdtype(key_bytes))
+    lib().wco_gen_zipf_streams(_ptr(in_), n_in, _ptr(out), n_out, key_bytes, float(s), seed)
     return out
 
 

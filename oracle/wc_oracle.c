@@ -1557,6 +1557,42 @@ void wco_gen_zipf_ranks(uint64_t n_in, double s, uint64_t n_out, uint64_t seed,
     }
 }
 
+/* Zipf draws with one splitmix64 stream per output (the counter-based form
+ * of the sampler above, as the library's generator draws them): output i's
+ * stream is seeded with mix(seed ^ (i * golden + c)); ranks are 1-based,
+ * or in[rank - 1] when `in` is given. */
+static uint64_t sm_mix(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+void wco_gen_zipf_streams(const void *in, uint64_t n_in, void *out, uint64_t n_out, int bytes,
+                          double s, uint64_t seed)
+{
+    const double t = (pow((double)n_in, 1.0 - s) - s) / (1.0 - s);
+    for (uint64_t i = 0; i < n_out; i++) {
+        const uint64_t st = sm_mix(seed ^ (i * 0x9e3779b97f4a7c15ull + 0x632be59bd9b4e019ull));
+        uint64_t draw = 0, k = 1;
+        for (;;) {
+            const double p = (double)(sm_mix(st + (++draw) * 0x9e3779b97f4a7c15ull) >> 11) *
+                             (1.0 / 9007199254740992.0);
+            const double pt = p * t;
+            const double inv_b = pt <= 1.0 ? pt : pow(pt * (1.0 - s) + s, 1.0 / (1.0 - s));
+            k = (uint64_t)(inv_b + 1.0);
+            const double y = (double)(sm_mix(st + (++draw) * 0x9e3779b97f4a7c15ull) >> 11) *
+                             (1.0 / 9007199254740992.0);
+            const double b = k <= 1 ? 1.0 / t : pow(inv_b, -s) / t;
+            const double rat = pow((double)k, -s) / (b * t);
+            if (y < rat || draw >= (1u << 20)) break;
+        }
+        if (k > n_in) k = n_in;
+        if (k < 1) k = 1;
+        store_elem(out, bytes, i, in ? load_elem(in, bytes, k - 1) : k);
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* multi-threaded CPU port of the reference insert/retrieve                  */
 /* ------------------------------------------------------------------------ */

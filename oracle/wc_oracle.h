@@ -175,6 +175,10 @@ uint64_t wco_mb_unique_keys(const wco_mb *t, void *keys_out);
 uint32_t wco_mb_peek_status(const wco_mb *t);
 uint32_t wco_mb_pop_status(wco_mb *t);
 
+/* Zipf draws, one splitmix64 stream per output (the library's generator) */
+void wco_gen_zipf_streams(const void *in, uint64_t n_in, void *out, uint64_t n_out, int bytes,
+                          double s, uint64_t seed);
+
 typedef struct wco_bloom wco_bloom;
 wco_bloom *wco_bloom_create(int key_bytes, int slot_bytes, uint64_t cg,
                             int hasher, uint64_t num_bits, uint64_t k,

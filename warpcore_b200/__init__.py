@@ -22,7 +22,8 @@ __all__ = [
     "Status", "SingleValueHashTable", "HashSet", "CountingHashTable", "MultiValueHashTable",
     "MultiBucketHashTable", "BucketListHashTable",
     "BloomFilter", "lib", "valid_capacity", "WarpcoreError", "set_l2_persistence",
-    "HostPipe", "set_fingerprint_policy", "set_fingerprint_ops", "launch_count", "FINGERPRINTS_AUTO", "FINGERPRINTS_ALWAYS",
+    "HostPipe", "set_fingerprint_policy", "set_fingerprint_ops", "launch_count",
+    "gen_uniform", "gen_unique", "gen_zipf", "FINGERPRINTS_AUTO", "FINGERPRINTS_ALWAYS",
     "FINGERPRINTS_NEVER",
     "HASH_MURMUR", "HASH_NVIDIA", "HASH_MUELLER", "HASH_IDENTITY32",
     "HASH_IDENTITY64", "PROBING_DOUBLE", "PROBING_LINEAR",
@@ -275,6 +276,9 @@ SIGNATURES = {
     "wc_fingerprint_policy": (_i, [_i, ctypes.POINTER(ctypes.c_int)]),
     "wc_fingerprint_ops": (_i, [_u32, ctypes.POINTER(ctypes.c_uint32)]),
     "wc_launch_count": (_i, [ctypes.POINTER(_u64)]),
+    "wc_gen_uniform": (_i, [_vp, _u64, _u32, _u64, _vp]),
+    "wc_gen_unique": (_i, [_vp, _u64, _u32, _u64, _vp]),
+    "wc_gen_zipf": (_i, [_vp, _u64, _vp, _u64, _u32, ctypes.c_double, _u64, _vp]),
     "wc_mvht_create": (_i, [ctypes.POINTER(TableConfig), _u64, _u64, _u64, _i, _pp]),
     "wc_mvht_insert": (_i, [_vp, _vp, _vp, _u64, _vp, _u64, _vp, _i, _u32]),
     "wc_mvht_num_values": (_i, [_vp, _vp, _u64, ctypes.POINTER(_u64), _vp, _vp, _u64, _vp, _i, _u32]),
@@ -380,6 +384,32 @@ def set_fingerprint_policy(mode):
     prev = ctypes.c_int(0)
     _check(lib().wc_fingerprint_policy(m, ctypes.byref(prev)))
     return prev.value
+
+
+def gen_uniform(out, seed, stream=None):
+    """fill a 4- or 8-byte CUDA tensor with uniform words
+    (random_distributions.cuh:50-137); element i depends only on (seed, i)"""
+    _check(lib().wc_gen_uniform(_ptr(out), out.numel(), out.element_size(), int(seed),
+                                _stream(stream)))
+    return out
+
+
+def gen_unique(out, seed, stream=None):
+    """fill a 4- or 8-byte CUDA tensor with distinct keys, none equal to 0 or
+    all ones (random_distributions.cuh:144-251)"""
+    _check(lib().wc_gen_unique(_ptr(out), out.numel(), out.element_size(), int(seed),
+                               _stream(stream)))
+    return out
+
+
+def gen_zipf(out, n_in, s, seed, in_=None, stream=None):
+    """fill `out` with Zipf(s) draws over ranks 1..n_in
+    (random_distributions.cuh:259-326): in_[rank - 1], or the rank itself"""
+    if in_ is not None:
+        _check_width(in_, out.element_size(), "in_")
+    _check(lib().wc_gen_zipf(_ptr(in_), int(n_in), _ptr(out), out.numel(), out.element_size(),
+                             float(s), int(seed), _stream(stream)))
+    return out
 
 
 def launch_count():
