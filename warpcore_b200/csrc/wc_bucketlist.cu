@@ -76,7 +76,7 @@ __device__ __forceinline__ void bl_write_status(const BlArgs &a, uint64_t i, uin
  * status of a key without a slot (invalid key, probing length exceeded)
  * unwritten, every key gets its status. */
 template <class K, class V, int kW>
-__global__ void __launch_bounds__(256, 4) bl_insert_kernel(const BlArgs a)
+__global__ void __launch_bounds__(256, WC_MULTI_MIN_BLOCKS) bl_insert_kernel(const BlArgs a)
 {
     uint32_t join = 0;
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(256, 4) bl_insert_kernel(const BlArgs a)
 
 /* num_values (kValues false) or retrieve (gpu_engine.cuh:305-346) */
 template <class K, class V, int kW, bool kValues>
-__global__ void __launch_bounds__(256, 4) bl_find_kernel(const BlArgs a)
+__global__ void __launch_bounds__(256, WC_MULTI_MIN_BLOCKS) bl_find_kernel(const BlArgs a)
 {
     uint32_t join = 0;
     unsigned long long total = 0;

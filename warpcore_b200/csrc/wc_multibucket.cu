@@ -87,7 +87,7 @@ __device__ __forceinline__ void mb_flush(const MbView &m, uint32_t join, unsigne
 }
 
 template <class K, class V, int kW, int kB>
-__global__ void __launch_bounds__(256, 4) mb_insert_kernel(const MbArgs a)
+__global__ void __launch_bounds__(256, WC_MULTI_MIN_BLOCKS) mb_insert_kernel(const MbArgs a)
 {
     uint32_t join = 0;
     unsigned claimed = 0, fresh = 0;
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(256, 4) mb_insert_kernel(const MbArgs a)
 
 /* num_values (kValues false) or retrieve of each key's values */
 template <class K, class V, int kW, int kB, bool kValues>
-__global__ void __launch_bounds__(256, 4) mb_find_kernel(const MbArgs a)
+__global__ void __launch_bounds__(256, WC_MULTI_MIN_BLOCKS) mb_find_kernel(const MbArgs a)
 {
     uint32_t join = 0;
     unsigned long long total = 0;

@@ -24,6 +24,14 @@
 namespace warpcore {
 namespace b200 {
 
+/* resident 256-thread blocks per SM the multi-value kernels (multi-value,
+ * multi-bucket, bucket-list) are built for: 4 measured best; 6 and 8
+ * (42 and 32 registers) ran 0-10 % slower on the mv32 / mb32 / bl32
+ * workloads, the register cap costing more than the extra warps bring */
+#ifndef WC_MULTI_MIN_BLOCKS
+#define WC_MULTI_MIN_BLOCKS 4
+#endif
+
 struct MvArgs {
     TableView t;
     const void *keys;
@@ -52,7 +60,7 @@ __device__ __forceinline__ void mv_write_status(const MvArgs &a, uint64_t i, uin
 }
 
 template <class L, int W>
-__global__ void __launch_bounds__(256) mv_insert_kernel(const MvArgs a)
+__global__ void __launch_bounds__(256, WC_MULTI_MIN_BLOCKS) mv_insert_kernel(const MvArgs a)
 {
     using K = typename L::key_t;
     using V = typename L::val_t;
@@ -81,7 +89,7 @@ __global__ void __launch_bounds__(256) mv_insert_kernel(const MvArgs a)
 
 /* num_values (values_out == NULL) or retrieve of each key's values */
 template <class L, int W, bool kValues>
-__global__ void __launch_bounds__(256) mv_find_kernel(const MvArgs a)
+__global__ void __launch_bounds__(256, WC_MULTI_MIN_BLOCKS) mv_find_kernel(const MvArgs a)
 {
     using K = typename L::key_t;
     using V = typename L::val_t;
