@@ -344,6 +344,78 @@ uint64_t warpcore::b200::host_valid_capacity(uint64_t min_capacity, uint64_t cg)
     return valid_capacity(min_capacity, cg);
 }
 
+/* counts in end -> end = inclusive prefix sums, begin = exclusive ones (the
+ * reference's cub::DeviceScan::InclusiveSum step): tile sums, tile offsets,
+ * apply.  The tile-sum buffer grows on demand. */
+int warpcore::b200::host_offsets_scan(void **scratch, uint64_t *scratch_bytes, uint64_t *begin,
+                                      uint64_t *end, uint64_t n, cudaStream_t s)
+{
+    const MvScanKernels k = mv_scan_kernels();
+    const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
+    const uint64_t need = ntiles * sizeof(unsigned long long);
+    if (need > *scratch_bytes) {
+        WC_CUDA(cudaStreamSynchronize(s));
+        if (*scratch) cudaFree(*scratch);
+        *scratch = nullptr;
+        *scratch_bytes = 0;
+        WC_CUDA(cudaMalloc(scratch, need));
+        *scratch_bytes = need;
+    }
+    auto *e = reinterpret_cast<unsigned long long *>(end);
+    auto *b = reinterpret_cast<unsigned long long *>(begin);
+    auto *ts = reinterpret_cast<unsigned long long *>(*scratch);
+    uint64_t nn = n, nt = ntiles;
+    void *a1[] = {&e, &nn, &ts};
+    WC_CUDA(cudaLaunchKernel(k.tile_sums, dim3(unsigned(ntiles)), dim3(kScanThreads), a1, 0, s));
+    void *a2[] = {&ts, &nt};
+    WC_CUDA(cudaLaunchKernel(k.tile_offsets, dim3(1), dim3(kScanThreads), a2, 0, s));
+    /* end == begin + 1: the scan writes end only, begin[0] is zero */
+    int write_begin = e == b + 1 ? 0 : 1;
+    if (!write_begin) WC_CUDA(cudaMemsetAsync(b, 0, sizeof(unsigned long long), s));
+    void *a3[] = {&e, &b, &nn, &ts, &write_begin};
+    WC_CUDA(cudaLaunchKernel(k.apply, dim3(unsigned(ntiles)), dim3(kScanThreads), a3, 0, s));
+    note_launches(3);
+    return WC_OK;
+}
+
+/* join bits into a device Status word from the host (synchronises) */
+int warpcore::b200::host_join_status(uint32_t *status, uint32_t bits, cudaStream_t s)
+{
+    uint32_t cur = 0;
+    WC_CUDA(cudaMemcpyAsync(&cur, status, sizeof(cur), cudaMemcpyDeviceToHost, s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    cur |= bits;
+    WC_CUDA(cudaMemcpyAsync(status, &cur, sizeof(cur), cudaMemcpyHostToDevice, s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    return WC_OK;
+}
+
+/* a dry run's per-key statuses: dry_run for every key */
+int warpcore::b200::host_dry_run_status(void *status_out, uint64_t n, int handler,
+                                        uint32_t ignore, cudaStream_t s)
+{
+    if (!status_out || handler == WC_HANDLER_NOTHING || n == 0) return WC_OK;
+    const MvScanKernels k = mv_scan_kernels();
+    uint64_t nn = n;
+    int h = handler;
+    uint32_t mask = (~ignore) ^ 0xFFFu;
+    void *args[] = {&status_out, &nn, &h, &mask};
+    WC_CUDA(cudaLaunchKernel(k.dry_status, dim3(grid_for(k.dry_status, kBlock, n, kBlock)),
+                             dim3(kBlock), args, 0, s));
+    note_launches(1);
+    return WC_OK;
+}
+
+/* one device counter read back (synchronises) */
+int warpcore::b200::host_read_counter(const unsigned long long *d, cudaStream_t s, uint64_t *out)
+{
+    unsigned long long h = 0;
+    WC_CUDA(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    *out = h;
+    return WC_OK;
+}
+
 static std::atomic<unsigned long long> g_launches{0};
 void warpcore::b200::note_launches(uint32_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
@@ -970,43 +1042,12 @@ int mv_count(wc_table *t, const void *keys, uint64_t n, uint64_t *counts_dev, ui
 /* counts in end -> end = inclusive prefix sums, begin = exclusive ones */
 int mv_scan(wc_table *t, uint64_t *begin, uint64_t *end, uint64_t n, cudaStream_t s)
 {
-    const MvScanKernels k = mv_scan_kernels();
-    const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
-    const uint64_t need = ntiles * sizeof(unsigned long long);
-    if (need > t->scratch_bytes) {
-        WC_CUDA(cudaStreamSynchronize(s));
-        if (t->scratch) cudaFree(t->scratch);
-        t->scratch = nullptr;
-        t->scratch_bytes = 0;
-        WC_CUDA(cudaMalloc(&t->scratch, need));
-        t->scratch_bytes = need;
-    }
-    auto *e = reinterpret_cast<unsigned long long *>(end);
-    auto *b = reinterpret_cast<unsigned long long *>(begin);
-    auto *ts = reinterpret_cast<unsigned long long *>(t->scratch);
-    uint64_t nn = n, nt = ntiles;
-    void *a1[] = {&e, &nn, &ts};
-    WC_CUDA(cudaLaunchKernel(k.tile_sums, dim3(unsigned(ntiles)), dim3(kScanThreads), a1, 0, s));
-    void *a2[] = {&ts, &nt};
-    WC_CUDA(cudaLaunchKernel(k.tile_offsets, dim3(1), dim3(kScanThreads), a2, 0, s));
-    /* end == begin + 1: the scan writes end only, begin[0] is zero */
-    int write_begin = e == b + 1 ? 0 : 1;
-    if (!write_begin) WC_CUDA(cudaMemsetAsync(b, 0, sizeof(unsigned long long), s));
-    void *a3[] = {&e, &b, &nn, &ts, &write_begin};
-    WC_CUDA(cudaLaunchKernel(k.apply, dim3(unsigned(ntiles)), dim3(kScanThreads), a3, 0, s));
-    note_launches(3);
-    return WC_OK;
+    return host_offsets_scan(&t->scratch, &t->scratch_bytes, begin, end, n, s);
 }
 
 int mv_join(wc_table *t, uint32_t bits, cudaStream_t s)
 {
-    uint32_t cur = 0;
-    WC_CUDA(cudaMemcpyAsync(&cur, t->status, sizeof(cur), cudaMemcpyDeviceToHost, s));
-    WC_CUDA(cudaStreamSynchronize(s));
-    cur |= bits;
-    WC_CUDA(cudaMemcpyAsync(t->status, &cur, sizeof(cur), cudaMemcpyHostToDevice, s));
-    WC_CUDA(cudaStreamSynchronize(s));
-    return WC_OK;
+    return host_join_status(t->status, bits, s);
 }
 
 } // namespace
@@ -1062,16 +1103,8 @@ int wc_mvht_retrieve(wc_table *t, const void *keys_in, uint64_t num_in,
     if (rc) return rc;
     if (!values_out) {
         /* dry run: per-key counts, status dry_run for every key */
-        if (status_out && status_handler != WC_HANDLER_NOTHING) {
-            const MvScanKernels k = mv_scan_kernels();
-            uint64_t nn = num_in;
-            int h = status_handler;
-            uint32_t mask = (~ignore) ^ 0xFFFu;
-            void *args[] = {&status_out, &nn, &h, &mask};
-            WC_CUDA(cudaLaunchKernel(k.dry_status, dim3(grid_for(k.dry_status, kBlock, num_in, kBlock)),
-                                     dim3(kBlock), args, 0, s));
-            note_launches(1);
-        }
+        rc = host_dry_run_status(status_out, num_in, status_handler, ignore, s);
+        if (rc) return rc;
         return mv_join(t, kStDryRun, s);
     }
     /* pass 2: offsets; pass 3: values, each key at its begin offset */

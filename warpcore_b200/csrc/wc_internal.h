@@ -59,6 +59,14 @@ int host_fail(int code, const char *msg);
 int host_cuda_fail(cudaError_t e, const char *what);
 unsigned host_grid(const void *kernel, int block, uint64_t items, uint64_t per_block);
 uint64_t host_valid_capacity(uint64_t min_capacity, uint64_t cg);
+/* the multi-value tables' shared host steps: per-key counts (in end) to
+ * begin / end offsets, a host-side Status join, a dry run's statuses, one
+ * device counter read back */
+int host_offsets_scan(void **scratch, uint64_t *scratch_bytes, uint64_t *begin, uint64_t *end,
+                      uint64_t n, cudaStream_t s);
+int host_join_status(uint32_t *status, uint32_t bits, cudaStream_t s);
+int host_dry_run_status(void *status_out, uint64_t n, int handler, uint32_t ignore, cudaStream_t s);
+int host_read_counter(const unsigned long long *d, cudaStream_t s, uint64_t *out);
 
 /* kernels this library launched (wc_launch_count) */
 void note_launches(uint32_t n);

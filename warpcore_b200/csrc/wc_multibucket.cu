@@ -306,11 +306,7 @@ int launch(const void *k, uint64_t items, MbArgs &a, cudaStream_t s)
 
 int read_counter(const unsigned long long *d, cudaStream_t s, uint64_t *out)
 {
-    unsigned long long h = 0;
-    MB_CUDA(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, s));
-    MB_CUDA(cudaStreamSynchronize(s));
-    *out = h;
-    return WC_OK;
+    return host_read_counter(d, s, out);
 }
 
 /* per-key counts (and their sum, read back) */
@@ -330,44 +326,13 @@ int count(wc_mbht *t, const void *keys, uint64_t n, uint64_t *counts_dev, uint64
 /* counts in end -> end = inclusive prefix sums, begin = exclusive ones */
 int scan(wc_mbht *t, uint64_t *begin, uint64_t *end, uint64_t n, cudaStream_t s)
 {
-    const MvScanKernels k = mv_scan_kernels();
-    const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
-    const uint64_t need = ntiles * sizeof(unsigned long long);
-    if (need > t->scan_bytes) {
-        MB_CUDA(cudaStreamSynchronize(s));
-        if (t->scan) cudaFree(t->scan);
-        t->scan = nullptr;
-        t->scan_bytes = 0;
-        MB_CUDA(cudaMalloc(&t->scan, need));
-        t->scan_bytes = need;
-    }
-    auto *e = reinterpret_cast<unsigned long long *>(end);
-    auto *b = reinterpret_cast<unsigned long long *>(begin);
-    auto *ts = reinterpret_cast<unsigned long long *>(t->scan);
-    uint64_t nn = n, nt = ntiles;
-    void *a1[] = {&e, &nn, &ts};
-    MB_CUDA(cudaLaunchKernel(k.tile_sums, dim3(unsigned(ntiles)), dim3(kScanThreads), a1, 0, s));
-    void *a2[] = {&ts, &nt};
-    MB_CUDA(cudaLaunchKernel(k.tile_offsets, dim3(1), dim3(kScanThreads), a2, 0, s));
-    /* end == begin + 1: the scan writes end only, begin[0] is zero */
-    int write_begin = e == b + 1 ? 0 : 1;
-    if (!write_begin) MB_CUDA(cudaMemsetAsync(b, 0, sizeof(unsigned long long), s));
-    void *a3[] = {&e, &b, &nn, &ts, &write_begin};
-    MB_CUDA(cudaLaunchKernel(k.apply, dim3(unsigned(ntiles)), dim3(kScanThreads), a3, 0, s));
-    note_launches(3);
-    return WC_OK;
+    return host_offsets_scan(&t->scan, &t->scan_bytes, begin, end, n, s);
 }
 
 /* host join of status bits into the table's Status word */
 int join_host(wc_mbht *t, uint32_t bits, cudaStream_t s)
 {
-    uint32_t cur = 0;
-    MB_CUDA(cudaMemcpyAsync(&cur, t->status, sizeof(cur), cudaMemcpyDeviceToHost, s));
-    MB_CUDA(cudaStreamSynchronize(s));
-    cur |= bits;
-    MB_CUDA(cudaMemcpyAsync(t->status, &cur, sizeof(cur), cudaMemcpyHostToDevice, s));
-    MB_CUDA(cudaStreamSynchronize(s));
-    return WC_OK;
+    return host_join_status(t->status, bits, s);
 }
 
 /* fill `bytes` (a multiple of 4) with a repeated 4- or 8-byte word */
@@ -527,16 +492,8 @@ int wc_mbht_retrieve(wc_mbht *t, const void *keys_in, uint64_t num_in,
     if (rc) return rc;
     if (!values_out) {
         /* dry run: per-key counts, status dry_run for every key */
-        if (status_out && status_handler != WC_HANDLER_NOTHING) {
-            const MvScanKernels k = mv_scan_kernels();
-            uint64_t nn = num_in;
-            int h = status_handler;
-            uint32_t mask = (~ignore) ^ 0xFFFu;
-            void *args[] = {&status_out, &nn, &h, &mask};
-            MB_CUDA(cudaLaunchKernel(k.dry_status, dim3(host_grid(k.dry_status, kBlock, num_in, kBlock)),
-                                     dim3(kBlock), args, 0, s));
-            note_launches(1);
-        }
+        rc = host_dry_run_status(status_out, num_in, status_handler, ignore, s);
+        if (rc) return rc;
         return join_host(t, kStDryRun, s);
     }
     /* pass 2: offsets; pass 3: values at each key's begin offset */
