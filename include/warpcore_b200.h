@@ -451,7 +451,8 @@ typedef struct wc_bloom_config {
 typedef struct wc_bloom_info {
     uint32_t key_bytes, slot_bytes, cg_size, hasher;
     uint64_t num_bits, num_slots, num_blocks, k, seed;
-    void *words; /* device pointer to the bit vector */
+    void *words; /* device pointer to the bit vector (this filter's blocks) */
+    uint64_t block_base, local_blocks; /* the blocks held: all, or a shard's */
 } wc_bloom_info;
 
 typedef struct wc_bloom wc_bloom;
@@ -461,6 +462,21 @@ int wc_bloom_create(const wc_bloom_config *cfg, uint64_t num_bits, uint64_t k,
                     uint64_t seed, wc_bloom **out);
 /* ~BloomFilter (bloom_filter.cuh:130-138) */
 int wc_bloom_destroy(wc_bloom *b);
+/* Sharded form (no counterpart in the reference, which is single-GPU):
+ * shard `shard` of `num_shards` holds the blocks b of the whole filter
+ * (num_bits, k, seed) with b * num_shards / num_blocks == shard, so each
+ * block, and every bit a key sets, lives on one shard, and the shards'
+ * words are the whole filter's words cut in block ranges.  Blocks of at most
+ * 128 bytes and num_bits a multiple of the block bits.  A shard skips keys
+ * of blocks it does not hold (query: absent).  wc_bloom_partition groups
+ * keys by the shard that holds their block (counts_out: num_parts entries;
+ * scratch: 2 * num_parts + 1 entries; perm_out: input position of each
+ * output key), for the exchange step of a multi-GPU filter. */
+int wc_bloom_create_shard(const wc_bloom_config *cfg, uint64_t num_bits, uint64_t k,
+                          uint64_t seed, uint32_t shard, uint32_t num_shards, wc_bloom **out);
+int wc_bloom_partition(const wc_bloom *b, const void *keys, uint64_t n, uint32_t num_parts,
+                       void *keys_out, uint64_t *perm_out, uint64_t *counts_out,
+                       uint64_t *scratch, wc_stream_t stream);
 /* init(seed, stream) (bloom_filter.cuh:143-152) */
 int wc_bloom_init(wc_bloom *b, uint64_t seed, wc_stream_t stream);
 /* insert(keys_in, num_in, stream) (bloom_filter.cuh:200-208) */
@@ -682,9 +698,10 @@ int wc_partition(const void *keys, const void *values, uint64_t n, uint32_t key_
                  uint64_t *scratch, wc_stream_t stream);
 /* The inverse step of a sharded retrieve: answer j, in the order
  * wc_partition produced, goes back to input position perm[j].  Its value is
- * written only if status[j] is 0 (a hit), as retrieve writes hits only; the
- * status is written if status_out is not NULL.  Entries whose perm[j] is
- * not below n are skipped.  Asynchronous on `stream`. */
+ * written only if status[j] is 0 (a hit), as retrieve writes hits only, or
+ * always if status is NULL (Bloom flags); the status is written if
+ * status_out is not NULL.  value_bytes 1 (flags), 4 or 8.  Entries whose
+ * perm[j] is not below n are skipped.  Asynchronous on `stream`. */
 int wc_partition_restore(const void *values, const uint32_t *status, const uint64_t *perm,
                          uint64_t n, uint32_t value_bytes, void *values_out,
                          uint32_t *status_out, wc_stream_t stream);

@@ -166,6 +166,8 @@ class BloomInfo(ctypes.Structure):
         ("k", ctypes.c_uint64),
         ("seed", ctypes.c_uint64),
         ("words", ctypes.c_void_p),
+        ("block_base", ctypes.c_uint64),
+        ("local_blocks", ctypes.c_uint64),
     ]
 
 
@@ -259,6 +261,8 @@ SIGNATURES = {
     "wc_counting_retrieve": (_i, [_vp, _vp, _u64, _vp, _vp, _u64, _vp, _i, _u32]),
     "wc_counting_erase": (_i, [_vp, _vp, _u64, _vp, _u64, _vp, _i, _u32]),
     "wc_bloom_create": (_i, [ctypes.POINTER(BloomConfig), _u64, _u64, _u64, _pp]),
+    "wc_bloom_create_shard": (_i, [ctypes.POINTER(BloomConfig), _u64, _u64, _u64, _u32, _u32, _pp]),
+    "wc_bloom_partition": (_i, [_vp, _vp, _u64, _u32, _vp, _vp, _vp, _vp, _vp]),
     "wc_bloom_destroy": (_i, [_vp]),
     "wc_bloom_init": (_i, [_vp, _u64, _vp]),
     "wc_bloom_insert": (_i, [_vp, _vp, _u64, _vp]),
@@ -1096,16 +1100,52 @@ class CountingHashTable(_Table):
 
 
 class BloomFilter:
-    """warpcore::BloomFilter<Key, Hasher, Slot, CGSize> (bloom_filter.cuh:15-20)."""
+    """warpcore::BloomFilter<Key, Hasher, Slot, CGSize> (bloom_filter.cuh:15-20).
+
+    With num_shards > 1, this object is shard `shard` of the filter
+    (num_bits, k, seed): it holds the blocks b with
+    b * num_shards // num_blocks == shard, skips the keys of other blocks on
+    insert and reports them absent on retrieve (wc_bloom_create_shard)."""
 
     def __init__(self, num_bits, k, seed=DEFAULT_SEED, key_bytes=8, slot_bytes=8,
-                 cg_size=1, hasher=HASH_MURMUR):
+                 cg_size=1, hasher=HASH_MURMUR, shard=0, num_shards=1):
         cfg = BloomConfig(key_bytes, slot_bytes, cg_size, hasher)
         h = ctypes.c_void_p()
-        _check(lib().wc_bloom_create(ctypes.byref(cfg), int(num_bits), int(k), int(seed),
-                                     ctypes.byref(h)))
+        if num_shards == 1 and shard == 0:
+            _check(lib().wc_bloom_create(ctypes.byref(cfg), int(num_bits), int(k), int(seed),
+                                         ctypes.byref(h)))
+        else:
+            _check(lib().wc_bloom_create_shard(ctypes.byref(cfg), int(num_bits), int(k),
+                                               int(seed), int(shard), int(num_shards),
+                                               ctypes.byref(h)))
         self._h = h
         self._cfg = cfg
+        self.num_shards = int(num_shards)
+
+    def block_range(self):
+        """(first block, number of blocks) this object holds"""
+        inf = self.info()
+        return inf.block_base, inf.local_blocks
+
+    def partition(self, keys_in, num_parts=None, stream=None):
+        """group keys by the shard holding their block: returns (keys_out,
+        perm, counts as a list of ints), perm[j] = input position of
+        keys_out[j] (wc_bloom_partition)"""
+        import torch
+        _check_width(keys_in, self._cfg.key_bytes, "keys_in")
+        parts = self.num_shards if num_parts is None else int(num_parts)
+        n = keys_in.numel()
+        keys_out = torch.empty_like(keys_in)
+        perm = torch.empty(n, dtype=torch.int64, device=keys_in.device)
+        buf = torch.zeros(3 * parts + 1, dtype=torch.int64, device=keys_in.device)
+        _check(lib().wc_bloom_partition(self._h, _ptr(keys_in) if n else None, n, parts,
+                                        _ptr(keys_out) if n else None, _ptr(perm) if n else None,
+                                        buf.data_ptr(), buf[parts:].data_ptr(), _stream(stream)))
+        host_buf = buf.tolist()
+        if host_buf[-1]:
+            raise WarpcoreError("wc_bloom_partition dropped %d keys whose position failed the "
+                                "bounds check (keys changed during the call)" % host_buf[-1])
+        return keys_out, perm, host_buf[:parts]
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -31,6 +31,12 @@ struct BloomArgs {
     uint64_t k;
     uint64_t seed;
     uint32_t hasher;
+    /* a shard holds the blocks [block_base, block_base + local_blocks) of a
+     * filter of num_blocks blocks (a whole filter: 0 and num_blocks); its
+     * words start at block_base, and a key whose block it does not hold is
+     * skipped (insert) or reported absent (query) */
+    uint64_t block_base;
+    uint64_t local_blocks;
 };
 
 template <class S>
@@ -205,7 +211,12 @@ __global__ void __launch_bounds__(256) bloom_lane_kernel(const BloomArgs a)
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.n; i += stride) {
         const K key = ld_stream(keys + i);
         const uint64_t blk =
-            fast_mod(hash_key<K>(a.hasher, K(key + seed)), a.num_blocks, a.magic_blocks);
+            fast_mod(hash_key<K>(a.hasher, K(key + seed)), a.num_blocks, a.magic_blocks) -
+            a.block_base;
+        if (blk >= a.local_blocks) {
+            if constexpr (!INSERT) a.flags_out[i] = 0;
+            continue;
+        }
         S m[CG];
         block_masks<K, S, CG>(key, seed, a.hasher, a.k, m);
         const uint64_t w0 = blk * CG;

@@ -450,6 +450,7 @@ struct wc_table {
 struct wc_bloom {
     wc_bloom_config cfg{};
     uint64_t num_bits = 0, num_slots = 0, num_blocks = 0, k = 0, seed = 0;
+    uint64_t block_base = 0, local_blocks = 0; /* the blocks this filter holds */
     void *words = nullptr;
     int device = 0;
     L2Window l2;
@@ -1228,8 +1229,10 @@ int wc_tune_reset(void)
 
 /* ---- Bloom filter ---- */
 
-int wc_bloom_create(const wc_bloom_config *cfg, uint64_t num_bits, uint64_t k, uint64_t seed,
-                    wc_bloom **out)
+/* shape of the whole filter, and the blocks [lo, hi) that this object holds
+ * (shard s of S holds the blocks b with b * S / num_blocks == s) */
+static int bloom_new(const wc_bloom_config *cfg, uint64_t num_bits, uint64_t k, uint64_t seed,
+                     uint32_t shard, uint32_t num_shards, wc_bloom **out)
 {
     if (!out || !cfg) return fail(WC_ERR_INVALID_ARGUMENT, "NULL argument");
     *out = nullptr;
@@ -1240,17 +1243,31 @@ int wc_bloom_create(const wc_bloom_config *cfg, uint64_t num_bits, uint64_t k, u
     if (!valid_cg(cfg->cg_size)) return fail(WC_ERR_INVALID_ARGUMENT, "bad cg_size");
     if (cfg->hasher > WC_HASH_IDENTITY64) return fail(WC_ERR_INVALID_ARGUMENT, "unknown hasher");
     if (num_bits == 0) return fail(WC_ERR_INVALID_ARGUMENT, "num_bits must be positive");
+    if (num_shards == 0 || shard >= num_shards)
+        return fail(WC_ERR_INVALID_ARGUMENT, "shard %u of %u", shard, num_shards);
+    const uint64_t slot_bits = uint64_t(cfg->slot_bytes) * 8;
+    const uint64_t num_slots = (num_bits + slot_bits - 1) / slot_bits;
+    if (num_shards > 1) {
+        if (cfg->cg_size * cfg->slot_bytes > 128)
+            return fail(WC_ERR_UNSUPPORTED, "sharded filters take blocks of at most 128 bytes");
+        if (num_slots % cfg->cg_size)
+            return fail(WC_ERR_UNSUPPORTED,
+                        "sharded filters take whole blocks (num_bits a multiple of the block bits)");
+    }
     auto *b = new wc_bloom();
     b->cfg = *cfg;
     b->num_bits = num_bits;
-    const uint64_t slot_bits = uint64_t(cfg->slot_bytes) * 8;
-    b->num_slots = (num_bits + slot_bits - 1) / slot_bits;
-    b->num_blocks = (b->num_slots + cfg->cg_size - 1) / cfg->cg_size;
+    b->num_slots = num_slots;
+    b->num_blocks = (num_slots + cfg->cg_size - 1) / cfg->cg_size;
     b->k = k;
     b->seed = seed & key_mask(cfg->key_bytes);
+    const uint64_t nb = b->num_blocks, S = num_shards;
+    b->block_base = (uint64_t(shard) * nb + S - 1) / S;
+    b->local_blocks = ((uint64_t(shard) + 1) * nb + S - 1) / S - b->block_base;
     cudaGetDevice(&b->device);
     /* padded to whole blocks so that full-block vector loads stay inside */
-    const uint64_t bytes = b->num_blocks * cfg->cg_size * cfg->slot_bytes;
+    const uint64_t bytes =
+        (b->local_blocks ? b->local_blocks : 1) * cfg->cg_size * cfg->slot_bytes;
     cudaError_t e = cudaMalloc(&b->words, bytes);
     if (e != cudaSuccess) {
         delete b;
@@ -1264,6 +1281,27 @@ int wc_bloom_create(const wc_bloom_config *cfg, uint64_t num_bits, uint64_t k, u
     }
     *out = b;
     return WC_OK;
+}
+
+int wc_bloom_create(const wc_bloom_config *cfg, uint64_t num_bits, uint64_t k, uint64_t seed,
+                    wc_bloom **out)
+{
+    return bloom_new(cfg, num_bits, k, seed, 0, 1, out);
+}
+
+int wc_bloom_create_shard(const wc_bloom_config *cfg, uint64_t num_bits, uint64_t k,
+                          uint64_t seed, uint32_t shard, uint32_t num_shards, wc_bloom **out)
+{
+    return bloom_new(cfg, num_bits, k, seed, shard, num_shards, out);
+}
+
+int wc_bloom_partition(const wc_bloom *b, const void *keys, uint64_t n, uint32_t num_parts,
+                       void *keys_out, uint64_t *perm_out, uint64_t *counts_out,
+                       uint64_t *scratch, wc_stream_t stream)
+{
+    if (!b) return fail(WC_ERR_INVALID_ARGUMENT, "filter is NULL");
+    return partition_by_bloom_block(keys, n, b->cfg.key_bytes, num_parts, b->seed, b->cfg.hasher,
+                                    b->num_blocks, keys_out, perm_out, counts_out, scratch, stream);
 }
 
 int wc_bloom_destroy(wc_bloom *b)
@@ -1280,7 +1318,7 @@ int wc_bloom_init(wc_bloom *b, uint64_t seed, wc_stream_t stream)
     if (!b) return fail(WC_ERR_INVALID_ARGUMENT, "filter is NULL");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     b->seed = seed & key_mask(b->cfg.key_bytes);
-    const uint64_t bytes = b->num_blocks * b->cfg.cg_size * b->cfg.slot_bytes;
+    const uint64_t bytes = b->local_blocks * b->cfg.cg_size * b->cfg.slot_bytes;
     WC_CUDA(cudaMemsetAsync(b->words, 0, bytes, s));
     WC_CUDA(cudaStreamSynchronize(s));
     return WC_OK;
@@ -1307,6 +1345,8 @@ static int bloom_op(wc_bloom *b, const void *keys, uint64_t n, uint8_t *flags, w
     a.k = b->k;
     a.seed = b->seed;
     a.hasher = b->cfg.hasher;
+    a.block_base = b->block_base;
+    a.local_blocks = b->local_blocks;
     const unsigned grid = grid_for(reinterpret_cast<const void *>(k), kBlock, n, kBlock);
     void *args[] = {&a};
     WC_CUDA(launch_in_window(reinterpret_cast<const void *>(k), grid, kBlock, args,
@@ -1335,6 +1375,8 @@ int wc_bloom_get_info(const wc_bloom *b, wc_bloom_info *info)
     info->num_bits = b->num_bits;
     info->num_slots = b->num_slots;
     info->num_blocks = b->num_blocks;
+    info->block_base = b->block_base;
+    info->local_blocks = b->local_blocks;
     info->k = b->k;
     info->seed = b->seed;
     info->words = b->words;

@@ -5,6 +5,8 @@
 #ifndef WC_INTERNAL_H
 #define WC_INTERNAL_H
 
+#include <warpcore_b200.h>
+
 #include "wc_bloom.cuh"
 #include "wc_batch.cuh"
 #include "wc_fp_kernels.cuh"
@@ -67,6 +69,13 @@ int host_offsets_scan(void **scratch, uint64_t *scratch_bytes, uint64_t *begin, 
 int host_join_status(uint32_t *status, uint32_t bits, cudaStream_t s);
 int host_dry_run_status(void *status_out, uint64_t n, int handler, uint32_t ignore, cudaStream_t s);
 int host_read_counter(const unsigned long long *d, cudaStream_t s, uint64_t *out);
+
+/* wc_partition's passes with the owner of a key = the shard holding its
+ * block of a Bloom filter of num_blocks blocks (wc_partition.cu) */
+int partition_by_bloom_block(const void *keys, uint64_t n, uint32_t key_bytes, uint32_t num_parts,
+                             uint64_t seed, uint32_t hasher, uint64_t num_blocks, void *keys_out,
+                             uint64_t *perm_out, uint64_t *counts_out, uint64_t *scratch,
+                             wc_stream_t stream);
 
 /* kernels this library launched (wc_launch_count) */
 void note_launches(uint32_t n);
