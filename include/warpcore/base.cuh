@@ -12,6 +12,7 @@
 #define WARPCORE_B200_CXX_BASE_CUH
 
 #include <cstdint>
+#include <cstring>
 #include <limits>
 #include <ostream>
 #include <string>
@@ -62,6 +63,19 @@ template <class T>
 __host__ __device__ constexpr bool is_valid_key_type() noexcept
 {
     return std::is_same<T, std::uint32_t>::value || std::is_same<T, std::uint64_t>::value;
+}
+/* checks.cuh:46-61: values are any trivially copyable type (this build
+ * stores 4- or 8-byte ones); counters are int, u32 or u64 */
+template <class T>
+__host__ __device__ constexpr bool is_valid_value_type() noexcept
+{
+    return std::is_trivially_copyable<T>::value;
+}
+template <class T>
+__host__ __device__ constexpr bool is_valid_counter_type() noexcept
+{
+    return std::is_same<T, int>::value || std::is_same<T, std::uint32_t>::value ||
+           std::is_same<T, std::uint64_t>::value;
 }
 template <class T>
 __host__ __device__ constexpr bool is_hasher() noexcept
@@ -393,6 +407,10 @@ template <>
 struct layout_of<std::uint32_t, std::uint32_t> { using type = b200::LayoutKV32; };
 template <>
 struct layout_of<std::uint64_t, std::uint64_t> { using type = b200::LayoutKV64; };
+template <>
+struct layout_of<std::uint32_t, std::uint64_t> { using type = b200::LayoutK32V64; };
+template <>
+struct layout_of<std::uint64_t, std::uint32_t> { using type = b200::LayoutK64V32; };
 template <>
 struct layout_of<std::uint32_t, void> { using type = b200::LayoutSet32; };
 template <>

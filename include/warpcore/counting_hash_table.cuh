@@ -18,8 +18,8 @@ template <class Key, class Value = index_t, Key EmptyKey = defaults::empty_key<K
           index_t TempMemoryBytes = defaults::temp_memory_bytes()>
 class CountingHashTable {
     static_assert(checks::is_valid_key_type<Key>(), "invalid key type");
-    static_assert(sizeof(Value) == sizeof(Key) && std::is_integral<Value>::value,
-                  "this build stores counts as wide as the key (u32/u32, u64/u64)");
+    static_assert(checks::is_valid_counter_type<Value>(),
+                  "counts are int, std::uint32_t or std::uint64_t");
     using layout = typename detail::layout_of<Key, typename std::make_unsigned<Value>::type>::type;
 
   public:

@@ -257,6 +257,21 @@ struct LayoutKV64 {
     static constexpr int kSlotBytes = 16;
     static constexpr bool kHasValue = true;
 };
+/* mixed widths, one 16-byte word each: the key in bytes 0..7 and the value
+ * in bytes 8..15, the narrower field zero-extended (its upper half stays 0
+ * in every state, so the 128-bit compare-and-swap sees whole words) */
+struct LayoutK32V64 {
+    using key_t = uint32_t;
+    using val_t = uint64_t;
+    static constexpr int kSlotBytes = 16;
+    static constexpr bool kHasValue = true;
+};
+struct LayoutK64V32 {
+    using key_t = uint64_t;
+    using val_t = uint32_t;
+    static constexpr int kSlotBytes = 16;
+    static constexpr bool kHasValue = true;
+};
 /* hash set of u32 / u64 keys */
 struct LayoutSet32 {
     using key_t = uint32_t;

@@ -30,10 +30,13 @@ class SingleValueHashTable {
     static_assert(checks::is_probing_scheme<ProbingScheme>(), "not a valid probing scheme type");
     static_assert(std::is_same<typename ProbingScheme::key_type, Key>::value,
                   "probing key type differs from table's key type");
-    static_assert(sizeof(Value) == sizeof(Key) && std::is_integral<Value>::value,
-                  "this build stores integral values as wide as the key (u32/u32, u64/u64)");
+    static_assert((sizeof(Value) == 4 || sizeof(Value) == 8) &&
+                      std::is_trivially_copyable<Value>::value,
+                  "this build stores trivially copyable values of 4 or 8 bytes");
 
-    using layout = typename detail::layout_of<Key, typename std::make_unsigned<Value>::type>::type;
+    /* the value's bits, held in the slot as an unsigned word of its width */
+    using value_word = typename std::conditional<sizeof(Value) == 4, std::uint32_t, std::uint64_t>::type;
+    using layout = typename detail::layout_of<Key, value_word>::type;
 
   public:
     using key_type = Key;
@@ -117,7 +120,7 @@ class SingleValueHashTable {
         bool found = false;
         const status_type s(b200::tile_find<layout>(view_, group, key_in, v, found, false,
                                                     probing_length));
-        if (found) value_out = value_type(v);
+        if (found) value_out = value_of(v);
         return s;
     }
 
@@ -235,9 +238,17 @@ class SingleValueHashTable {
     friend __global__ void detail::svht_for_each_kernel(F, const Table);
 
     static wc_stream_t stream_of(cudaStream_t s) { return reinterpret_cast<wc_stream_t>(s); }
-    __host__ __device__ static typename layout::val_t value_bits(const value_type &v)
+    __host__ __device__ static value_word value_bits(const value_type &v)
     {
-        return typename layout::val_t(v);
+        value_word w;
+        memcpy(&w, &v, sizeof(w));
+        return w;
+    }
+    __host__ __device__ static value_type value_of(const value_word w)
+    {
+        value_type v;
+        memcpy(&v, &w, sizeof(v));
+        return v;
     }
     void refresh() noexcept
     {
@@ -260,13 +271,13 @@ template <class F, class Table>
 __global__ void svht_for_each_kernel(F f, const Table table)
 {
     using K = typename Table::key_type;
-    using V = typename Table::value_type;
+    using L = typename Table::layout;
     const index_t tid = index_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (tid >= table.capacity()) return;
     const b200::TableView &t = table.device_view();
-    const K *sp = reinterpret_cast<const K *>(t.slots) + 2 * tid;
-    const K key = sp[0];
-    if (Table::is_valid_key(key)) f(key, V(sp[1]));
+    unsigned char *const sp = reinterpret_cast<unsigned char *>(t.slots) + tid * L::kSlotBytes;
+    const K key = *reinterpret_cast<const K *>(sp);
+    if (Table::is_valid_key(key)) f(key, Table::value_of(*b200::slot_value_ptr<L>(sp)));
 }
 } // namespace detail
 

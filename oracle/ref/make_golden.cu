@@ -405,10 +405,11 @@ static void set_case(const char *tag, uint64_t n, uint64_t min_cap, uint64_t kse
     cudaFree(dk); cudaFree(dk2); cudaFree(dq); cudaFree(de); cudaFree(dflags); cudaFree(dst);
 }
 
+template <class V>
 static void counting_case(const char *tag, uint64_t distinct, uint64_t occ,
-                          uint64_t min_cap, uint32_t max_count, uint64_t kseed)
+                          uint64_t min_cap, V max_count, uint64_t kseed)
 {
-    using Table = wc::CountingHashTable<uint32_t, uint32_t>;
+    using Table = wc::CountingHashTable<uint32_t, V>;
     using SH = wc::status_handlers::ReturnStatus;
     const std::string p = tag;
     std::vector<uint32_t> all = unique_keys<uint32_t>(distinct + distinct / 4, kseed);
@@ -420,8 +421,8 @@ static void counting_case(const char *tag, uint64_t distinct, uint64_t occ,
 
     Table t(min_cap, wc::defaults::seed<uint32_t>(), max_count);
     uint32_t *dk = to_dev(keys), *dq = to_dev(q);
-    std::vector<uint32_t> fill(q.size(), 0xA5A5A5A5u);
-    uint32_t *dout = to_dev(fill);
+    std::vector<V> fill(q.size(), V(0xA5A5A5A5A5A5A5A5ull));
+    V *dout = to_dev(fill);
     uint32_t *dst;
     CK(cudaMalloc(&dst, sizeof(uint32_t) * q.size()));
     t.insert(dk, keys.size());
@@ -808,8 +809,12 @@ static void run_gpu()
     svht_case<uint64_t, uint64_t>("svht_u64u64", 20000, 25000, 21);
     set_case<uint64_t>("set_u64", 20000, 25000, 31);
     set_case<uint32_t>("set_u32", 20000, 25000, 41);
-    counting_case("count_u32", 5000, 200000, 6000, 0xffffffffu, 51);
-    counting_case("count_u32_max10", 5000, 200000, 6000, 10u, 52);
+    counting_case<uint32_t>("count_u32", 5000, 200000, 6000, 0xffffffffu, 51);
+    counting_case<uint32_t>("count_u32_max10", 5000, 200000, 6000, 10u, 52);
+    counting_case<uint64_t>("count_u32u64", 5000, 200000, 6000, ~uint64_t(0), 53);
+    counting_case<uint64_t>("count_u32u64_max10", 5000, 200000, 6000, uint64_t(10), 54);
+    svht_case<uint32_t, uint64_t>("svht_u32u64", 20000, 25000, 12);
+    svht_case<uint64_t, uint32_t>("svht_u64u32", 20000, 25000, 22);
     bloom_case<uint64_t, uint64_t, 8>("bloom_u64_s64_cg8", 1ull << 16, 8, 4000, 61);
     bloom_case<uint64_t, uint64_t, 1>("bloom_u64_s64_cg1", (1ull << 16) + 100, 6, 3000, 62);
     bloom_case<uint32_t, uint32_t, 4>("bloom_u32_s32_cg4", 3000, 5, 300, 63);

@@ -302,6 +302,142 @@ static void test_bloom()
     cudaFree(dk); cudaFree(dflag);
 }
 
+/* The reference's filtered-histogram example (examples/src/
+ * advanced_usage_from_device.cu), in this test's words: a CG-1 Bloom
+ * filter's insert_and_query tells whether a key was seen before, and the
+ * keys seen before are counted in a CountingHashTable<u32, u64>, one key at
+ * a time by the counting table's tile. */
+template <class Filter, class Counter>
+__global__ void filtered_histogram(const uint32_t *keys, uint64_t n, Filter f, Counter c)
+{
+    const auto fg = cg::tiled_partition<1>(cg::this_thread_block());
+    const auto tg = cg::tiled_partition<Counter::cg_size()>(cg::this_thread_block());
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    uint32_t key = 0;
+    bool seen = false;
+    if (i < n) {
+        key = keys[i];
+        seen = f.insert_and_query(key, fg);
+    }
+    unsigned todo = tg.ballot(seen);
+    while (todo) {
+        const int src = __ffs(todo) - 1;
+        c.insert(tg.shfl(key, src), tg);
+        todo &= todo - 1;
+    }
+}
+
+static void test_filtered_histogram()
+{
+    using Filter = wc::BloomFilter<uint32_t, wc::hashers::MuellerHash, uint32_t>;
+    using Counter = wc::CountingHashTable<uint32_t, uint64_t>;
+    const uint64_t n = 1 << 20, mult = 4;
+    std::vector<uint32_t> keys(n);
+    for (uint64_t i = 0; i < n / 2; ++i) keys[i] = uint32_t(i + 1); /* seen once */
+    for (uint64_t i = n / 2; i < n; i += mult)                      /* seen 4 times */
+        for (uint64_t j = 0; j < mult; ++j) keys[i + j] = uint32_t(i + 1);
+    std::shuffle(keys.begin(), keys.end(), std::mt19937(77));
+    Filter f(n * 16, 6, 420);
+    Counter c(n);
+    uint32_t *dk = dcopy(keys);
+    filtered_histogram<<<unsigned(n / 256), 256>>>(dk, n, f, c);
+    /* ask for every distinct key */
+    std::vector<uint32_t> q;
+    for (uint64_t i = 0; i < n / 2; ++i) q.push_back(uint32_t(i + 1));
+    for (uint64_t i = n / 2; i < n; i += mult) q.push_back(uint32_t(i + 1));
+    uint32_t *dq = dcopy(q);
+    uint64_t *dcnt;
+    cudaMalloc(&dcnt, sizeof(uint64_t) * q.size());
+    cudaMemset(dcnt, 0, sizeof(uint64_t) * q.size());
+    c.retrieve(dq, q.size(), dcnt);
+    auto cnt = hcopy(dcnt, q.size());
+    /* a repeated key is counted 3 times (its first occurrence is new to the
+     * filter), 4 if that first occurrence was a false positive; a unique key
+     * 0 times, or once after a false positive */
+    uint64_t odd_unique = 0, odd_repeat = 0, bad = 0;
+    for (uint64_t i = 0; i < n / 2; ++i) {
+        odd_unique += cnt[i] == 1;
+        bad += cnt[i] > 1;
+    }
+    for (uint64_t i = n / 2; i < q.size(); ++i) {
+        odd_repeat += cnt[i] == mult;
+        bad += cnt[i] != mult - 1 && cnt[i] != mult;
+    }
+    CHECK(bad == 0);
+    CHECK(odd_unique < n / 2 / 100);
+    CHECK(odd_repeat < (n / 2 / mult) / 100);
+    /* the table holds exactly the repeated keys and the false positives */
+    CHECK(c.size() == (n / 2) / mult + odd_unique);
+    cudaFree(dk); cudaFree(dq); cudaFree(dcnt);
+}
+
+/* values of other widths than the key, and non-integral values */
+static void test_mixed_widths()
+{
+    {
+        using Table = wc::SingleValueHashTable<uint32_t, uint64_t>;
+        const uint64_t n = 20000;
+        auto keys = distinct_keys<uint32_t>(2 * n, 8);
+        std::vector<uint64_t> vals(n);
+        for (uint64_t i = 0; i < n; ++i) vals[i] = (uint64_t(keys[i]) << 32) | (i * 7 + 1);
+        Table t(2 * n);
+        uint32_t *dk = dcopy(keys);
+        uint64_t *dv = dcopy(vals), *dout;
+        cudaMalloc(&dout, sizeof(uint64_t) * 2 * n);
+        cudaMemset(dout, 0xff, sizeof(uint64_t) * 2 * n);
+        t.insert(dk, dv, n);
+        CHECK(t.size() == n);
+        t.retrieve(dk, 2 * n, dout);
+        auto out = hcopy(dout, 2 * n);
+        for (uint64_t i = 0; i < n; ++i) CHECK(out[i] == vals[i]);
+        for (uint64_t i = n; i < 2 * n; ++i) CHECK(out[i] == ~0ull); /* misses untouched */
+        /* device retrieve through the tile API */
+        wc::Status *dst;
+        cudaMalloc(&dst, sizeof(wc::Status) * n);
+        cudaMemset(dout, 0, sizeof(uint64_t) * n);
+        device_retrieve<<<blocks_for(n, Table::cg_size()), 256>>>(t, dk, n, dout, dst);
+        out = hcopy(dout, n);
+        for (uint64_t i = 0; i < n; ++i) CHECK(out[i] == vals[i]);
+        /* for_each sees every pair */
+        unsigned long long *dsum;
+        cudaMalloc(&dsum, sizeof(unsigned long long));
+        cudaMemset(dsum, 0, sizeof(unsigned long long));
+        t.for_each([=] __device__(uint32_t k, uint64_t v) {
+            if ((v >> 32) == k) atomicAdd(dsum, 1ull);
+        });
+        CHECK(hcopy(dsum, 1)[0] == n);
+        cudaFree(dk); cudaFree(dv); cudaFree(dout); cudaFree(dst); cudaFree(dsum);
+    }
+    {
+        using Table = wc::SingleValueHashTable<uint64_t, float>;
+        const uint64_t n = 10000;
+        auto keys = distinct_keys<uint64_t>(n, 9);
+        std::vector<float> vals(n);
+        for (uint64_t i = 0; i < n; ++i) vals[i] = 0.5f * float(i) - 17.25f;
+        Table t(2 * n);
+        uint64_t *dk = dcopy(keys);
+        float *dv = dcopy(vals), *dout;
+        cudaMalloc(&dout, sizeof(float) * n);
+        t.insert(dk, dv, n);
+        t.retrieve(dk, n, dout);
+        auto out = hcopy(dout, n);
+        CHECK(out == vals);
+        uint64_t *dak;
+        float *dav;
+        cudaMalloc(&dak, sizeof(uint64_t) * n);
+        cudaMalloc(&dav, sizeof(float) * n);
+        wc::index_t num = 0;
+        t.retrieve_all(dak, dav, num);
+        CHECK(num == n);
+        auto ak = hcopy(dak, n);
+        auto av = hcopy(dav, n);
+        std::unordered_map<uint64_t, float> m;
+        for (uint64_t i = 0; i < n; ++i) m[keys[i]] = vals[i];
+        for (uint64_t i = 0; i < n; ++i) CHECK(m.count(ak[i]) && m[ak[i]] == av[i]);
+        cudaFree(dk); cudaFree(dv); cudaFree(dout); cudaFree(dak); cudaFree(dav);
+    }
+}
+
 /* device per-key MultiValueHashTable methods: each group inserts one pair,
  * then counts a key's values and reads them */
 template <class Table>
@@ -637,6 +773,8 @@ int main()
     test_hash_set();
     test_counting();
     test_bloom();
+    test_filtered_histogram();
+    test_mixed_widths();
     test_multi_value();
     test_multi_bucket();
     test_bucket_list();

@@ -13,22 +13,24 @@ def _dt(kb):
     return np.uint32 if kb == 4 else np.uint64
 
 
-def svht_scenario(F, tag, kb, make_table):
+def svht_scenario(F, tag, kb, make_table, vb=None):
     """make_table(min_cap) -> object with insert/retrieve/erase/size/
-    pop_status like oracle.Table"""
+    pop_status like oracle.Table; vb = value width (default: kb)"""
+    vb = kb if vb is None else vb
     n, min_cap, kseed, cap, size1, size2, size3, s1, s2, s3, s4, s5 = F[tag + "_meta"].tolist()
     allk = o.gen_unique_keys(kb, 2 * n, kseed)
     keys = allk[:n]
-    vals = o.gen_uniform(kb, n, kseed + 1)
+    vals = o.gen_uniform(vb, n, kseed + 1)
     nd = n // 8
     km = (1 << (8 * kb)) - 1
+    vm = (1 << (8 * vb)) - 1
     k2 = np.concatenate([keys[:nd], np.array([0, km], dtype=_dt(kb))])
-    v2 = np.concatenate([o.gen_uniform(kb, nd, kseed + 2), np.array([1, 2], dtype=_dt(kb))])
+    v2 = np.concatenate([o.gen_uniform(vb, nd, kseed + 2), np.array([1, 2], dtype=_dt(vb))])
     q = np.empty(2 * n, dtype=_dt(kb))
     q[0::2] = keys
     q[1::2] = allk[n:]
     er = np.concatenate([keys[::5], allk[n:n + 16]])
-    fill = np.full(2 * n, SENT64 & km, dtype=_dt(kb))
+    fill = np.full(2 * n, SENT64 & vm, dtype=_dt(vb))
 
     t = make_table(min_cap)
     assert t.capacity == cap
@@ -78,7 +80,8 @@ def set_scenario(F, tag, kb, make_set):
     assert s.pop_status() == s3
 
 
-def counting_scenario(F, tag, make_counter):
+def counting_scenario(F, tag, make_counter, vb=4):
+    """u32 keys, counts of vb bytes"""
     distinct, occ, min_cap, max_count, kseed, cap, size1, s1 = F[tag + "_meta"].tolist()
     allk = o.gen_unique_keys(4, distinct + distinct // 4, kseed)
     ranks = o.gen_zipf_ranks(distinct, 1.1, occ, kseed + 3)
@@ -87,7 +90,8 @@ def counting_scenario(F, tag, make_counter):
     assert c.capacity == cap
     c.insert(keys)
     assert c.pop_status() == s1
-    out, st = c.retrieve(allk, np.full(allk.size, 0xA5A5A5A5, dtype=np.uint32), want_status=True)
+    fill = np.full(allk.size, SENT64 & ((1 << (8 * vb)) - 1), dtype=_dt(vb))
+    out, st = c.retrieve(allk, fill, want_status=True)
     assert np.array_equal(out, F[tag + "_counts"])
     assert np.array_equal(st, F[tag + "_status"])
     assert c.size() == size1
@@ -103,9 +107,11 @@ def bloom_scenario(F, tag, make_bloom):
     assert np.array_equal(b.retrieve(allk), F[tag + "_flags"])
 
 
-SVHT_CASES = [("svht_u32u32", 4), ("svht_u64u64", 8)]
+SVHT_CASES = [("svht_u32u32", 4, 4), ("svht_u64u64", 8, 8), ("svht_u32u64", 4, 8),
+              ("svht_u64u32", 8, 4)]
 SET_CASES = [("set_u64", 8), ("set_u32", 4)]
-COUNT_CASES = ["count_u32", "count_u32_max10"]
+COUNT_CASES = [("count_u32", 4), ("count_u32_max10", 4), ("count_u32u64", 8),
+               ("count_u32u64_max10", 8)]
 BLOOM_CASES = ["bloom_u64_s64_cg8", "bloom_u64_s64_cg1", "bloom_u32_s32_cg4", "bloom_u32_s64_cg2"]
 
 

@@ -71,10 +71,10 @@ class BloomAdapter:
         return host(f)
 
 
-@pytest.mark.parametrize("tag,kb", gs.SVHT_CASES)
-def test_svht(tag, kb):
+@pytest.mark.parametrize("tag,kb,vb", gs.SVHT_CASES)
+def test_svht(tag, kb, vb):
     gs.svht_scenario(F, tag, kb, lambda cap: TableAdapter(
-        wc.SingleValueHashTable(cap, key_bytes=kb), kb, kb))
+        wc.SingleValueHashTable(cap, key_bytes=kb, value_bytes=vb), kb, vb), vb)
 
 
 @pytest.mark.parametrize("tag,kb", gs.SET_CASES)
@@ -82,10 +82,10 @@ def test_hashset(tag, kb):
     gs.set_scenario(F, tag, kb, lambda cap: TableAdapter(wc.HashSet(cap, key_bytes=kb), kb, 1))
 
 
-@pytest.mark.parametrize("tag", gs.COUNT_CASES)
-def test_counting(tag):
+@pytest.mark.parametrize("tag,vb", gs.COUNT_CASES)
+def test_counting(tag, vb):
     gs.counting_scenario(F, tag, lambda cap, mx: TableAdapter(
-        wc.CountingHashTable(cap, max_count=mx, key_bytes=4), 4, 4))
+        wc.CountingHashTable(cap, max_count=mx, key_bytes=4, value_bytes=vb), 4, vb), vb)
 
 
 @pytest.mark.parametrize("tag", gs.BLOOM_CASES)

@@ -36,9 +36,9 @@ def test_return_boolean_handler():
         assert np.array_equal(got, exp), name
 
 
-@pytest.mark.parametrize("tag,kb", gs.SVHT_CASES)
-def test_svht(tag, kb):
-    gs.svht_scenario(F, tag, kb, lambda cap: o.Table(o.SVHT, kb, kb, cap))
+@pytest.mark.parametrize("tag,kb,vb", gs.SVHT_CASES)
+def test_svht(tag, kb, vb):
+    gs.svht_scenario(F, tag, kb, lambda cap: o.Table(o.SVHT, kb, vb, cap), vb)
 
 
 @pytest.mark.parametrize("tag,kb", gs.SET_CASES)
@@ -46,10 +46,10 @@ def test_hashset(tag, kb):
     gs.set_scenario(F, tag, kb, lambda cap: o.Table(o.HASHSET, kb, 0, cap, cg=16))
 
 
-@pytest.mark.parametrize("tag", gs.COUNT_CASES)
-def test_counting(tag):
-    gs.counting_scenario(F, tag, lambda cap, mx: o.Table(o.COUNTING, 4, 4, cap, cg=4,
-                                                         max_count=mx))
+@pytest.mark.parametrize("tag,vb", gs.COUNT_CASES)
+def test_counting(tag, vb):
+    gs.counting_scenario(F, tag, lambda cap, mx: o.Table(o.COUNTING, 4, vb, cap, cg=4,
+                                                         max_count=mx), vb)
 
 
 @pytest.mark.parametrize("tag", gs.BLOOM_CASES)

@@ -21,18 +21,20 @@ ORACLE_PROBE = {wc.PROBING_DOUBLE: o.PROBE_DOUBLE, wc.PROBING_LINEAR: o.PROBE_LI
 
 
 def make_pair(kind, kb, n_cap, cg, probing=wc.PROBING_DOUBLE, h1=wc.HASH_MURMUR,
-              h2=wc.HASH_MURMUR, seed=wc.DEFAULT_SEED, max_count=None, empty=0, tomb=None):
+              h2=wc.HASH_MURMUR, seed=wc.DEFAULT_SEED, max_count=None, empty=0, tomb=None,
+              vb=None):
     if tomb is None:
         tomb = (1 << (8 * kb)) - 1
+    vb = kb if vb is None else vb
     kw = dict(key_bytes=kb, cg_size=cg, probing=probing, hasher1=h1, hasher2=h2,
               empty_key=empty, tombstone_key=tomb)
     if kind == o.SVHT:
-        g = wc.SingleValueHashTable(n_cap, seed=seed, **kw)
+        g = wc.SingleValueHashTable(n_cap, seed=seed, value_bytes=vb, **kw)
     elif kind == o.HASHSET:
         g = wc.HashSet(n_cap, seed=seed, **kw)
     else:
-        g = wc.CountingHashTable(n_cap, seed=seed, max_count=max_count, **kw)
-    r = o.Table(kind, kb, 0 if kind == o.HASHSET else kb, n_cap, seed=seed, cg=cg,
+        g = wc.CountingHashTable(n_cap, seed=seed, max_count=max_count, value_bytes=vb, **kw)
+    r = o.Table(kind, kb, 0 if kind == o.HASHSET else vb, n_cap, seed=seed, cg=cg,
                 scheme=ORACLE_PROBE[probing], h1=h1, h2=h2, empty_key=empty,
                 tombstone_key=tomb, max_count=max_count)
     assert g.capacity == r.capacity
@@ -40,12 +42,13 @@ def make_pair(kind, kb, n_cap, cg, probing=wc.PROBING_DOUBLE, h1=wc.HASH_MURMUR,
 
 
 def svht_round_trip(kb, cg, probing=wc.PROBING_DOUBLE, h1=wc.HASH_MURMUR,
-                    h2=wc.HASH_MURMUR, n=20000, load=0.8, seed=7):
+                    h2=wc.HASH_MURMUR, n=20000, load=0.8, seed=7, vb=None):
+    vb = kb if vb is None else vb
     n_cap = int(n / load)
-    g, r = make_pair(o.SVHT, kb, n_cap, cg, probing, h1, h2)
+    g, r = make_pair(o.SVHT, kb, n_cap, cg, probing, h1, h2, vb=vb)
     allk = o.gen_unique_keys(kb, 2 * n, seed)
     keys, absent = allk[:n], allk[n:]
-    vals = o.gen_uniform(kb, n, seed + 1)
+    vals = o.gen_uniform(vb, n, seed + 1)
     st = empty_dev(n, 4)
     g.insert(dev(keys), dev(vals), status_out=st)
     r_st = r.insert(keys, vals, want_status=True)
@@ -56,7 +59,7 @@ def svht_round_trip(kb, cg, probing=wc.PROBING_DOUBLE, h1=wc.HASH_MURMUR,
     # duplicates with new values, plus both sentinels
     nd = n // 8
     k2 = np.concatenate([keys[:nd], np.array([0, (1 << (8 * kb)) - 1], dtype=keys.dtype)])
-    v2 = o.gen_uniform(kb, nd + 2, seed + 2)
+    v2 = o.gen_uniform(vb, nd + 2, seed + 2)
     st2 = empty_dev(nd + 2, 4)
     g.insert(dev(k2), dev(v2), status_out=st2)
     assert np.array_equal(host(st2), r.insert(k2, v2, want_status=True))
@@ -65,10 +68,10 @@ def svht_round_trip(kb, cg, probing=wc.PROBING_DOUBLE, h1=wc.HASH_MURMUR,
     q = np.empty(2 * n, dtype=keys.dtype)
     q[0::2] = keys
     q[1::2] = absent
-    out = empty_dev(2 * n, kb, SENT[kb])
+    out = empty_dev(2 * n, vb, SENT[vb])
     st3 = empty_dev(2 * n, 4)
     g.retrieve(dev(q), out, status_out=st3)
-    r_out = np.full(2 * n, SENT[kb], dtype=keys.dtype)
+    r_out = np.full(2 * n, SENT[vb], dtype=vals.dtype)
     r_out, r_st3 = r.retrieve(q, r_out, want_status=True)
     assert np.array_equal(host(out), r_out)
     assert np.array_equal(host(st3), r_st3)
@@ -81,17 +84,17 @@ def svht_round_trip(kb, cg, probing=wc.PROBING_DOUBLE, h1=wc.HASH_MURMUR,
     assert g.size() == r.size()
     assert g.pop_status() == r.pop_status()
 
-    out = empty_dev(2 * n, kb, SENT[kb])
+    out = empty_dev(2 * n, vb, SENT[vb])
     st5 = empty_dev(2 * n, 4)
     g.retrieve(dev(q), out, status_out=st5)
-    r_out = np.full(2 * n, SENT[kb], dtype=keys.dtype)
+    r_out = np.full(2 * n, SENT[vb], dtype=vals.dtype)
     r_out, r_st5 = r.retrieve(q, r_out, want_status=True)
     assert np.array_equal(host(out), r_out)
     assert np.array_equal(host(st5), r_st5)
 
     # contents as a multiset
     ko = empty_dev(g.capacity, kb)
-    vo = empty_dev(g.capacity, kb)
+    vo = empty_dev(g.capacity, vb)
     m = g.retrieve_all(ko, vo)
     rk, rv = r.retrieve_all()
     assert m == rk.size
@@ -187,11 +190,43 @@ def test_hashset(kb, cg):
     assert np.array_equal(np.sort(host(ko)[:m]), np.sort(r.retrieve_all()))
 
 
-@pytest.mark.parametrize("kb", [4, 8])
+@pytest.mark.parametrize("kb,vb", [(4, 8), (8, 4)])
+@pytest.mark.parametrize("cg", [1, 8, 32])
+@pytest.mark.parametrize("policy", ["never", "always"])
+def test_svht_mixed_widths(kb, vb, cg, policy):
+    """u32 keys with u64 values and u64 keys with u32 values (16-byte slots),
+    on the window and the fingerprint kernels"""
+    old = wc.set_fingerprint_policy(policy)
+    try:
+        svht_round_trip(kb, cg, vb=vb, load=0.9)
+    finally:
+        wc.set_fingerprint_policy(old)
+
+
+def test_svht_mixed_widths_rebuild_route():
+    """a large insert into a table with fingerprints larger than half of
+    L2 takes the window kernel and the fingerprint rebuild; every pair reads
+    back and the size is exact"""
+    import torch
+    n = 1 << 26
+    t = wc.SingleValueHashTable(int(n / 0.9), key_bytes=4, value_bytes=8)
+    assert t.info().fingerprints
+    keys = wc.gen_unique(torch.empty(n, dtype=torch.int32, device="cuda"), 5)
+    vals = wc.gen_uniform(torch.empty(n, dtype=torch.int64, device="cuda"), 6)
+    t.insert(keys, vals)
+    assert t.size() == n
+    out = torch.zeros(n, dtype=torch.int64, device="cuda")
+    st = torch.empty(n, dtype=torch.int32, device="cuda")
+    t.retrieve(keys, out, status_out=st)
+    assert bool((st == 0).all())
+    assert torch.equal(out, vals)
+
+
+@pytest.mark.parametrize("kb,vb", [(4, 4), (8, 8), (4, 8), (8, 4)])
 @pytest.mark.parametrize("max_count", [None, 10])
-def test_counting_zipf(kb, max_count):
+def test_counting_zipf(kb, vb, max_count):
     distinct, occ = 5000, 200000
-    g, r = make_pair(o.COUNTING, kb, 6000, 4, max_count=max_count)
+    g, r = make_pair(o.COUNTING, kb, 6000, 4, max_count=max_count, vb=vb)
     allk = o.gen_unique_keys(kb, distinct + distinct // 4, 51)
     ranks = o.gen_zipf_ranks(distinct, 1.1, occ, 54)
     keys = allk[(ranks - 1).astype(np.int64)]
@@ -203,10 +238,10 @@ def test_counting_zipf(kb, max_count):
     # number of claims and of duplicates is not
     assert np.array_equal(np.sort(g_st), np.sort(r_st))
     assert g.pop_status() == r.pop_status()
-    out = empty_dev(allk.size, kb, SENT[kb])
+    out = empty_dev(allk.size, vb, SENT[vb])
     st2 = empty_dev(allk.size, 4)
     g.retrieve(dev(allk), out, status_out=st2)
-    r_out = np.full(allk.size, SENT[kb], dtype=allk.dtype)
+    r_out = np.full(allk.size, SENT[vb], dtype=np.uint32 if vb == 4 else np.uint64)
     r_out, r_st2 = r.retrieve(allk, r_out, want_status=True)
     assert np.array_equal(host(out), r_out)
     assert np.array_equal(host(st2), r_st2)

@@ -49,6 +49,8 @@ CountKernel count_kernel(int layout)
     case kLayoutKV64: return count_valid_kernel<LayoutKV64>;
     case kLayoutSet32: return count_valid_kernel<LayoutSet32>;
     case kLayoutSet64: return count_valid_kernel<LayoutSet64>;
+    case kLayoutK32V64: return count_valid_kernel<LayoutK32V64>;
+    case kLayoutK64V32: return count_valid_kernel<LayoutK64V32>;
     default: return nullptr;
     }
 }
@@ -60,6 +62,8 @@ RebuildKernel fp_rebuild_kernel_ptr(int layout)
     case kLayoutKV64: return fp_rebuild_kernel<LayoutKV64>;
     case kLayoutSet32: return fp_rebuild_kernel<LayoutSet32>;
     case kLayoutSet64: return fp_rebuild_kernel<LayoutSet64>;
+    case kLayoutK32V64: return fp_rebuild_kernel<LayoutK32V64>;
+    case kLayoutK64V32: return fp_rebuild_kernel<LayoutK64V32>;
     default: return nullptr;
     }
 }
@@ -71,6 +75,8 @@ DumpKernel dump_kernel_ptr(int layout)
     case kLayoutKV64: return dump_kernel<LayoutKV64>;
     case kLayoutSet32: return dump_kernel<LayoutSet32>;
     case kLayoutSet64: return dump_kernel<LayoutSet64>;
+    case kLayoutK32V64: return dump_kernel<LayoutK32V64>;
+    case kLayoutK64V32: return dump_kernel<LayoutK64V32>;
     default: return nullptr;
     }
 }

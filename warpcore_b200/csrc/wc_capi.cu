@@ -488,7 +488,11 @@ int check_config(const wc_table_config *cfg, int kind)
     if (!cfg) return fail(WC_ERR_INVALID_ARGUMENT, "config is NULL");
     if (cfg->key_bytes != 4 && cfg->key_bytes != 8)
         return fail(WC_ERR_UNSUPPORTED, "key_bytes must be 4 or 8");
-    if (kind != 1 && cfg->value_bytes != cfg->key_bytes)
+    /* SingleValue and Counting tables take 4- or 8-byte values with either
+     * key width; the multi-value table takes values of the key's width */
+    if (kind != 1 && cfg->value_bytes != 4 && cfg->value_bytes != 8)
+        return fail(WC_ERR_UNSUPPORTED, "value_bytes must be 4 or 8 (got %u)", cfg->value_bytes);
+    if (kind == 3 && cfg->value_bytes != cfg->key_bytes)
         return fail(WC_ERR_UNSUPPORTED, "value_bytes must equal key_bytes (got %u/%u)",
                     cfg->key_bytes, cfg->value_bytes);
     if (!valid_cg(cfg->cg_size))
@@ -510,7 +514,9 @@ int fill_slots(wc_table *t, cudaStream_t stream)
     uint32_t w[4];
     switch (t->layout) {
     case kLayoutKV32: w[0] = uint32_t(e); w[1] = 0; w[2] = uint32_t(e); w[3] = 0; break;
-    case kLayoutKV64: w[0] = uint32_t(e); w[1] = uint32_t(e >> 32); w[2] = 0; w[3] = 0; break;
+    case kLayoutKV64:
+    case kLayoutK32V64: /* e < 2^32 there: the key's upper half is 0 */
+    case kLayoutK64V32: w[0] = uint32_t(e); w[1] = uint32_t(e >> 32); w[2] = 0; w[3] = 0; break;
     case kLayoutSet32: w[0] = w[1] = w[2] = w[3] = uint32_t(e); break;
     default: w[0] = uint32_t(e); w[1] = uint32_t(e >> 32); w[2] = w[0]; w[3] = w[1]; break;
     }
@@ -547,9 +553,12 @@ int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, ui
     if (kind == 1) {
         t->layout = cfg->key_bytes == 4 ? kLayoutSet32 : kLayoutSet64;
         t->slot_bytes = cfg->key_bytes;
-    } else {
+    } else if (cfg->value_bytes == cfg->key_bytes) {
         t->layout = cfg->key_bytes == 4 ? kLayoutKV32 : kLayoutKV64;
         t->slot_bytes = 2 * cfg->key_bytes;
+    } else {
+        t->layout = cfg->key_bytes == 4 ? kLayoutK32V64 : kLayoutK64V32;
+        t->slot_bytes = 16;
     }
     t->capacity = cap;
     t->num_buckets = cap / cfg->cg_size;
@@ -621,6 +630,8 @@ TableKernel pick_window_kernel(const wc_table *t, int op)
     case kLayoutKV32: return table_kernel_kv32(W, op, false);
     case kLayoutKV64: return table_kernel_kv64(W, op, false);
     case kLayoutSet32: return table_kernel_set32(W, op, false);
+    case kLayoutK32V64: return table_kernel_k32v64(W, op, false);
+    case kLayoutK64V32: return table_kernel_k64v32(W, op, false);
     default: return table_kernel_set64(W, op, false);
     }
 }
@@ -633,6 +644,8 @@ TableKernel pick_table_kernel(const wc_table *t, int op)
     case kLayoutKV32: return table_kernel_kv32(W, op, fp);
     case kLayoutKV64: return table_kernel_kv64(W, op, fp);
     case kLayoutSet32: return table_kernel_set32(W, op, fp);
+    case kLayoutK32V64: return table_kernel_k32v64(W, op, fp);
+    case kLayoutK64V32: return table_kernel_k64v32(W, op, fp);
     default: return table_kernel_set64(W, op, fp);
     }
 }

@@ -15,7 +15,14 @@
 namespace warpcore {
 namespace b200 {
 
-enum : int { kLayoutKV32 = 0, kLayoutKV64 = 1, kLayoutSet32 = 2, kLayoutSet64 = 3 };
+enum : int {
+    kLayoutKV32 = 0,
+    kLayoutKV64 = 1,
+    kLayoutSet32 = 2,
+    kLayoutSet64 = 3,
+    kLayoutK32V64 = 4,
+    kLayoutK64V32 = 5
+};
 
 using TableKernel = void (*)(TableOpArgs);
 using BloomKernel = void (*)(BloomArgs);
@@ -28,6 +35,8 @@ TableKernel table_kernel_kv32(int W, int op, bool fingerprints);
 TableKernel table_kernel_kv64(int W, int op, bool fingerprints);
 TableKernel table_kernel_set32(int W, int op, bool fingerprints);
 TableKernel table_kernel_set64(int W, int op, bool fingerprints);
+TableKernel table_kernel_k32v64(int W, int op, bool fingerprints);
+TableKernel table_kernel_k64v32(int W, int op, bool fingerprints);
 
 CountKernel count_kernel(int layout);
 using RebuildKernel = void (*)(const void *, uint64_t, uint64_t, uint64_t, unsigned char *);

@@ -1,33 +1,10 @@
 /* bulk table kernels for the LayoutKV32 slot layout (see wc_kernels.cuh) */
-#include "wc_internal.h"
+#include "wc_tables_pick.cuh"
 
 namespace warpcore {
 namespace b200 {
 
-template <int W, class L = LayoutKV32>
-static TableKernel pick_kv32(int op, bool fp)
-{
-    switch (op) {
-    case kOpInsert: return fp ? fp_op_kernel<L, W, kOpInsert> : table_op_kernel<L, W, kOpInsert>;
-    case kOpCount: return fp ? fp_op_kernel<L, W, kOpCount> : table_op_kernel<L, W, kOpCount>;
-    case kOpRetrieve: return fp ? fp_op_kernel<L, W, kOpRetrieve> : table_op_kernel<L, W, kOpRetrieve>;
-    case kOpErase: return fp ? fp_op_kernel<L, W, kOpErase> : table_op_kernel<L, W, kOpErase>;
-    default: return nullptr;
-    }
-}
-
-TableKernel table_kernel_kv32(int W, int op, bool fp)
-{
-    switch (W) {
-    case 1: return pick_kv32<1>(op, fp);
-    case 2: return pick_kv32<2>(op, fp);
-    case 4: return pick_kv32<4>(op, fp);
-    case 8: return pick_kv32<8>(op, fp);
-    case 16: return pick_kv32<16>(op, fp);
-    case 32: return pick_kv32<32>(op, fp);
-    default: return nullptr;
-    }
-}
+TableKernel table_kernel_kv32(int W, int op, bool fp) { return pick_table_kernel_for<LayoutKV32>(W, op, fp); }
 
 } // namespace b200
 } // namespace warpcore
