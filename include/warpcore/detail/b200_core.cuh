@@ -506,19 +506,23 @@ __device__ __forceinline__ void count_add(void *sp, uint32_t c, uint64_t max_cou
     }
 }
 
-/* window bit of (lane-in-group qq, slot s) is qq * SPL + s */
+/* A window's hit / free masks are slot-major inside a lane group: lane qq
+ * of the group holds slots qq * SPL .. qq * SPL + SPL - 1, and the ballot of
+ * its slot s lands at bits s * TPK .. s * TPK + TPK - 1, so building a mask
+ * is one shift per slot.  Which free slot a key claims first is not
+ * observable (no answer depends on a key's position inside its window), so
+ * the mask needs no slot-order interleave; slot_of_bit maps a bit back to
+ * the slot index it stands for. */
 template <int TPK, int SPL>
-__device__ __forceinline__ uint32_t spread_bits(uint32_t group_bits, int s)
+__device__ __forceinline__ uint32_t window_bits(uint32_t group_bits, int s)
 {
-    if constexpr (SPL == 1) {
-        return group_bits;
-    } else {
-        uint32_t r = 0;
-#pragma unroll
-        for (int qq = 0; qq < TPK; ++qq)
-            r |= ((group_bits >> qq) & 1u) << (qq * SPL + s);
-        return r;
-    }
+    return SPL == 1 ? group_bits : group_bits << (s * TPK);
+}
+
+template <int TPK, int SPL>
+__device__ __forceinline__ int slot_of_bit(int p)
+{
+    return SPL == 1 ? p : (p % TPK) * SPL + p / TPK;
 }
 
 __device__ __forceinline__ int nth_set_bit(uint32_t mask, int n)

@@ -174,7 +174,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs a)
 
             if (pending && claiming) {
                 const BatchDesc &d = a.desc[req];
-                const int s = __ffs(claim_bits) - 1;
+                const int s = slot_of_bit<TPK, SPL>(__ffs(claim_bits) - 1);
                 unsigned char *const sp = reinterpret_cast<unsigned char *>(d.t.slots) +
                                           (bucket * W + uint64_t(s)) * SB;
                 cas_old = cas_slot<L>(sp, empty, claim_expect, key, val, &cas_old_payload);
@@ -197,8 +197,8 @@ __device__ __forceinline__ void batch_body(const BatchArgs a)
                         const unsigned hb = __ballot_sync(kFull, h);
                         const unsigned eb = __ballot_sync(kFull, served && sk == em);
                         if (loading && my_round == rr) {
-                            hit_bits |= spread_bits<TPK, SPL>((hb >> (my_g * TPK)) & kGroupMask, s);
-                            empty_bits |= spread_bits<TPK, SPL>((eb >> (my_g * TPK)) & kGroupMask, s);
+                            hit_bits |= window_bits<TPK, SPL>((hb >> (my_g * TPK)) & kGroupMask, s);
+                            empty_bits |= window_bits<TPK, SPL>((eb >> (my_g * TPK)) & kGroupMask, s);
                         }
                         if (h && a.desc[rq].op == kOpRetrieve) {
                             const BatchDesc &d = a.desc[rq];
@@ -226,7 +226,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs a)
                     }
                 } else {
                     if (hit_bits) {
-                        store_value<L>(bptr + (__ffs(hit_bits) - 1) * SB, val);
+                        store_value<L>(bptr + slot_of_bit<TPK, SPL>(__ffs(hit_bits) - 1) * SB, val);
                         st = kStDuplicateKey;
                         pending = false;
                     } else if (empty_bits) {
@@ -240,7 +240,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs a)
             }
             if (did_cas) {
                 const BatchDesc &d = a.desc[req];
-                const int s = __ffs(claim_bits) - 1;
+                const int s = slot_of_bit<TPK, SPL>(__ffs(claim_bits) - 1);
                 unsigned char *const sp = reinterpret_cast<unsigned char *>(d.t.slots) +
                                           (bucket * W + uint64_t(s)) * SB;
                 if (cas_old == empty && cas_old_payload == claim_expect) {

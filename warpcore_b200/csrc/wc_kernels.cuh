@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
 
             if constexpr (OP == kOpInsert || OP == kOpCount) {
                 if (pending && claiming) {
-                    const int s = __ffs(claim_bits) - 1;
+                    const int s = slot_of_bit<TPK, SPL>(__ffs(claim_bits) - 1);
                     unsigned char *const sp = slots + (bucket * W + uint64_t(s)) * SB;
                     const V payload = OP == kOpCount ? V(cnt_add) : val;
                     cas_old = cas_slot<L>(sp, empty, claim_expect, key, payload, &cas_old_payload);
@@ -360,8 +360,8 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
                         const unsigned hb = __ballot_sync(kFull, h);
                         const unsigned eb = __ballot_sync(kFull, served && sk == empty);
                         if (loading && my_round == rr) {
-                            hit_bits |= spread_bits<TPK, SPL>((hb >> (my_g * TPK)) & kGroupMask, s);
-                            empty_bits |= spread_bits<TPK, SPL>((eb >> (my_g * TPK)) & kGroupMask, s);
+                            hit_bits |= window_bits<TPK, SPL>((hb >> (my_g * TPK)) & kGroupMask, s);
+                            empty_bits |= window_bits<TPK, SPL>((eb >> (my_g * TPK)) & kGroupMask, s);
                         }
                         if constexpr (OP == kOpRetrieve && L::kHasValue) {
                             /* a key occupies at most one slot, so the lane
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
             if (loading) {
                 unsigned char *const bptr = slots + bucket * uint64_t(W) * SB;
                 if (hit_bits) {
-                    const int fh = __ffs(hit_bits) - 1;
+                    const int fh = slot_of_bit<TPK, SPL>(__ffs(hit_bits) - 1);
                     unsigned char *const sp = bptr + fh * SB;
                     if constexpr (OP == kOpRetrieve) {
                         st = kStNone;
@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
             }
             if constexpr (OP == kOpInsert || OP == kOpCount) {
                 if (did_cas) {
-                    const int s = __ffs(claim_bits) - 1;
+                    const int s = slot_of_bit<TPK, SPL>(__ffs(claim_bits) - 1);
                     unsigned char *const sp = slots + (bucket * W + uint64_t(s)) * SB;
                     if (cas_old == empty && cas_old_payload == claim_expect) {
                         fp_store(t, bucket * W + uint64_t(s), fingerprint(key));
