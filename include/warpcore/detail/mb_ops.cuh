@@ -226,10 +226,12 @@ __device__ uint32_t mb_insert_one(const MbView &m, K key, V value, uint64_t max_
  * returns the status (none, key_not_found, probing_length_exceeded,
  * invalid_key) and the count in num.  The count takes bucket values per
  * hit slot less the empty places of each window's last hit slot, so a
- * count-only walk reads that one bucket per window. */
+ * count-only walk reads that one bucket per window.  A walk that already
+ * knows the key's count passes it as stop_at and ends at the window where
+ * that many values are read (status none). */
 template <class K, class V, int kW = 0, int kB = 0, bool kValues = true, class F>
 __device__ uint32_t mb_for_each_one(const MbView &m, K key, uint64_t max_windows, uint64_t &num,
-                                    F f)
+                                    F f, uint64_t stop_at = ~uint64_t(0))
 {
     const TableView &t = m.t;
     const uint32_t W = mb_w<kW>(m), B = mb_b<kB>(m);
@@ -259,6 +261,7 @@ __device__ uint32_t mb_for_each_one(const MbView &m, K key, uint64_t max_windows
             const uint32_t le = __popc(mb_bucket_empties<V, kB>(
                 vals + (b * W + uint64_t(last)) * B, B, ev, nullptr));
             num += uint64_t(B) * uint64_t(__popc(hits)) - le;
+            if (num >= stop_at) return kStNone;
         }
         if (emp || num >= m.max_values) return num ? kStNone : kStKeyNotFound;
         if (w == 0) step = probe_step<K>(t, key);

@@ -101,24 +101,25 @@ __global__ void __launch_bounds__(256, WC_MULTI_MIN_BLOCKS) bl_find_kernel(const
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.n; i += stride) {
         uint64_t num = 0;
-        uint32_t st;
         const K key = reinterpret_cast<const K *>(a.keys)[i];
         if constexpr (kValues) {
-            V *const out = reinterpret_cast<V *>(a.values_out) + a.begin[i];
+            /* The counting pass looked every key up and wrote its status;
+             * this pass only reads lists.  A key counted at 0 needs no
+             * lookup.  Values go inside the key's own segment only. */
             const uint64_t room = a.end[i] - a.begin[i];
-            st = bl_for_each_one<K, V, kW, true>(a.v, key, a.max_windows, num, [&](V x, uint64_t j) {
+            if (room == 0) continue;
+            V *const out = reinterpret_cast<V *>(a.values_out) + a.begin[i];
+            bl_for_each_one<K, V, kW, true>(a.v, key, a.max_windows, num, [&](V x, uint64_t j) {
                 if (j < room) out[j] = x;
             });
-            /* a count other than the counting pass's is a phase overlap */
-            if (num != room) st |= kStInvalidPhaseOverlap;
         } else {
-            st = bl_for_each_one<K, V, kW, false>(a.v, key, a.max_windows, num,
-                                                  [](V, uint64_t) {});
+            const uint32_t st = bl_for_each_one<K, V, kW, false>(a.v, key, a.max_windows, num,
+                                                                 [](V, uint64_t) {});
+            join |= st;
+            if (a.counts_out) a.counts_out[i] = num;
+            total += num;
+            bl_write_status(a, i, st);
         }
-        join |= st;
-        if (a.counts_out) a.counts_out[i] = num;
-        total += num;
-        bl_write_status(a, i, st);
     }
     const uint32_t wj = __reduce_or_sync(0xffffffffu, join);
     const unsigned lo = __reduce_add_sync(0xffffffffu, unsigned(total & 0xffffffffu));
@@ -470,8 +471,10 @@ int wc_blht_retrieve(wc_blht *t, const void *keys_in, uint64_t num_in,
     if (!keys_in || !end_offsets_out || (values_out && !begin_offsets_out))
         return bl_fail(WC_ERR_INVALID_ARGUMENT, "NULL buffer");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    rc = count(t, keys_in, num_in, end_offsets_out, num_out, s, probing_length, nullptr,
-               WC_HANDLER_NOTHING, 0);
+    /* pass 1: counts, and each key's status (the values pass reads lists only) */
+    rc = count(t, keys_in, num_in, end_offsets_out, num_out, s, probing_length,
+               values_out ? status_out : nullptr, values_out ? status_handler : WC_HANDLER_NOTHING,
+               ignore);
     if (rc) return rc;
     if (!values_out) {
         rc = host_dry_run_status(status_out, num_in, status_handler, ignore, s);

@@ -1111,9 +1111,11 @@ int wc_mvht_retrieve(wc_table *t, const void *keys_in, uint64_t num_in,
     if (!keys_in || !end_offsets_out || (values_out && !begin_offsets_out))
         return fail(WC_ERR_INVALID_ARGUMENT, "NULL buffer");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    /* pass 1: counts per key into end_offsets (no per-key status) */
-    rc = mv_count(t, keys_in, num_in, end_offsets_out, num_out, s, probing_length, nullptr,
-                  WC_HANDLER_NOTHING, 0);
+    /* pass 1: counts per key into end_offsets, and each key's status (the
+     * values pass reads values only) */
+    rc = mv_count(t, keys_in, num_in, end_offsets_out, num_out, s, probing_length,
+                  values_out ? status_out : nullptr,
+                  values_out ? status_handler : WC_HANDLER_NOTHING, ignore);
     if (rc) return rc;
     if (!values_out) {
         /* dry run: per-key counts, status dry_run for every key */

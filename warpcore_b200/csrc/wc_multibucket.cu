@@ -115,24 +115,28 @@ __global__ void __launch_bounds__(256, WC_MULTI_MIN_BLOCKS) mb_find_kernel(const
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.n; i += stride) {
         uint64_t num = 0;
-        uint32_t st;
         const K key = reinterpret_cast<const K *>(a.keys)[i];
         if constexpr (kValues) {
-            /* values go inside the key's own segment only; another count
-             * than the counting pass saw means the table changed in between */
-            V *const out = reinterpret_cast<V *>(a.values_out) + a.begin[i];
+            /* The counting pass walked every key to its end and wrote its
+             * status; this pass only reads values.  A key counted at 0
+             * needs no walk, and a walk ends once the counted values are
+             * read.  Values go inside the key's own segment only. */
             const uint64_t room = a.end[i] - a.begin[i];
-            st = mb_for_each_one<K, V, kW, kB, true>(a.m, key, a.max_windows, num, [&](V v, uint64_t j) {
-                if (j < room) out[j] = v;
-            });
-            if (st != kStInvalidKey && num != room) st |= kStInvalidPhaseOverlap;
+            if (room == 0) continue;
+            V *const out = reinterpret_cast<V *>(a.values_out) + a.begin[i];
+            mb_for_each_one<K, V, kW, kB, true>(
+                a.m, key, a.max_windows, num, [&](V v, uint64_t j) {
+                    if (j < room) out[j] = v;
+                },
+                room);
         } else {
-            st = mb_for_each_one<K, V, kW, kB, false>(a.m, key, a.max_windows, num, [](V, uint64_t) {});
+            const uint32_t st = mb_for_each_one<K, V, kW, kB, false>(a.m, key, a.max_windows, num,
+                                                                     [](V, uint64_t) {});
+            join |= st;
+            if (a.counts_out) a.counts_out[i] = num;
+            total += num;
+            mb_write_status(a, i, st);
         }
-        join |= st;
-        if (a.counts_out) a.counts_out[i] = num;
-        total += num;
-        mb_write_status(a, i, st);
     }
     const uint32_t wj = __reduce_or_sync(0xffffffffu, join);
     const unsigned lo = __reduce_add_sync(0xffffffffu, unsigned(total & 0xffffffffu));
@@ -486,9 +490,11 @@ int wc_mbht_retrieve(wc_mbht *t, const void *keys_in, uint64_t num_in,
     if (!keys_in || !end_offsets_out || (values_out && !begin_offsets_out))
         return mb_fail(WC_ERR_INVALID_ARGUMENT, "NULL buffer");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    /* pass 1: counts per key into end_offsets */
-    rc = count(t, keys_in, num_in, end_offsets_out, num_out, s, probing_length, nullptr,
-               WC_HANDLER_NOTHING, 0);
+    /* pass 1: counts per key into end_offsets, and each key's status (the
+     * values pass reads values only) */
+    rc = count(t, keys_in, num_in, end_offsets_out, num_out, s, probing_length,
+               values_out ? status_out : nullptr, values_out ? status_handler : WC_HANDLER_NOTHING,
+               ignore);
     if (rc) return rc;
     if (!values_out) {
         /* dry run: per-key counts, status dry_run for every key */

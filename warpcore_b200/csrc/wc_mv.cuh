@@ -98,26 +98,29 @@ __global__ void __launch_bounds__(256, WC_MULTI_MIN_BLOCKS) mv_find_kernel(const
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.n; i += stride) {
         uint64_t num = 0;
-        uint32_t st;
         if constexpr (kValues) {
-            /* values are written inside the key's own segment only; more
-             * values than the counting pass saw mean the table changed in
-             * between (invalid_phase_overlap) */
-            V *const out = reinterpret_cast<V *>(a.values_out) + a.begin[i];
+            /* The counting pass walked every key to its end and wrote its
+             * status; this pass only reads values.  A key counted at 0
+             * needs no walk, and a walk ends at the window where the
+             * counted values are read (its value limit).  Values are
+             * written inside the key's own segment only. */
             const uint64_t room = a.end[i] - a.begin[i];
-            st = mv_for_each_one<L, W>(a.t, reinterpret_cast<const K *>(a.keys)[i], a.max_windows,
-                                       a.max_values, num, [&](V v, uint64_t j) {
-                                           if (j < room) out[j] = v;
-                                       });
-            if (st != kStInvalidKey && num != room) st |= kStInvalidPhaseOverlap;
+            if (room == 0) continue;
+            V *const out = reinterpret_cast<V *>(a.values_out) + a.begin[i];
+            mv_for_each_one<L, W>(a.t, reinterpret_cast<const K *>(a.keys)[i], a.max_windows,
+                                  room < a.max_values ? room : a.max_values, num,
+                                  [&](V v, uint64_t j) {
+                                      if (j < room) out[j] = v;
+                                  });
         } else {
-            st = mv_for_each_one<L, W>(a.t, reinterpret_cast<const K *>(a.keys)[i], a.max_windows,
-                                       a.max_values, num, [](V, uint64_t) {});
+            const uint32_t st = mv_for_each_one<L, W>(a.t, reinterpret_cast<const K *>(a.keys)[i],
+                                                      a.max_windows, a.max_values, num,
+                                                      [](V, uint64_t) {});
+            join |= st;
+            if (a.counts_out) a.counts_out[i] = num;
+            total += num;
+            mv_write_status(a, i, st);
         }
-        join |= st;
-        if (a.counts_out) a.counts_out[i] = num;
-        total += num;
-        mv_write_status(a, i, st);
     }
     /* every lane of the warp arrives here (no early exits); 64-bit sum as
      * two 32-bit halves */
