@@ -11,6 +11,20 @@
 
 namespace warpcore {
 
+namespace detail {
+/* f(key, count) on every occupied slot, one thread per slot */
+template <class F, class L, class K, class V>
+__global__ void counting_for_each_kernel(F f, const b200::TableView t, index_t capacity, K empty,
+                                         K tomb)
+{
+    const index_t tid = index_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (tid >= capacity) return;
+    unsigned char *const sp = reinterpret_cast<unsigned char *>(t.slots) + tid * L::kSlotBytes;
+    const K key = *reinterpret_cast<const K *>(sp);
+    if (key != empty && key != tomb) f(key, V(*b200::slot_value_ptr<L>(sp)));
+}
+} // namespace detail
+
 template <class Key, class Value = index_t, Key EmptyKey = defaults::empty_key<Key>(),
           Key TombstoneKey = defaults::tombstone_key<Key>(),
           class ProbingScheme = defaults::probing_scheme_t<Key, 4>,
@@ -142,6 +156,18 @@ class CountingHashTable {
                           (void *)status_out, StatusHandler::kId, StatusHandler::kIgnore);
     }
 
+    /* for_each (counting_hash_table.cuh:303-317): f(key, count) on every
+     * key of the table, a device lambda, asynchronous on `stream` */
+    template <class Func>
+    void for_each(Func f, cudaStream_t stream = 0, index_type smem_bytes = 0) const noexcept
+    {
+        if (!is_initialized_ || capacity_ == 0) return;
+        const index_type blocks = (capacity_ + 255) / 256;
+        detail::counting_for_each_kernel<Func, layout, key_type, value_type>
+            <<<unsigned(blocks), 256, smem_bytes, stream>>>(f, view_, capacity_, EmptyKey,
+                                                            TombstoneKey);
+    }
+
     index_type size(cudaStream_t stream = 0) const noexcept
     {
         if (!is_initialized_) return 0;
@@ -170,6 +196,14 @@ class CountingHashTable {
         std::uint32_t s = WC_STATUS_NOT_INITIALIZED;
         if (handle_) wc_table_pop_status(handle_, stream_of(stream), &s);
         return status_type(s);
+    }
+    __host__ __device__ static constexpr bool is_empty_key(key_type key) noexcept
+    {
+        return key == empty_key();
+    }
+    __host__ __device__ static constexpr bool is_tombstone_key(key_type key) noexcept
+    {
+        return key == tombstone_key();
     }
     __host__ __device__ static constexpr bool is_valid_key(key_type key) noexcept
     {

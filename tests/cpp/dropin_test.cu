@@ -261,6 +261,19 @@ static void test_counting()
     c.retrieve(dk, distinct, dout);
     auto out = hcopy(dout, distinct);
     for (uint64_t i = 0; i < distinct; ++i) CHECK(out[i] == 2 * (1 + (i % 7)));
+    /* for_each visits every key once with its count */
+    unsigned long long *dacc;
+    cudaMalloc(&dacc, 2 * sizeof(unsigned long long));
+    cudaMemset(dacc, 0, 2 * sizeof(unsigned long long));
+    c.for_each([=] __device__(uint32_t k, uint32_t n) {
+        atomicAdd(dacc, 1ull);
+        atomicAdd(dacc + 1, (unsigned long long)n);
+    });
+    auto acc = hcopy(dacc, 2);
+    CHECK(acc[0] == distinct);
+    CHECK(acc[1] == 2 * occ.size());
+    CHECK(Counter::is_empty_key(0) && Counter::is_tombstone_key(~0u) && !Counter::is_empty_key(5));
+    cudaFree(dacc);
     Counter capped(2 * distinct, wc::defaults::seed<uint32_t>(), 3);
     capped.insert(docc, occ.size());
     capped.retrieve(dk, distinct, dout);
