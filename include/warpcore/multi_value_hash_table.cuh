@@ -27,7 +27,7 @@ class MultiValueHashTable {
     static_assert(checks::is_probing_scheme<ProbingScheme>(), "not a valid probing scheme type");
     static_assert(std::is_same<typename ProbingScheme::key_type, Key>::value,
                   "probing key type differs from table's key type");
-    static_assert(sizeof(Value) == sizeof(Key) && std::is_integral<Value>::value,
+    static_assert((sizeof(Value) == 4 || sizeof(Value) == 8) && std::is_integral<Value>::value,
                   "this build stores integral values as wide as the key (u32/u32, u64/u64)");
 
     using layout = typename detail::layout_of<Key, typename std::make_unsigned<Value>::type>::type;

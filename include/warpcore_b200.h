@@ -86,9 +86,7 @@ typedef struct CUstream_st *wc_stream_t;
  * counting_hash_table.cuh:18-26) as run-time values. */
 typedef struct wc_table_config {
     uint32_t key_bytes;     /* 4 or 8 */
-    uint32_t value_bytes;   /* 4 or 8 with either key width (SingleValue,
-                             * Counting); equal to key_bytes (MultiValue);
-                             * 0 for a hash set */
+    uint32_t value_bytes;   /* 4 or 8, with either key width; 0 for a hash set */
     uint64_t empty_key;     /* EmptyKey, default 0 */
     uint64_t tombstone_key; /* TombstoneKey, default ~0 */
     uint32_t probing;       /* WC_PROBING_* */

@@ -821,6 +821,8 @@ static void run_gpu()
     bloom_case<uint32_t, uint64_t, 2>("bloom_u32_s64_cg2", 5000, 3, 400, 64);
     mv_case<uint32_t, uint32_t>("mv_u32u32_max3", 4000, 16000, 71, 3);
     mv_case<uint64_t, uint64_t>("mv_u64u64", 4000, 16000, 72, ~uint64_t(0));
+    mv_case<uint32_t, uint64_t>("mv_u32u64_max3", 4000, 16000, 73, 3);
+    mv_case<uint64_t, uint32_t>("mv_u64u32", 4000, 16000, 74, ~uint64_t(0));
     mb_case<uint32_t, uint32_t, 1>("mb_u32u32_b1", 4000, 16000, 81, ~uint64_t(0));
     mb_case<uint32_t, uint32_t, 2>("mb_u32u32_b2", 4000, 16000, 82, ~uint64_t(0));
     mb_case<uint32_t, uint32_t, 2>("mb_u32u32_b2_max3", 4000, 16000, 83, 3);

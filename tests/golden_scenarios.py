@@ -115,10 +115,11 @@ COUNT_CASES = [("count_u32", 4), ("count_u32_max10", 4), ("count_u32u64", 8),
 BLOOM_CASES = ["bloom_u64_s64_cg8", "bloom_u64_s64_cg1", "bloom_u32_s32_cg4", "bloom_u32_s64_cg2"]
 
 
-MV_CASES = [("mv_u32u32_max3", 4), ("mv_u64u64", 8)]
+MV_CASES = [("mv_u32u32_max3", 4, 4), ("mv_u64u64", 8, 8), ("mv_u32u64_max3", 4, 8),
+            ("mv_u64u32", 8, 4)]
 
 
-def mv_scenario(F, tag, kb, make_table):
+def mv_scenario(F, tag, kb, make_table, vb=None):
     """make_table(min_cap, max_values_per_key) -> object with insert /
     num_keys / size / pop_status / retrieve(keys, dry_run) /
     unique_keys like oracle.MVTable"""
@@ -131,7 +132,7 @@ def mv_scenario(F, tag, kb, make_table):
     st_all, vals_all = [], []
     for r in range(5):
         m = n - r * (n // 5)
-        v = o.gen_uniform(kb, m, kseed + 10 + r)
+        v = o.gen_uniform(kb if vb is None else vb, m, kseed + 10 + r)
         st_all.append(t.insert(keys[:m], v, want_status=True))
         vals_all.append(v)
     assert np.array_equal(np.concatenate(st_all), F[tag + "_insert_status"])

@@ -20,9 +20,11 @@ F = fixtures("ref_gpu")
 class GpuMV:
     """the oracle.MVTable interface over wc.MultiValueHashTable"""
 
-    def __init__(self, kb, cap, max_values, **kw):
+    def __init__(self, kb, cap, max_values, vb=None, **kw):
         self.kb = kb
-        self.t = wc.MultiValueHashTable(cap, key_bytes=kb, max_values_per_key=max_values, **kw)
+        self.vb = kb if vb is None else vb
+        self.t = wc.MultiValueHashTable(cap, key_bytes=kb, value_bytes=self.vb,
+                                        max_values_per_key=max_values, **kw)
 
     @property
     def capacity(self):
@@ -52,7 +54,7 @@ class GpuMV:
             self.t.retrieve(dk, b, e, None, status_out=st)
             return None, host(e), None, host(st)
         total = self.t.num_values(dk)
-        v = empty_dev(max(total, 1), self.kb)
+        v = empty_dev(max(total, 1), self.vb)
         num = self.t.retrieve(dk, b, e, v, status_out=st)
         assert num == total
         return host(b), host(e), host(v)[:num], host(st)
@@ -64,24 +66,24 @@ class GpuMV:
         return host(out)[:m]
 
 
-@pytest.mark.parametrize("tag,kb", gs.MV_CASES)
-def test_multi_value_golden(tag, kb):
-    gs.mv_scenario(F, tag, kb, lambda cap, mx: GpuMV(kb, cap, mx))
+@pytest.mark.parametrize("tag,kb,vb", gs.MV_CASES)
+def test_multi_value_golden(tag, kb, vb):
+    gs.mv_scenario(F, tag, kb, lambda cap, mx: GpuMV(kb, cap, mx, vb=vb), vb)
 
 
-@pytest.mark.parametrize("kb", [4, 8])
+@pytest.mark.parametrize("kb,vb", [(4, 4), (8, 8), (4, 8), (8, 4)])
 @pytest.mark.parametrize("cg", [1, 4, 8, 16, 32])
-def test_multi_value_vs_oracle(kb, cg):
+def test_multi_value_vs_oracle(kb, vb, cg):
     # rounds of unique keys: values per key in insertion order; then a
     # round that mixes new keys with held ones
     n = 3000
     keys = o.gen_unique_keys(kb, n + 500, 101 + cg)
-    g = GpuMV(kb, 4 * n, 4, cg_size=cg)
-    r = o.MVTable(kb, kb, 4 * n, cg=cg, max_values_per_key=4)
+    g = GpuMV(kb, 4 * n, 4, vb=vb, cg_size=cg)
+    r = o.MVTable(kb, vb, 4 * n, cg=cg, max_values_per_key=4)
     assert g.capacity == r.capacity
     for rnd in range(6):
         m = n - rnd * 400
-        v = o.gen_uniform(kb, m, 200 + rnd)
+        v = o.gen_uniform(vb, m, 200 + rnd)
         assert np.array_equal(g.insert(keys[:m], v, want_status=True),
                               r.insert(keys[:m], v, want_status=True)), rnd
     assert g.num_keys() == r.num_keys()

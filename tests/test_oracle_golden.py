@@ -59,9 +59,9 @@ def test_bloom(tag):
     gs.bloom_scenario(F, tag, make)
 
 
-@pytest.mark.parametrize("tag,kb", gs.MV_CASES)
-def test_multi_value(tag, kb):
-    gs.mv_scenario(F, tag, kb, lambda cap, mx: o.MVTable(kb, kb, cap, max_values_per_key=mx))
+@pytest.mark.parametrize("tag,kb,vb", gs.MV_CASES)
+def test_multi_value(tag, kb, vb):
+    gs.mv_scenario(F, tag, kb, lambda cap, mx: o.MVTable(kb, vb, cap, max_values_per_key=mx), vb)
 
 
 @pytest.mark.parametrize("tag,kb,vb", gs.MB_CASES)

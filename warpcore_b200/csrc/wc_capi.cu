@@ -488,13 +488,9 @@ int check_config(const wc_table_config *cfg, int kind)
     if (!cfg) return fail(WC_ERR_INVALID_ARGUMENT, "config is NULL");
     if (cfg->key_bytes != 4 && cfg->key_bytes != 8)
         return fail(WC_ERR_UNSUPPORTED, "key_bytes must be 4 or 8");
-    /* SingleValue and Counting tables take 4- or 8-byte values with either
-     * key width; the multi-value table takes values of the key's width */
+    /* tables with values take 4- or 8-byte values with either key width */
     if (kind != 1 && cfg->value_bytes != 4 && cfg->value_bytes != 8)
         return fail(WC_ERR_UNSUPPORTED, "value_bytes must be 4 or 8 (got %u)", cfg->value_bytes);
-    if (kind == 3 && cfg->value_bytes != cfg->key_bytes)
-        return fail(WC_ERR_UNSUPPORTED, "value_bytes must equal key_bytes (got %u/%u)",
-                    cfg->key_bytes, cfg->value_bytes);
     if (!valid_cg(cfg->cg_size))
         return fail(WC_ERR_INVALID_ARGUMENT, "cg_size must be 1, 2, 4, 8, 16 or 32");
     if (cfg->probing > WC_PROBING_QUADRATIC)

@@ -55,6 +55,7 @@ struct MvKernels {
     const void *insert = nullptr, *count = nullptr, *values = nullptr, *unique = nullptr;
 };
 MvKernels mv_kernels(int layout, int W);
+MvKernels mv_kernels_mixed(int layout, int W); /* u32/u64 and u64/u32 */
 struct MvScanKernels {
     const void *tile_sums, *tile_offsets, *apply, *dry_status;
 };

@@ -1,38 +1,14 @@
 /* MultiValueHashTable kernels for the u32/u32 and u64/u64 layouts (see wc_mv.cuh) */
-#include "wc_internal.h"
+#include "wc_mv_pick.cuh"
 
 namespace warpcore {
 namespace b200 {
-
-template <class L, int W>
-static MvKernels mv_pick()
-{
-    MvKernels k;
-    k.insert = reinterpret_cast<const void *>(mv_insert_kernel<L, W>);
-    k.count = reinterpret_cast<const void *>(mv_find_kernel<L, W, false>);
-    k.values = reinterpret_cast<const void *>(mv_find_kernel<L, W, true>);
-    k.unique = reinterpret_cast<const void *>(mv_unique_keys_kernel<L, W>);
-    return k;
-}
-
-template <class L>
-static MvKernels mv_pick_w(int W)
-{
-    switch (W) {
-    case 1: return mv_pick<L, 1>();
-    case 2: return mv_pick<L, 2>();
-    case 4: return mv_pick<L, 4>();
-    case 8: return mv_pick<L, 8>();
-    case 16: return mv_pick<L, 16>();
-    case 32: return mv_pick<L, 32>();
-    default: return MvKernels{};
-    }
-}
 
 MvKernels mv_kernels(int layout, int W)
 {
     if (layout == kLayoutKV32) return mv_pick_w<LayoutKV32>(W);
     if (layout == kLayoutKV64) return mv_pick_w<LayoutKV64>(W);
+    if (layout == kLayoutK32V64 || layout == kLayoutK64V32) return mv_kernels_mixed(layout, W);
     return MvKernels{};
 }
 
