@@ -247,19 +247,25 @@ __device__ uint32_t mb_for_each_one(const MbView &m, K key, uint64_t max_windows
         mb_window<K, kW>(keys + b * W, W, key, empty, hits, emp);
         if (hits) {
             const int last = 31 - __clz(hits);
+            uint32_t le;
             if constexpr (kValues) {
+                /* hit slots in ascending order: the last one read is the
+                 * window's last bucket, whose free places the count needs */
                 uint64_t j = num;
+                uint32_t e = 0;
                 for (uint32_t x = hits; x; x &= x - 1u) {
                     const uint64_t slot = b * W + uint64_t(__ffs(x) - 1);
                     V v[kB ? kB : 32];
-                    const uint32_t e = mb_bucket_empties<V, kB>(vals + slot * B, B, ev, v);
+                    e = mb_bucket_empties<V, kB>(vals + slot * B, B, ev, v);
                     for (uint32_t r = 0; r < (kB ? uint32_t(kB) : B); ++r)
                         if (!((e >> r) & 1u)) f(v[r], j + r);
                     j += B;
                 }
+                le = __popc(e);
+            } else {
+                le = __popc(mb_bucket_empties<V, kB>(vals + (b * W + uint64_t(last)) * B, B, ev,
+                                                     nullptr));
             }
-            const uint32_t le = __popc(mb_bucket_empties<V, kB>(
-                vals + (b * W + uint64_t(last)) * B, B, ev, nullptr));
             num += uint64_t(B) * uint64_t(__popc(hits)) - le;
             if (num >= stop_at) return kStNone;
         }
