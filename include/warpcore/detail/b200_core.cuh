@@ -509,10 +509,13 @@ __device__ __forceinline__ void count_add(void *sp, uint32_t c, uint64_t max_cou
 /* A window's hit / free masks are slot-major inside a lane group: lane qq
  * of the group holds slots qq * SPL .. qq * SPL + SPL - 1, and the ballot of
  * its slot s lands at bits s * TPK .. s * TPK + TPK - 1, so building a mask
- * is one shift per slot.  Which free slot a key claims first is not
- * observable (no answer depends on a key's position inside its window), so
- * the mask needs no slot-order interleave; slot_of_bit maps a bit back to
- * the slot index it stands for. */
+ * is one shift per slot.  slot_of_bit maps a bit back to the slot index it
+ * stands for (a key has at most one hit, so any bit order finds it).
+ * Claims are different: every insert path (window and fingerprint kernels,
+ * the count cache's flush, the device per-key API) must try a window's free
+ * slots in the same order, lowest slot first, or two paths inserting one key
+ * at the same time could each claim a different slot for it.  A free mask
+ * is read lowest slot first (lowest_slot_bit). */
 template <int TPK, int SPL>
 __device__ __forceinline__ uint32_t window_bits(uint32_t group_bits, int s)
 {
@@ -523,6 +526,27 @@ template <int TPK, int SPL>
 __device__ __forceinline__ int slot_of_bit(int p)
 {
     return SPL == 1 ? p : (p % TPK) * SPL + p / TPK;
+}
+
+/* the bit, in a non-empty slot-major mask, of its lowest slot: the lowest
+ * lane that has any bit set, then that lane's first slot */
+template <int TPK, int SPL>
+__device__ __forceinline__ int lowest_slot_bit(uint32_t m)
+{
+    if constexpr (SPL == 1) {
+        return __ffs(m) - 1;
+    } else {
+        constexpr uint32_t kLane = TPK == 32 ? 0xffffffffu : ((1u << TPK) - 1u);
+        uint32_t lanes = 0;
+#pragma unroll
+        for (int s = 0; s < SPL; ++s) lanes |= (m >> (s * TPK)) & kLane;
+        const int qq = __ffs(lanes) - 1;
+        int p = qq;
+#pragma unroll
+        for (int s = SPL - 1; s >= 0; --s)
+            if ((m >> (s * TPK + qq)) & 1u) p = s * TPK + qq;
+        return p;
+    }
 }
 
 __device__ __forceinline__ int nth_set_bit(uint32_t mask, int n)

@@ -192,13 +192,18 @@ __device__ __forceinline__ unsigned long long bl_alloc(const BlView &v, uint64_t
 
 /* append (storage.cuh:1108-1285) of one value to the list of handle h */
 template <class V>
-__device__ uint32_t bl_append(const BlView &v, unsigned long long *h, V value)
+__device__ uint32_t bl_append(const BlView &v, unsigned long long *h, V value,
+                             unsigned long long cur)
 {
+    /* cur: the handle as the caller read it.  Every step is checked by a
+     * compare-and-swap, whose result is the handle's current value, so a
+     * stale cur costs one retry and the handle is reloaded only after
+     * waiting on a list that another thread is growing. */
     const uint64_t head = bl_head(v.ib);
-    unsigned long long cur = bl_load(h);
     if (bl_unpack(v, cur).state == kBlUninit) {
         const unsigned long long blocked = bl_pack(v, kBlBlocking, head, 0, 0);
-        if (atomicCAS(h, cur, blocked) == cur) {
+        const unsigned long long old = atomicCAS(h, cur, blocked);
+        if (old == cur) {
             /* this thread allocates the first bucket */
             const unsigned long long alloc = bl_alloc(v, v.min_bucket);
             if (alloc + v.min_bucket <= v.capacity) {
@@ -210,12 +215,13 @@ __device__ uint32_t bl_append(const BlView &v, unsigned long long *h, V value)
             atomicExch(h, bl_pack(v, kBlFull, head, 0, 0));
             return kStOutOfMemory;
         }
+        cur = old;
     }
     for (uint32_t spin = 0; spin < kBlSpinLimit; ++spin) {
-        cur = bl_load(h);
         const BlHandle c = bl_unpack(v, cur);
         if (c.state == kBlBlocking || c.state == kBlUninit) {
             __nanosleep(32);
+            cur = bl_load(h);
             continue;
         }
         if (c.state == kBlFull) return kStOutOfMemory;
@@ -224,7 +230,12 @@ __device__ uint32_t bl_append(const BlView &v, unsigned long long *h, V value)
             c.count <= v.min_bucket ? v.min_bucket : bl_header_size(v, bl_load(v.pool + c.index));
         if (c.tail == size) {
             /* the newest bucket is full: block the handle, allocate the next */
-            if (atomicCAS(h, cur, bl_pack(v, kBlBlocking, c.index, c.count, c.tail)) != cur) continue;
+            const unsigned long long old =
+                atomicCAS(h, cur, bl_pack(v, kBlBlocking, c.index, c.count, c.tail));
+            if (old != cur) {
+                cur = old;
+                continue;
+            }
             const float grown = ceilf(float(size) * v.grow);
             const float cap = float(v.max_bucket);
             const uint64_t nsize = uint64_t(cap < grown ? cap : grown);
@@ -239,11 +250,14 @@ __device__ uint32_t bl_append(const BlView &v, unsigned long long *h, V value)
             atomicExch(h, bl_pack(v, kBlFull, c.index, c.count, c.tail));
             return kStOutOfMemory;
         }
-        if (atomicCAS(h, cur, bl_pack(v, kBlInit, c.index, c.count + 1, c.tail + 1)) == cur) {
+        const unsigned long long old =
+            atomicCAS(h, cur, bl_pack(v, kBlInit, c.index, c.count + 1, c.tail + 1));
+        if (old == cur) {
             const uint64_t j = c.count + 1 <= v.min_bucket ? c.tail : c.tail + 1;
             v.pool[c.index + j] = (unsigned long long)value;
             return kStNone;
         }
+        cur = old;
     }
     return kStUnknownError;
 }
@@ -260,8 +274,9 @@ __device__ uint32_t bl_insert_one(const BlView &v, K key, V value, uint64_t max_
     if (slot == ~0ull) return st;
     unsigned long long *const h = v.handles + slot;
     uint32_t ast;
-    if (bl_unpack(v, bl_load(h)).count >= v.max_values) ast = kStMaxValuesReached;
-    else ast = bl_append<V>(v, h, value);
+    const unsigned long long cur = bl_load(h);
+    if (bl_unpack(v, cur).count >= v.max_values) ast = kStMaxValuesReached;
+    else ast = bl_append<V>(v, h, value, cur);
     join |= ast;
     return st | ast;
 }

@@ -395,6 +395,29 @@ def test_counting_block_cache_path(kb, skew):
     assert g.size() == r.size()
 
 
+@pytest.mark.parametrize("kb", [4, 8])
+def test_counting_cache_and_direct_claims_agree(kb):
+    """A counting insert without statuses adds through a per-block cache and
+    straight into the table in the same launch (each block sees more keys
+    than its cache holds). Both paths must claim a window's free slots in
+    the same order, or one key can take two slots and split its count.
+    Every key here appears 4 times; each of them must hold one slot with
+    count 4, on several fresh tables."""
+    import torch
+    distinct = 1 << 19
+    keys = o.gen_unique_keys(kb, distinct, 81)
+    occ = np.repeat(keys, 4)
+    for rep in range(3):
+        perm = np.random.default_rng(90 + rep).permutation(occ.size)
+        t = wc.CountingHashTable(int(distinct / 0.8), key_bytes=kb, cg_size=4)
+        t.insert(dev(occ[perm]))
+        assert t.size() == distinct, rep
+        out = empty_dev(distinct, kb, 0)
+        t.retrieve(dev(keys), out)
+        assert bool((out == 4).all()), rep
+        assert int(t.peek_status()) == o.ST_DUPLICATE_KEY
+
+
 def test_launch_count_counts_this_librarys_kernels():
     # init is one fill kernel; a bulk call on a table without fingerprints
     # is one kernel; a retrieve on a fingerprint table is one kernel too

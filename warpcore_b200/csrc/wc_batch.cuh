@@ -174,7 +174,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs a)
 
             if (pending && claiming) {
                 const BatchDesc &d = a.desc[req];
-                const int s = slot_of_bit<TPK, SPL>(__ffs(claim_bits) - 1);
+                const int s = slot_of_bit<TPK, SPL>(lowest_slot_bit<TPK, SPL>(claim_bits));
                 unsigned char *const sp = reinterpret_cast<unsigned char *>(d.t.slots) +
                                           (bucket * W + uint64_t(s)) * SB;
                 cas_old = cas_slot<L>(sp, empty, claim_expect, key, val, &cas_old_payload);
@@ -240,7 +240,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs a)
             }
             if (did_cas) {
                 const BatchDesc &d = a.desc[req];
-                const int s = slot_of_bit<TPK, SPL>(__ffs(claim_bits) - 1);
+                const int s = slot_of_bit<TPK, SPL>(lowest_slot_bit<TPK, SPL>(claim_bits));
                 unsigned char *const sp = reinterpret_cast<unsigned char *>(d.t.slots) +
                                           (bucket * W + uint64_t(s)) * SB;
                 if (cas_old == empty && cas_old_payload == claim_expect) {
@@ -254,7 +254,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs a)
                 } else if (cas_old == empty) {
                     claim_expect = cas_old_payload;
                 } else {
-                    claim_bits &= claim_bits - 1u;
+                    claim_bits &= ~(1u << lowest_slot_bit<TPK, SPL>(claim_bits));
                     if (!claim_bits) {
                         claiming = false;
                         advance = true;

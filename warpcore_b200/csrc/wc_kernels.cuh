@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
 
             if constexpr (OP == kOpInsert || OP == kOpCount) {
                 if (pending && claiming) {
-                    const int s = slot_of_bit<TPK, SPL>(__ffs(claim_bits) - 1);
+                    const int s = slot_of_bit<TPK, SPL>(lowest_slot_bit<TPK, SPL>(claim_bits));
                     unsigned char *const sp = slots + (bucket * W + uint64_t(s)) * SB;
                     const V payload = OP == kOpCount ? V(cnt_add) : val;
                     cas_old = cas_slot<L>(sp, empty, claim_expect, key, payload, &cas_old_payload);
@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
             }
             if constexpr (OP == kOpInsert || OP == kOpCount) {
                 if (did_cas) {
-                    const int s = slot_of_bit<TPK, SPL>(__ffs(claim_bits) - 1);
+                    const int s = slot_of_bit<TPK, SPL>(lowest_slot_bit<TPK, SPL>(claim_bits));
                     unsigned char *const sp = slots + (bucket * W + uint64_t(s)) * SB;
                     if (cas_old == empty && cas_old_payload == claim_expect) {
                         fp_store(t, bucket * W + uint64_t(s), fingerprint(key));
@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
                         /* free slot with a stale payload: try again on it */
                         claim_expect = cas_old_payload;
                     } else {
-                        claim_bits &= claim_bits - 1u;
+                        claim_bits &= ~(1u << lowest_slot_bit<TPK, SPL>(claim_bits));
                         if (!claim_bits) {
                             claiming = false;
                             advance = true;
