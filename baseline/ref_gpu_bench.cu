@@ -20,6 +20,7 @@
 #include <warpcore/bucket_list_hash_table.cuh>
 
 #include <cfloat>
+#include <cstring>
 #include <cstdint>
 
 namespace wc = warpcore;
@@ -55,10 +56,14 @@ __global__ void set_contains(const typename Set::key_type *keys, uint64_t n, boo
     }
 }
 
+/* After the timed repetitions, `status_out` (if not null) receives the
+ * per-key statuses of one more, untimed retrieve with the ReturnStatus
+ * handler (single_value_hash_table.cuh:318-337), so that the caller can
+ * compare them with its own. */
 template <class Table, class K, class V>
 int run_table(const K *keys, const V *vals, uint64_t n, const K *q, uint64_t nq, V *out,
               uint64_t min_cap, int reps, float *ms_insert, float *ms_retrieve,
-              uint64_t *capacity)
+              uint64_t *capacity, uint32_t *status_out)
 {
     Table t(min_cap);
     *capacity = t.capacity();
@@ -74,6 +79,10 @@ int run_table(const K *keys, const V *vals, uint64_t n, const K *q, uint64_t nq,
         t.retrieve(q, nq, out);
         br = fminf(br, tm.stop());
     }
+    if (status_out)
+        t.template retrieve<wc::status_handlers::ReturnStatus>(
+            q, nq, out, 0, wc::defaults::probing_length(),
+            reinterpret_cast<wc::Status *>(status_out));
     *ms_insert = bi;
     *ms_retrieve = br;
     return int(cudaDeviceSynchronize());
@@ -120,18 +129,18 @@ extern "C" {
 
 int ref_svht64_run(const uint64_t *keys, const uint64_t *vals, uint64_t n, const uint64_t *q,
                    uint64_t nq, uint64_t *out, uint64_t min_cap, int reps, float *ms_insert,
-                   float *ms_retrieve, uint64_t *capacity)
+                   float *ms_retrieve, uint64_t *capacity, uint32_t *status_out)
 {
     return run_table<wc::SingleValueHashTable<uint64_t, uint64_t>>(
-        keys, vals, n, q, nq, out, min_cap, reps, ms_insert, ms_retrieve, capacity);
+        keys, vals, n, q, nq, out, min_cap, reps, ms_insert, ms_retrieve, capacity, status_out);
 }
 
 int ref_svht32_run(const uint32_t *keys, const uint32_t *vals, uint64_t n, const uint32_t *q,
                    uint64_t nq, uint32_t *out, uint64_t min_cap, int reps, float *ms_insert,
-                   float *ms_retrieve, uint64_t *capacity)
+                   float *ms_retrieve, uint64_t *capacity, uint32_t *status_out)
 {
     return run_table<wc::SingleValueHashTable<uint32_t, uint32_t>>(
-        keys, vals, n, q, nq, out, min_cap, reps, ms_insert, ms_retrieve, capacity);
+        keys, vals, n, q, nq, out, min_cap, reps, ms_insert, ms_retrieve, capacity, status_out);
 }
 
 /* HashSet<u64>: the host bulk retrieve does not compile (hash_set.cuh:356),
@@ -163,7 +172,7 @@ int ref_hashset64_run(const uint64_t *keys, uint64_t n, const uint64_t *q, uint6
 
 int ref_counting32_run(const uint32_t *keys, uint64_t n, const uint32_t *q, uint64_t nq,
                        uint32_t *out, uint64_t min_cap, int reps, float *ms_insert,
-                       float *ms_retrieve, uint64_t *capacity)
+                       float *ms_retrieve, uint64_t *capacity, uint32_t *status_out)
 {
     using Table = wc::CountingHashTable<uint32_t, uint32_t>;
     Table t(min_cap);
@@ -180,17 +189,26 @@ int ref_counting32_run(const uint32_t *keys, uint64_t n, const uint32_t *q, uint
         t.retrieve(q, nq, out);
         br = fminf(br, tm.stop());
     }
+    if (status_out)
+        t.template retrieve<wc::status_handlers::ReturnStatus>(
+            q, nq, out, 0, wc::defaults::probing_length(),
+            reinterpret_cast<wc::Status *>(status_out));
     *ms_insert = bi;
     *ms_retrieve = br;
     return int(cudaDeviceSynchronize());
 }
 
+/* BloomFilter<u64, MurmurHash<u64>, u64, 8>.  After the timed repetitions
+ * (each re-initialises the filter, so it ends holding exactly the inserted
+ * keys), `words_out` (if not null, num_slots() words of device memory)
+ * receives the filter's bit vector and *num_slots its length. */
 int ref_bloom64_run(const uint64_t *keys, uint64_t n, const uint64_t *q, uint64_t nq,
                     bool *flags, uint64_t num_bits, uint64_t k, int reps, float *ms_insert,
-                    float *ms_retrieve)
+                    float *ms_retrieve, uint64_t *words_out, uint64_t *num_slots)
 {
     using Filter = wc::BloomFilter<uint64_t, wc::hashers::MurmurHash<uint64_t>, uint64_t, 8>;
     Filter f(num_bits, k);
+    *num_slots = f.num_slots();
     Timer tm;
     float bi = FLT_MAX, br = FLT_MAX;
     for (int r = 0; r < reps; ++r) {
@@ -202,6 +220,13 @@ int ref_bloom64_run(const uint64_t *keys, uint64_t n, const uint64_t *q, uint64_
         tm.start();
         f.retrieve(q, nq, flags);
         br = fminf(br, tm.stop());
+    }
+    if (words_out) {
+        /* BloomFilter keeps its bit vector private and has no accessor; the
+         * device pointer is its first data member (bloom_filter.cuh:410) */
+        uint64_t *words_d = nullptr;
+        std::memcpy(&words_d, &f, sizeof(words_d));
+        cudaMemcpy(words_out, words_d, sizeof(uint64_t) * f.num_slots(), cudaMemcpyDeviceToDevice);
     }
     *ms_insert = bi;
     *ms_retrieve = br;

@@ -19,6 +19,7 @@ oracle code besides the cpu_baseline leg.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -26,11 +27,14 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 MASK64 = (1 << 64) - 1
+KEY_NOT_FOUND = 1 << 5  # Status::key_not_found (status.cuh:44-68)
 
 
 # ---------------------------------------------------------------------------
@@ -190,6 +194,7 @@ class Workload:
             keys = unique_keys32(0, distinct + (distinct >> 2), seed, device)
             self.dkeys = keys[:distinct]
             ranks = zipf_ranks_t(distinct, 1.1, n, gen, device)
+            self.ranks = ranks
             self.keys = self.dkeys[ranks].contiguous()
             self.values = None
             self.queries = keys.contiguous()
@@ -326,15 +331,16 @@ class Workload:
         insert of this workload) holds the right answers"""
         import torch
         if self.kind in ("svht32", "svht64"):
-            return bool(torch.equal(out[self.hit], self.expected[self.hit]))
+            return (bool(torch.equal(out[self.hit], self.expected[self.hit]))
+                    and bool((out[~self.hit] == -1).all()))
         if self.kind == "hashset64":
             return bool((out == self.hit.to(torch.uint8)).all())
         if self.kind == "counting32":
             got = out[: self.distinct].to(torch.int64)
-            present = self.hist > 0
-            return bool(torch.equal(got[present], self.hist[present]))
+            return (bool(torch.equal(got, self.hist))
+                    and bool((out[self.distinct:] == 0).all()))
         if self.kind == "bloom64":
-            return bool(out[self.n:].all())
+            return bool((out[self.n:] == 1).all())
         if self.kind in ("mv32", "mb32", "bl32"):
             return self.mv_ok(self.begin, self.end, out)
         return False
@@ -355,15 +361,28 @@ class Workload:
         return bool(torch.equal(s1, self.exp_sum)) and bool(torch.equal(s2, self.exp_sq))
 
     def verify(self):
-        """size-independent properties of one fresh step"""
+        """size-independent properties of one fresh step; the step's answers
+        stay in self.answers for the exact comparison with the reference
+        build (reference_gpu)"""
         import torch
         s = torch.cuda.current_stream()
         self.init(s)
         self.insert(s)
+        self.answers = {}
         if self.kind in ("svht32", "svht64"):
             self.out.fill_(-1)
-            self.retrieve(s)
+            if self.sharded:
+                self.retrieve(s)
+            else:
+                st = torch.zeros(self.q, dtype=torch.int32, device=self.out.device)
+                self.table.retrieve(self.queries, self.out, stream=s, status_out=st)
+                self.answers["status"] = st
+                if not bool(torch.equal(st != 0, ~self.hit)):
+                    return False
+                if not bool((st[~self.hit] == KEY_NOT_FOUND).all()):
+                    return False
             torch.cuda.synchronize()
+            self.answers["out"] = self.out.clone()
             ok_hits = bool(torch.equal(self.out[self.hit], self.expected[self.hit]))
             ok_miss = bool((self.out[~self.hit] == -1).all())
             ok_size = self.table.size() == self.n * (self.table.world if self.sharded else 1)
@@ -372,19 +391,38 @@ class Workload:
             self.out.fill_(7)
             self.retrieve(s)
             torch.cuda.synchronize()
+            self.answers["out"] = self.out.clone()
             return bool((self.out == self.hit.to(torch.uint8)).all()) and self.table.size() == self.n
         if self.kind == "counting32":
             self.out.fill_(0)
-            self.retrieve(s)
+            st = torch.zeros(self.q, dtype=torch.int32, device=self.out.device)
+            self.table.retrieve(self.queries, self.out, stream=s, status_out=st)
             torch.cuda.synchronize()
+            self.answers["out"] = self.out.clone()
+            self.answers["status"] = st
             got = self.out[: self.distinct].to(torch.int64)
             present = self.hist > 0
-            ok = bool(torch.equal(got[present], self.hist[present]))
-            return ok and bool((self.out[self.distinct:] == 0).all())
+            # the device histogram of the stream against its CPU histogram
+            # (np.bincount over all ranks), then the table against it
+            cpu_hist = np.bincount(self.ranks.cpu().numpy(), minlength=self.distinct)
+            self.cpu_hist_ok = bool(np.array_equal(cpu_hist, self.hist.cpu().numpy()))
+            ok = self.cpu_hist_ok and bool(torch.equal(got[present], self.hist[present]))
+            # keys never drawn and the absent keys: untouched, key_not_found
+            ok = ok and bool((self.out[self.distinct:] == 0).all()) and bool((got[~present] == 0).all())
+            miss = torch.cat([~present, torch.ones(self.q - self.distinct, dtype=torch.bool,
+                                                   device=st.device)])
+            ok = ok and bool(torch.equal(st != 0, miss)) and bool((st[miss] == KEY_NOT_FOUND).all())
+            self.distinct_drawn = int(present.sum())
+            return ok and self.table.size() == self.distinct_drawn
         if self.kind == "bloom64":
+            self.out.fill_(7)
             self.retrieve(s)
             torch.cuda.synchronize()
-            return bool(self.out[self.n:].all())
+            self.answers["out"] = self.out.clone()
+            self.answers["words"] = self.table.words_tensor().clone()
+            # measured false-positive rate: the absent half of the queries
+            self.fpr_measured = float(self.out[: self.n].double().mean())
+            return bool((self.out[self.n:] == 1).all()) and bool((self.out <= 1).all())
         if self.kind in ("mv32", "mb32", "bl32"):
             self.retrieve(s)
             torch.cuda.synchronize()
@@ -414,20 +452,29 @@ def reference_gpu(wl, reps=5):
     out = torch.empty_like(wl.out)
     min_cap = int(wl.n / wl.load) if wl.kind != "counting32" else int(wl.distinct / wl.load)
     rb = re_ = None
+    st = words = None
+    nslots = ctypes.c_uint64(0)
     if wl.kind in ("svht64", "svht32"):
+        # misses must stay untouched: the same fill as our verification run
+        out.fill_(-1)
+        st = torch.zeros(wl.q, dtype=torch.int32, device=out.device)
         fn = lib.ref_svht64_run if wl.kind == "svht64" else lib.ref_svht32_run
         rc = fn(vp(wl.keys.data_ptr()), vp(wl.values.data_ptr()), u64(wl.n),
                 vp(wl.queries.data_ptr()), u64(wl.q), vp(out.data_ptr()), u64(min_cap),
-                ctypes.c_int(reps), ctypes.byref(ti), ctypes.byref(tr), ctypes.byref(cap))
+                ctypes.c_int(reps), ctypes.byref(ti), ctypes.byref(tr), ctypes.byref(cap),
+                vp(st.data_ptr()))
     elif wl.kind == "hashset64":
+        out.fill_(7)
         rc = lib.ref_hashset64_run(vp(wl.keys.data_ptr()), u64(wl.n), vp(wl.queries.data_ptr()),
                                    u64(wl.q), vp(out.data_ptr()), u64(min_cap), ctypes.c_int(reps),
                                    ctypes.byref(ti), ctypes.byref(tr), ctypes.byref(cap))
     elif wl.kind == "counting32":
         out.zero_()
+        st = torch.zeros(wl.q, dtype=torch.int32, device=out.device)
         rc = lib.ref_counting32_run(vp(wl.keys.data_ptr()), u64(wl.n), vp(wl.queries.data_ptr()),
                                     u64(wl.q), vp(out.data_ptr()), u64(min_cap), ctypes.c_int(reps),
-                                    ctypes.byref(ti), ctypes.byref(tr), ctypes.byref(cap))
+                                    ctypes.byref(ti), ctypes.byref(tr), ctypes.byref(cap),
+                                    vp(st.data_ptr()))
     elif wl.kind == "mv32":
         rb, re_ = torch.empty_like(wl.begin), torch.empty_like(wl.end)
         num = ctypes.c_uint64(0)
@@ -453,24 +500,46 @@ def reference_gpu(wl, reps=5):
                               u64(wl.key_cap), u64(wl.value_cap), ctypes.c_int(reps),
                               ctypes.byref(ti), ctypes.byref(tr), ctypes.byref(cap))
     elif wl.kind == "bloom64":
+        out.fill_(7)
+        words = torch.full((wl.table.num_slots(),), -1, dtype=torch.int64, device=out.device)
         rc = lib.ref_bloom64_run(vp(wl.keys.data_ptr()), u64(wl.n), vp(wl.queries.data_ptr()),
                                  u64(wl.q), vp(out.data_ptr()), u64(16 * wl.n), u64(8),
-                                 ctypes.c_int(reps), ctypes.byref(ti), ctypes.byref(tr))
+                                 ctypes.c_int(reps), ctypes.byref(ti), ctypes.byref(tr),
+                                 vp(words.data_ptr()), ctypes.byref(nslots))
     else:
         return None
     torch.cuda.synchronize()
     if rc != 0:
         return {"error": "CUDA error %d" % rc}
     # the reference's answers on the same inputs must equal ours
-    same = wl.mv_ok(rb, re_, out) if wl.kind in ("mv32", "mb32", "bl32") else wl.answers_ok(out)
+    compared = {}
+    if wl.kind in ("mv32", "mb32", "bl32"):
+        same = wl.mv_ok(rb, re_, out)
+    else:
+        ans = getattr(wl, "answers", {})
+        same = wl.answers_ok(out)
+        if "out" in ans:
+            # every output element, misses included (same fill before the call)
+            compared["outputs"] = bool(torch.equal(out, ans["out"]))
+        if st is not None and "status" in ans:
+            compared["statuses"] = bool(torch.equal(st, ans["status"]))
+        if words is not None:
+            ours = wl.table.words_tensor()
+            compared["filter_words"] = int(nslots.value)
+            compared["words_equal"] = (int(nslots.value) == ours.numel()
+                                       and bool(torch.equal(words, ours)))
+        same = same and all(v for k, v in compared.items() if k != "filter_words")
     ins_g = wl.n / (ti.value * 1e-3) / 1e9
     ret_g = wl.q / (tr.value * 1e-3) / 1e9
-    return {"insert_gops": round(ins_g, 4), "retrieve_gops": round(ret_g, 4),
-            "value": round((wl.n + wl.q) / ((ti.value + tr.value) * 1e-3) / 1e9, 4),
-            "insert_ms": round(ti.value, 4), "retrieve_ms": round(tr.value, 4),
-            "capacity": int(cap.value) if cap.value else None, "reps": reps,
-            "timing": "cudaEvent min of %d on the reference's own bulk methods" % reps,
-            "same_answers": same}
+    r = {"insert_gops": round(ins_g, 4), "retrieve_gops": round(ret_g, 4),
+         "value": round((wl.n + wl.q) / ((ti.value + tr.value) * 1e-3) / 1e9, 4),
+         "insert_ms": round(ti.value, 4), "retrieve_ms": round(tr.value, 4),
+         "capacity": int(cap.value) if cap.value else None, "reps": reps,
+         "timing": "cudaEvent min of %d on the reference's own bulk methods" % reps,
+         "same_answers": same}
+    if compared:
+        r["compared"] = compared
+    return r
 
 
 WORKLOAD_NAMES = {
@@ -645,10 +714,39 @@ def run_ours(args):
             "clocks": clocks,
             "wall_s": round(wall, 3),
         }
+        if wl.kind == "bloom64":
+            line["fpr"] = bloom_fpr_report(wl)
+        if wl.kind == "counting32":
+            line["config"]["distinct_keys"] = wl.distinct
+            line["config"]["distinct_drawn"] = getattr(wl, "distinct_drawn", None)
+            line["cpu_histogram_equal"] = getattr(wl, "cpu_hist_ok", None)
         print(json.dumps(line), flush=True)
     if world > 1 or args.shard:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def bloom_fpr_report(wl):
+    """False-positive rate of the filter after the step's inserts: measured
+    on the absent half of the queries, beside the reference's estimator
+    (bloom_filter.cuh:342-408).  The library's fpr() follows the reference
+    literally and overflows to NaN at this size (its binomial coefficient is
+    a product of n factors); the same sum is evaluated here with log-space
+    binomial probabilities."""
+    from scipy.stats import binom
+    nb = int(wl.table.num_blocks())
+    m = int(wl.table.num_bits()) // nb          # bits per block
+    k = int(wl.table.k())
+    n = wl.n
+    i = np.arange(0, 5 * n // nb)
+    base = (1.0 - np.power(1.0 - 1.0 / m, i * k)) ** k
+    est = float(np.sum(binom.pmf(i, n, 1.0 / nb) * base))
+    lib_fpr = wl.table.fpr(n)
+    return {"measured": getattr(wl, "fpr_measured", None),
+            "absent_queries": wl.n,
+            "estimate": est,
+            "estimate_how": "the reference's pattern-blocked estimator, log-space binomials",
+            "library_fpr_call": None if math.isnan(lib_fpr) else lib_fpr}
 
 
 def run_e2e(wl, stream, args, world):
@@ -984,7 +1082,7 @@ def main():
     if args.log2n is None:
         args.log2n = 24 if args.workload == "mv32" else 27
     if args.load is None:
-        args.load = 0.8 if args.workload in ("mv32", "mb32") else 0.9
+        args.load = {"mv32": 0.8, "mb32": 0.8, "counting32": 0.85}.get(args.workload, 0.9)
     if args.warmup < 3:
         log("warm-up raised to 3 steps")
         args.warmup = 3

@@ -332,11 +332,14 @@ struct AoSStore {
     using value_type = Value;
     using tag = tags::key_value_storage;
 };
-/* SoAStore (storage.cuh:218-432): accepted wherever AoSStore is.  It names
- * the same key and value types; the tables choose their own layout in HBM
- * (single-value tables keep {key, value} slots so that one compare-and-swap
- * publishes both; the multi-bucket and bucket-list tables keep keys apart
- * from values), so answers do not depend on this parameter. */
+/* SoAStore (storage.cuh:218-432): accepted wherever AoSStore is, as a
+ * type, but it does NOT select a struct-of-arrays layout.  It names the same
+ * key and value types; the tables choose their own layout in HBM whichever
+ * store is named (single-value tables, sets and counters keep {key, value}
+ * slots so that one compare-and-swap publishes both; the multi-bucket and
+ * bucket-list tables keep keys apart from values).  Answers do not depend on
+ * this parameter; code that relies on the SoA layout's memory (reading a
+ * separate key array through the table's storage) is not supported. */
 template <class Key, class Value>
 struct SoAStore {
     using key_type = Key;

@@ -554,6 +554,23 @@ int wc_fingerprint_policy(int mode, int *previous);
 int wc_fingerprint_ops(uint32_t op_mask, uint32_t *previous);
 
 /* ------------------------------------------------------------------ */
+/* Region passes (no counterpart in the reference)                       */
+/* ------------------------------------------------------------------ */
+
+/* Random reads on B200 slow down sharply once the array they hit outgrows
+ * the GPU's address-translation reach (64-byte reads at random: 64 G/s over
+ * 256 MiB, 13.5 G/s over 512 MiB).  A Bloom filter with blocks of at most
+ * 128 bytes whose words exceed the region size of the operation is inserted
+ * into (WC_REGION_INSERT, default 128 MiB) or queried (WC_REGION_QUERY,
+ * default 256 MiB) in passes, each streaming all keys and serving those
+ * whose block lies in one region of the filter.  0 = always one pass;
+ * otherwise 1 MiB .. 1 TiB.  Applies to later calls (*previous gets the old
+ * value).  Results do not depend on it. */
+#define WC_REGION_INSERT 0
+#define WC_REGION_QUERY 1
+int wc_region_bytes(int op, uint64_t bytes, uint64_t *previous);
+
+/* ------------------------------------------------------------------ */
 /* L2 persistence for tables that fit in L2 (no counterpart in the       */
 /* reference)                                                            */
 /* ------------------------------------------------------------------ */
@@ -717,15 +734,20 @@ int wc_partition_restore(const void *values, const uint32_t *status, const uint6
  * empty_key nor tombstone_key) of a slot array in this library's layout
  * (key_bytes 4 or 8; value_bytes 0 for a hash set, else equal to key_bytes)
  * and writes the count to *size_out, a DEVICE pointer to one uint64, on
- * `stream`, without allocating any device memory.  It is meant for callers
+ * `stream`, without allocating any device memory.  A key-only array (a hash
+ * set's slots, or the separate key array of a multi-bucket or bucket-list
+ * table, whose wc_table_info reports value_bytes equal to key_bytes) must be
+ * passed with value_bytes 0: the 8- or 16-byte key+value layout would count
+ * it wrongly.  It is meant for callers
  * that hold a table's slots without a handle of this library and may not
  * allocate: e.g. a process that received the table's memory through CUDA
  * IPC, or a plugin whose host framework owns all device memory.  Scratch is
  * a fixed 512 KiB array inside the library (held by every GPU that loads
  * it); slot arrays above WC_NOALLOC_MAX_SLOTS are rejected with
  * WC_ERR_INVALID_ARGUMENT.  All calls share that array, so calls that
- * overlap on the GPU race; the first call on each device resolves the
- * array's address and should come before any stream capture.  `slots` must
+ * overlap on the GPU race.  Every call looks the array's address up in the
+ * current context (the first call on a device loads it there and should come
+ * before any stream capture).  `slots` must
  * be 16-byte aligned (wc_table_get_info's `slots` is). */
 int wc_slots_size_noalloc(const void *slots, uint64_t capacity, uint32_t key_bytes,
                           uint32_t value_bytes, uint64_t empty_key,

@@ -41,6 +41,34 @@ def test_bloom_words_and_flags(kb, sb, cg, num_bits, k, n):
     assert got[:n].all()  # no false negatives
 
 
+@pytest.mark.parametrize("kb,sb,cg,num_bits,k,n,region", [
+    (8, 8, 8, 1 << 25, 8, 1 << 21, 1 << 20),              # 4 passes of 2^14 blocks
+    (8, 8, 8, (1 << 25) + 512 * 3 + 64, 8, 1 << 20, 1 << 20),  # ragged last block
+    (4, 4, 4, 3 << 23, 5, 1 << 19, 1 << 20),              # 16-byte blocks, 3 passes
+    (8, 4, 16, (1 << 24) + 4096, 7, 1 << 18, 1 << 20),    # 3 uneven passes
+])
+def test_bloom_region_passes(kb, sb, cg, num_bits, k, n, region):
+    """A filter larger than the random-access region runs in region passes;
+    words and flags must not change."""
+    prev = wc.set_region_bytes(region)
+    try:
+        f = wc.BloomFilter(num_bits, k, key_bytes=kb, slot_bytes=sb, cg_size=cg)
+        allk = o.gen_unique_keys(kb, 2 * n, 78)
+        keys = allk[:n]
+        f.insert(dev(keys))
+        flags = empty_dev(2 * n, 1, 9)
+        f.retrieve(dev(allk), flags)
+    finally:
+        wc.set_region_bytes(prev)
+    assert f.num_slots() * sb > region  # more than one pass ran
+    r = o.Bloom(num_bits, k, key_bytes=kb, slot_bytes=sb, cg=cg)
+    r.insert(keys)
+    assert np.array_equal(words_of(f, sb), r.words())
+    got = host(flags)
+    assert np.array_equal(got, r.retrieve(allk))
+    assert got[:n].all()
+
+
 def test_bloom_config4_shape_fpr():
     # the filter shape of the 2^32-bit configuration at a reduced key count
     f = wc.BloomFilter(1 << 32, 8, key_bytes=8, slot_bytes=8, cg_size=8)

@@ -265,3 +265,34 @@ def test_sharded_set_counting_bloom_one_rank_nccl():
         assert np.array_equal(bfl.cpu().numpy().astype(np.uint8), rb.retrieve(q))
     finally:
         dist.destroy_process_group()
+
+
+def test_bloom_shards_in_region_passes():
+    """shards larger than the random-access region run in region passes over
+    their own blocks; words and flags stay the whole filter's slices"""
+    kb, sb, cg = 8, 8, 8
+    bits = 1 << 26                      # 8 MiB: 3 shards of about 2.7 MiB
+    k, seed, parts, n = 6, 0x77, 3, 1 << 19
+    keys = o.gen_unique_keys(kb, 2 * n, 43)
+    ref = o.Bloom(bits, k, seed=seed, key_bytes=kb, slot_bytes=sb, cg=cg)
+    ref.insert(keys[:n])
+    words = ref.words()
+    want_flags = ref.retrieve(keys)
+    nb = bits // (64 * cg)
+    blk = bloom_block_np(keys, seed, nb).astype(np.int64)
+    prev = wc.set_region_bytes(1 << 20)
+    try:
+        for s in range(parts):
+            sh = wc.BloomFilter(bits, k, seed=seed, key_bytes=kb, slot_bytes=sb, cg_size=cg,
+                                shard=s, num_shards=parts)
+            lo, hi = bloom_shard_range(nb, s, parts)
+            assert (hi - lo) * cg * sb > 2 << 20   # at least 3 passes
+            sh.insert(dev(keys[:n]))
+            got = copy_device_words(sh.words_ptr(), (hi - lo) * cg, sb)
+            assert np.array_equal(got, words[lo * cg:hi * cg])
+            fl = torch.full((2 * n,), 9, dtype=torch.uint8, device="cuda")
+            sh.retrieve(dev(keys), fl)
+            mine = (blk >= lo) & (blk < hi)
+            assert np.array_equal(fl.cpu().numpy(), np.where(mine, want_flags, 0))
+    finally:
+        wc.set_region_bytes(prev)

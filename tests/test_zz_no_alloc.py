@@ -79,3 +79,58 @@ def test_empty_slot_array_counts_zero():
                                         torch.cuda.current_stream().cuda_stream, out.data_ptr())
     assert rc == 0
     assert int(out.item()) == 0
+
+
+def noalloc_count(slots, capacity, key_bytes, value_bytes, empty, tomb):
+    import torch
+    out = torch.full((1,), -1, dtype=torch.int64, device="cuda")
+    rc = wc.lib().wc_slots_size_noalloc(slots, capacity, key_bytes, value_bytes, empty, tomb,
+                                        torch.cuda.current_stream().cuda_stream, out.data_ptr())
+    assert rc == 0, wc.lib().wc_last_error()
+    return int(out.item())
+
+
+@pytest.mark.parametrize("kind,kb", [("svht", 4), ("set", 4), ("set", 8)])
+def test_ragged_prefix_against_host_count(kind, kb):
+    """A prefix of 2^18 + 3 slots of a larger table: the last chunk holds 3
+    slots, fewer than one 16-byte load for 4-byte set keys, and not a
+    multiple of the slots per load for 8-byte slots; the count must equal a
+    host count of the same slots copied back."""
+    from tests.wc_helpers import copy_device_words
+    n = 400000
+    t = (wc.SingleValueHashTable(n, key_bytes=kb, cg_size=1) if kind == "svht"
+         else wc.HashSet(n, key_bytes=kb, cg_size=1))
+    keys = o.gen_unique_keys(kb, n // 2, 97)
+    if kind == "svht":
+        t.insert(dev(keys), dev(o.gen_uniform(kb, n // 2, 96)))
+    else:
+        t.insert(dev(keys))
+    t.erase(dev(keys[::5]))
+    inf = t.info()
+    prefix = (1 << 18) + 3
+    assert inf.capacity > prefix
+    vb = 0 if kind == "set" else kb
+    slot_bytes = kb + vb
+    words = copy_device_words(inf.slots, prefix * slot_bytes // kb, kb)
+    host_keys = words[:: slot_bytes // kb]
+    expect = int(((host_keys != inf.empty_key) & (host_keys != inf.tombstone_key)).sum())
+    assert 0 < expect < prefix
+    for _ in range(2):
+        assert noalloc_count(inf.slots, prefix, kb, vb, inf.empty_key, inf.tombstone_key) == expect
+
+
+def test_multi_bucket_key_array_counted_as_keys_only():
+    """The multi-bucket table keeps its keys in an array of their own, and
+    its info reports value_bytes equal to key_bytes.  Passed with
+    value_bytes 0, the key array counts exactly the table's keys."""
+    n = 50000
+    t = wc.MultiBucketHashTable(4 * n, key_bytes=4, bucket_size=2)
+    keys = o.gen_unique_keys(4, n, 95)
+    vals = o.gen_uniform(4, n, 94)
+    vals[vals == 0] = 1
+    t.insert(dev(keys), dev(vals))
+    inf = t.info()
+    assert inf.value_bytes == inf.key_bytes
+    got = noalloc_count(inf.keys, inf.capacity, inf.key_bytes, 0, inf.empty_key,
+                        inf.tombstone_key)
+    assert got == t.num_keys() == n

@@ -277,6 +277,7 @@ SIGNATURES = {
     "wc_table_insert_host": (_i, [_vp, _vp, _vp, _vp, _u64, _vp, _u64]),
     "wc_table_retrieve_host": (_i, [_vp, _vp, _vp, _u64, _vp, _vp, _vp, _u64]),
     "wc_l2_persistence": (_i, [_i, ctypes.POINTER(ctypes.c_int)]),
+    "wc_region_bytes": (_i, [_i, _u64, ctypes.POINTER(ctypes.c_uint64)]),
     "wc_fingerprint_policy": (_i, [_i, ctypes.POINTER(ctypes.c_int)]),
     "wc_fingerprint_ops": (_i, [_u32, ctypes.POINTER(ctypes.c_uint32)]),
     "wc_launch_count": (_i, [ctypes.POINTER(_u64)]),
@@ -388,6 +389,22 @@ def set_fingerprint_policy(mode):
     prev = ctypes.c_int(0)
     _check(lib().wc_fingerprint_policy(m, ctypes.byref(prev)))
     return prev.value
+
+
+def set_region_bytes(nbytes, op=None):
+    """Random-access region of the multi-pass kernels: a Bloom filter
+    larger than this is inserted into (op "insert", default 128 MiB) or
+    queried (op "query", default 256 MiB) in passes, one region of its blocks
+    per pass; 0 = always one pass.  `nbytes` is one value for both, or a
+    pair (insert, query); op=None sets both.  Returns the previous value(s)
+    in the same form."""
+    ops = {"insert": 0, "query": 1}
+    if op is not None:
+        prev = ctypes.c_uint64(0)
+        _check(lib().wc_region_bytes(ops[op], int(nbytes), ctypes.byref(prev)))
+        return prev.value
+    vals = nbytes if isinstance(nbytes, (tuple, list)) else (nbytes, nbytes)
+    return tuple(set_region_bytes(v, o) for v, o in zip(vals, ("insert", "query")))
 
 
 def gen_uniform(out, seed, stream=None):
@@ -1172,6 +1189,21 @@ class BloomFilter:
 
     def words_ptr(self):
         return self.info().words
+
+    def words_tensor(self):
+        """The words this object holds (local_blocks x cg_size of them) as a
+        torch tensor viewing the filter's device memory, int32 or int64
+        holding the unsigned bit patterns.  The view does not own the memory:
+        it is valid while the filter lives and is not re-created."""
+        import torch
+        inf = self.info()
+        count = int(inf.local_blocks) * int(inf.cg_size)
+
+        class _DeviceWords:
+            __cuda_array_interface__ = {
+                "shape": (count,), "typestr": "<i%d" % inf.slot_bytes,
+                "data": (int(inf.words or 0), False), "version": 3, "strides": None}
+        return torch.as_tensor(_DeviceWords(), device="cuda")
 
     def init(self, seed=None, stream=None):
         _check(lib().wc_bloom_init(self._h, int(self.info().seed if seed is None else seed),

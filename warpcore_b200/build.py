@@ -79,8 +79,7 @@ def build(jobs=None, force=False, verbose=False):
             for f in futs:
                 logs.append(f.result())
     if force or todo or not _newer(LIB, objs):
-        _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcuda"] if False else
-             [nvcc] + ARCH + ["-shared", "-o", LIB] + objs)
+        _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs)
     if verbose:
         for l in logs:
             sys.stdout.write(l)

@@ -10,36 +10,51 @@ namespace b200 {
 #define WC_BLOOM_LANE 1
 #endif
 
-template <class K, class S, int CG>
-static BloomKernel pick_bloom(bool insert)
+/* a single pass runs the one-key-per-lane kernel, region passes the
+ * compacting region kernel */
+template <class K, class S, int CG, bool INSERT>
+static BloomKernel pick_lane(bool multi_pass)
 {
-    if constexpr (WC_BLOOM_LANE && CG * sizeof(S) <= 128)
-        return insert ? bloom_lane_kernel<K, S, CG, true> : bloom_lane_kernel<K, S, CG, false>;
-    else
+    return multi_pass ? bloom_region_kernel<K, S, CG, INSERT> : bloom_lane_kernel<K, S, CG, INSERT>;
+}
+
+template <class K, class S, int CG>
+static BloomKernel pick_bloom(bool insert, bool multi_pass, bool *lane)
+{
+    if constexpr (WC_BLOOM_LANE && CG * sizeof(S) <= 128) {
+        *lane = true;
+        return insert ? pick_lane<K, S, CG, true>(multi_pass) : pick_lane<K, S, CG, false>(multi_pass);
+    } else {
+        *lane = false;
         return insert ? bloom_kernel<K, S, CG, true> : bloom_kernel<K, S, CG, false>;
+    }
 }
 
 template <class K, class S>
-static BloomKernel pick_bloom_cg(int cg, bool insert)
+static BloomKernel pick_bloom_cg(int cg, bool insert, bool multi_pass, bool *lane)
 {
     switch (cg) {
-    case 1: return pick_bloom<K, S, 1>(insert);
-    case 2: return pick_bloom<K, S, 2>(insert);
-    case 4: return pick_bloom<K, S, 4>(insert);
-    case 8: return pick_bloom<K, S, 8>(insert);
-    case 16: return pick_bloom<K, S, 16>(insert);
-    case 32: return pick_bloom<K, S, 32>(insert);
+    case 1: return pick_bloom<K, S, 1>(insert, multi_pass, lane);
+    case 2: return pick_bloom<K, S, 2>(insert, multi_pass, lane);
+    case 4: return pick_bloom<K, S, 4>(insert, multi_pass, lane);
+    case 8: return pick_bloom<K, S, 8>(insert, multi_pass, lane);
+    case 16: return pick_bloom<K, S, 16>(insert, multi_pass, lane);
+    case 32: return pick_bloom<K, S, 32>(insert, multi_pass, lane);
     default: return nullptr;
     }
 }
 
-BloomKernel bloom_kernel_ptr(int key_bytes, int slot_bytes, int cg, bool insert)
+BloomKernel bloom_kernel_ptr(int key_bytes, int slot_bytes, int cg, bool insert, bool multi_pass,
+                             bool *lane_kernel)
 {
-    if (key_bytes == 4 && slot_bytes == 4) return pick_bloom_cg<uint32_t, uint32_t>(cg, insert);
-    if (key_bytes == 4 && slot_bytes == 8) return pick_bloom_cg<uint32_t, uint64_t>(cg, insert);
-    if (key_bytes == 8 && slot_bytes == 4) return pick_bloom_cg<uint64_t, uint32_t>(cg, insert);
-    if (key_bytes == 8 && slot_bytes == 8) return pick_bloom_cg<uint64_t, uint64_t>(cg, insert);
-    return nullptr;
+    bool lane = false;
+    BloomKernel k = nullptr;
+    if (key_bytes == 4 && slot_bytes == 4) k = pick_bloom_cg<uint32_t, uint32_t>(cg, insert, multi_pass, &lane);
+    if (key_bytes == 4 && slot_bytes == 8) k = pick_bloom_cg<uint32_t, uint64_t>(cg, insert, multi_pass, &lane);
+    if (key_bytes == 8 && slot_bytes == 4) k = pick_bloom_cg<uint64_t, uint32_t>(cg, insert, multi_pass, &lane);
+    if (key_bytes == 8 && slot_bytes == 8) k = pick_bloom_cg<uint64_t, uint64_t>(cg, insert, multi_pass, &lane);
+    if (lane_kernel) *lane_kernel = lane;
+    return k;
 }
 
 CountKernel count_kernel(int layout)

@@ -37,6 +37,11 @@ struct BloomArgs {
      * skipped (insert) or reported absent (query) */
     uint64_t block_base;
     uint64_t local_blocks;
+    /* this launch serves only the keys whose local block lies in
+     * [region_lo, region_hi) (bloom_lane_kernel; see region passes below);
+     * region_lo == 0 also answers the keys of other shards */
+    uint64_t region_lo;
+    uint64_t region_hi;
 };
 
 template <class S>
@@ -193,7 +198,8 @@ __global__ void __launch_bounds__(256) bloom_kernel(const BloomArgs a)
  * key's masks, reads its own block with BB / 16 vector loads (all lanes'
  * loads independent, so a warp keeps 32 blocks in flight), tests it, and
  * ORs only the words that miss bits.  Against the cooperative kernel above
- * it spends no shuffles on block indices and masks. */
+ * it spends no shuffles on block indices and masks.  It serves the keys
+ * whose block lies in [region_lo, region_hi) (one pass: the whole filter). */
 template <class K, class S, int CG, bool INSERT>
 __global__ void __launch_bounds__(256) bloom_lane_kernel(const BloomArgs a)
 {
@@ -214,9 +220,12 @@ __global__ void __launch_bounds__(256) bloom_lane_kernel(const BloomArgs a)
             fast_mod(hash_key<K>(a.hasher, K(key + seed)), a.num_blocks, a.magic_blocks) -
             a.block_base;
         if (blk >= a.local_blocks) {
-            if constexpr (!INSERT) a.flags_out[i] = 0;
+            if constexpr (!INSERT) {
+                if (a.region_lo == 0) a.flags_out[i] = 0;
+            }
             continue;
         }
+        if (blk < a.region_lo || blk >= a.region_hi) continue;
         S m[CG];
         block_masks<K, S, CG>(key, seed, a.hasher, a.k, m);
         const uint64_t w0 = blk * CG;
@@ -251,6 +260,133 @@ __global__ void __launch_bounds__(256) bloom_lane_kernel(const BloomArgs a)
             }
         }
         if constexpr (!INSERT) a.flags_out[i] = (unsigned char)ok;
+    }
+}
+
+/* Region passes, for blocks of at most 128 bytes.  On B200, random reads
+ * slow down sharply once the array they hit outgrows the GPU's
+ * address-translation reach: 64-byte reads at random measured 64 G/s over
+ * 256 MiB but 13.5 G/s over 512 MiB and 9.5 G/s over 4 GiB.  A filter
+ * larger than one region is therefore processed in passes, one launch per
+ * region of its blocks; each pass streams all keys and serves those whose
+ * block lies in its region, so that its random reads (and an insert's
+ * atomics) stay inside the region.
+ *
+ * A pass must keep many block reads in flight although only a fraction of
+ * the keys it streams belongs to its region.  So a warp takes a tile of
+ * kRegionKpl x 32 keys (kRegionKpl coalesced loads per lane in flight),
+ * computes their blocks, and compacts the keys of its region into a list
+ * in shared memory (ballot + prefix count, input order kept).  The lanes
+ * then take the list densely, kRegionU entries per lane at a time, issue
+ * all their block reads before testing any, and write flags / OR words as
+ * the one-key-per-lane kernel does.  Each key is served by exactly one
+ * pass; a query's flag is written there (a key of another shard's block
+ * gets 0 in the first pass). */
+constexpr int kRegionKpl = 8;   /* keys per lane per warp tile */
+constexpr int kRegionU = 4;     /* compacted keys per lane in flight */
+constexpr int kRegionWarps = 8; /* 256 threads */
+
+template <class K, class S, int CG, bool INSERT>
+__global__ void __launch_bounds__(256) bloom_region_kernel(const BloomArgs a)
+{
+    constexpr int SB = sizeof(S);
+    constexpr int BB = CG * SB;
+    constexpr int VB = BB < 16 ? BB : 16;
+    constexpr int NV = BB / VB;
+    constexpr int WPV = VB / SB;
+    constexpr int WT = 32 * kRegionKpl; /* keys per warp tile */
+    static_assert(BB <= 128 && NV * VB == BB && WPV * SB == VB, "block split");
+    static_assert(WT <= 256, "tile offsets are one byte");
+    constexpr bool kRead = !INSERT || WC_BLOOM_INSERT_READS_BLOCK;
+
+    __shared__ K s_key[kRegionWarps][WT];
+    __shared__ uint32_t s_rel[kRegionWarps][WT];       /* block - region_lo */
+    __shared__ unsigned char s_off[kRegionWarps][WT];  /* position in the tile */
+
+    S *const words = reinterpret_cast<S *>(a.words);
+    const K *const keys = reinterpret_cast<const K *>(a.keys);
+    const K seed = K(a.seed);
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const unsigned lanemask_lt = (1u << lane) - 1u;
+    const uint64_t gwarp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+
+    for (uint64_t base = gwarp * WT; base < a.n; base += nwarps * WT) {
+        K kk[kRegionKpl];
+#pragma unroll
+        for (int j = 0; j < kRegionKpl; ++j) {
+            const uint64_t i = base + uint64_t(j) * 32 + lane;
+            kk[j] = i < a.n ? ld_stream(keys + i) : K(0);
+        }
+        int cnt = 0;
+#pragma unroll
+        for (int j = 0; j < kRegionKpl; ++j) {
+            const uint64_t i = base + uint64_t(j) * 32 + lane;
+            const uint64_t blk =
+                fast_mod(hash_key<K>(a.hasher, K(kk[j] + seed)), a.num_blocks, a.magic_blocks) -
+                a.block_base;
+            if constexpr (!INSERT) {
+                if (i < a.n && a.region_lo == 0 && blk >= a.local_blocks) a.flags_out[i] = 0;
+            }
+            const bool in = i < a.n && blk < a.local_blocks && blk >= a.region_lo &&
+                            blk < a.region_hi;
+            const unsigned m = __ballot_sync(kFull, in);
+            if (in) {
+                const int pos = cnt + __popc(m & lanemask_lt);
+                s_key[wib][pos] = kk[j];
+                s_rel[wib][pos] = uint32_t(blk - a.region_lo);
+                s_off[wib][pos] = (unsigned char)(j * 32 + lane);
+            }
+            cnt += __popc(m);
+        }
+        __syncwarp();
+        for (int e0 = 0; e0 < cnt; e0 += 32 * kRegionU) {
+            S w[kRegionU][CG];
+#pragma unroll
+            for (int u = 0; u < kRegionU; ++u) {
+                const int e = e0 + u * 32 + lane;
+                if (kRead && e < cnt) {
+                    const uint64_t w0 = (a.region_lo + s_rel[wib][e]) * CG;
+                    if (w0 + CG <= a.num_slots) {
+#pragma unroll
+                        for (int v = 0; v < NV; ++v) {
+                            const LaneWords lw = load_lane<VB>(words + w0 + uint64_t(v) * WPV);
+#pragma unroll
+                            for (int s = 0; s < WPV; ++s) w[u][v * WPV + s] = lane_word<S>(lw, s);
+                        }
+                    } else {
+#pragma unroll
+                        for (int s = 0; s < CG; ++s) w[u][s] = __ldcg(words + (w0 + s) % a.num_slots);
+                    }
+                } else {
+#pragma unroll
+                    for (int s = 0; s < CG; ++s) w[u][s] = 0;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kRegionU; ++u) {
+                const int e = e0 + u * 32 + lane;
+                if (e >= cnt) continue;
+                const K key = s_key[wib][e];
+                const uint64_t w0 = (a.region_lo + s_rel[wib][e]) * CG;
+                S m[CG];
+                block_masks<K, S, CG>(key, seed, a.hasher, a.k, m);
+                bool ok = true;
+#pragma unroll
+                for (int s = 0; s < CG; ++s) {
+                    const bool missing = (w[u][s] & m[s]) != m[s];
+                    ok &= !missing;
+                    if (INSERT && m[s] && (!kRead || missing)) {
+                        uint64_t wi = w0 + uint64_t(s);
+                        if (wi >= a.num_slots) wi -= a.num_slots;
+                        atomic_or_any(words + wi, m[s]);
+                    }
+                }
+                if constexpr (!INSERT) a.flags_out[base + s_off[wib][e]] = (unsigned char)ok;
+            }
+        }
+        __syncwarp();
     }
 }
 

@@ -142,6 +142,23 @@ std::atomic<int> g_fp_mode{-1}; /* -1: not yet read from the environment */
  * (11.7 G/s), so every operation reads fingerprints first. */
 std::atomic<uint32_t> g_fp_ops{0xFu};
 
+/* Random-access regions of the multi-pass kernels, for inserts and for
+ * queries (bytes; 0 = one pass).  Random 64-byte reads on B200 measured
+ * 64 G/s over 256 MiB, 19 G/s over 320 MiB and 13.5 G/s over 512 MiB, so a
+ * query pass works on at most 256 MiB.  An insert pass also ORs words:
+ * Bloom inserts into 128 MiB regions (about L2's size) ran 26.8 G keys/s
+ * against 16.0 into 256 MiB regions. */
+std::atomic<uint64_t> g_region_bytes[2] = {{128ull << 20}, {256ull << 20}};
+
+} // namespace
+
+uint64_t warpcore::b200::region_bytes(bool insert)
+{
+    return g_region_bytes[insert ? 0 : 1].load(std::memory_order_relaxed);
+}
+
+namespace {
+
 int fp_mode()
 {
     int m = g_fp_mode.load(std::memory_order_relaxed);
@@ -1197,6 +1214,17 @@ int wc_fingerprint_policy(int mode, int *previous)
     return WC_OK;
 }
 
+int wc_region_bytes(int op, uint64_t bytes, uint64_t *previous)
+{
+    if (op != WC_REGION_INSERT && op != WC_REGION_QUERY)
+        return fail(WC_ERR_INVALID_ARGUMENT, "unknown region operation %d", op);
+    if (bytes && (bytes < (1ull << 20) || bytes > (1ull << 40)))
+        return fail(WC_ERR_INVALID_ARGUMENT, "region must be 0 (one pass) or 1 MiB .. 1 TiB");
+    const uint64_t prev = g_region_bytes[op == WC_REGION_INSERT ? 0 : 1].exchange(bytes);
+    if (previous) *previous = prev;
+    return WC_OK;
+}
+
 /* ---- launch tuning ---- */
 
 int wc_l2_persistence(int enable, int *previous)
@@ -1342,9 +1370,22 @@ static int bloom_op(wc_bloom *b, const void *keys, uint64_t n, uint8_t *flags, w
     if (n == 0) return WC_OK;
     if (!keys) return fail(WC_ERR_INVALID_ARGUMENT, "keys_in is NULL");
     if (!insert && !flags) return fail(WC_ERR_INVALID_ARGUMENT, "flags_out is NULL");
+    /* a filter whose words outgrow one random-access region runs in region
+     * passes (bloom_lane_kernel): pass r serves the keys of blocks
+     * [r * local_blocks / R, (r + 1) * local_blocks / R) */
+    const uint64_t block_bytes = uint64_t(b->cfg.cg_size) * b->cfg.slot_bytes;
+    const uint64_t fbytes = b->local_blocks * block_bytes;
+    const uint64_t rb = region_bytes(insert);
+    uint64_t passes = rb ? (fbytes + rb - 1) / rb : 1;
+    if (passes < 1) passes = 1;
+    /* the region kernel keeps a block's offset in its region in 32 bits */
+    const uint64_t min_passes = (b->local_blocks >> 31) + 1;
+    if (passes > 1 && passes < min_passes) passes = min_passes;
+    bool lane = false;
     BloomKernel k = bloom_kernel_ptr(int(b->cfg.key_bytes), int(b->cfg.slot_bytes),
-                                     int(b->cfg.cg_size), insert);
+                                     int(b->cfg.cg_size), insert, passes > 1, &lane);
     if (!k) return fail(WC_ERR_UNSUPPORTED, "no kernel for this configuration");
+    if (!lane) passes = 1;
     BloomArgs a;
     a.words = b->words;
     a.keys = keys;
@@ -1360,8 +1401,12 @@ static int bloom_op(wc_bloom *b, const void *keys, uint64_t n, uint8_t *flags, w
     a.local_blocks = b->local_blocks;
     const unsigned grid = grid_for(reinterpret_cast<const void *>(k), kBlock, n, kBlock);
     void *args[] = {&a};
-    WC_CUDA(launch_in_window(reinterpret_cast<const void *>(k), grid, kBlock, args,
-                             reinterpret_cast<cudaStream_t>(stream), b->l2));
+    for (uint64_t r = 0; r < passes; ++r) {
+        a.region_lo = r * b->local_blocks / passes;
+        a.region_hi = (r + 1) * b->local_blocks / passes; /* local_blocks for the last */
+        WC_CUDA(launch_in_window(reinterpret_cast<const void *>(k), grid, kBlock, args,
+                                 reinterpret_cast<cudaStream_t>(stream), b->l2));
+    }
     return WC_OK;
 }
 

@@ -43,7 +43,15 @@ using RebuildKernel = void (*)(const void *, uint64_t, uint64_t, uint64_t, unsig
 RebuildKernel fp_rebuild_kernel_ptr(int layout);
 DumpKernel dump_kernel_ptr(int layout);
 
-BloomKernel bloom_kernel_ptr(int key_bytes, int slot_bytes, int cg, bool insert);
+/* the Bloom kernel of a configuration; multi_pass selects the variant built
+ * for region passes, *lane_kernel (if not null) tells whether the kernel is
+ * the one-key-per-lane kernel, the only one that honours region bounds */
+BloomKernel bloom_kernel_ptr(int key_bytes, int slot_bytes, int cg, bool insert, bool multi_pass,
+                             bool *lane_kernel);
+
+/* random-access region of the multi-pass kernels for inserts or queries
+ * (bytes; wc_region_bytes) */
+uint64_t region_bytes(bool insert);
 
 /* multi-table batch kernel for a slot layout (KV32 / KV64) and window width;
  * inline_desc selects the variant taking BatchInlineArgs */

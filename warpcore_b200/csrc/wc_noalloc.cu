@@ -19,17 +19,16 @@
  * kernels overlap on the GPU (two streams, or two host threads) race on it
  * and must be serialised by the caller.
  *
- * The first call on each device resolves the array's device address with
- * cudaGetSymbolAddress while that device is current; make that first call
- * before any stream capture.
+ * Every call resolves the array's device address with cudaGetSymbolAddress
+ * in the current device's context (the first call on a device also loads the
+ * module there); make the first call on each device before any stream
+ * capture.
  */
 #include <warpcore_b200.h>
 
 #include "wc_internal.h"
 
-#include <mutex>
 #include <string>
-#include <unordered_map>
 
 using namespace warpcore::b200;
 
@@ -100,28 +99,17 @@ __global__ void __launch_bounds__(256) sum_partials_kernel(const unsigned long l
     if (threadIdx.x == 0) *out = sm[0];
 }
 
-/* device address of the scratch array on the current device, resolved once
- * per device with that device current */
+/* Device address of the scratch array in the current device's context.  It
+ * is looked up on every call (a lookup allocates nothing): a cached address
+ * would go stale when the context it came from is destroyed and the module
+ * is loaded again, e.g. after cudaDeviceReset. */
 int scratch_address(unsigned long long **out)
 {
-    static std::mutex mu;
-    static std::unordered_map<int, unsigned long long *> addr;
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess)
-        return noalloc_fail(WC_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    std::lock_guard<std::mutex> lock(mu);
-    auto it = addr.find(dev);
-    if (it != addr.end()) {
-        *out = it->second;
-        return WC_OK;
-    }
     void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
     if (e != cudaSuccess || p == nullptr)
         return noalloc_fail(WC_ERR_CUDA,
                             std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    addr.emplace(dev, reinterpret_cast<unsigned long long *>(p));
     *out = reinterpret_cast<unsigned long long *>(p);
     return WC_OK;
 }
