@@ -426,6 +426,7 @@ inline b200::TableView view_from(const wc_table_info &inf)
     v.slots = inf.slots;
     v.status = inf.status;
     v.fps = inf.fingerprints;
+    v.live = inf.live;
     v.num_buckets = inf.num_buckets;
     v.seed = inf.seed;
     v.empty_key = inf.empty_key;

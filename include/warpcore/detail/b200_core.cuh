@@ -159,10 +159,19 @@ __host__ __device__ __forceinline__ uint64_t fast_mod(uint64_t x, uint64_t d, ui
 /* table view and bucket probing                                        */
 /* ------------------------------------------------------------------ */
 
+/* A table's count of valid keys is kept in kLiveStripes counters,
+ * kLiveStride words apart (one 32-byte sector each), so that writers spread
+ * their atomics; size() is the sum of the stripes modulo 2^64.  Every claim
+ * of an empty slot adds one, every erase that turns a key into a tombstone
+ * subtracts one. */
+constexpr int kLiveStripes = 32;
+constexpr int kLiveStride = 4;
+
 struct TableView {
     void *slots;
     uint32_t *status;
     unsigned char *fps;   /* one fingerprint byte per slot, or NULL */
+    unsigned long long *live; /* kLiveStripes striped key counters, or NULL */
     uint64_t num_buckets; /* capacity / cg_size; prime under the capacity rule */
     uint64_t seed;
     uint64_t empty_key;
@@ -446,6 +455,59 @@ __device__ __forceinline__ void store_key(void *sp, typename L::key_t k)
 {
     volatile typename L::key_t *p = reinterpret_cast<typename L::key_t *>(sp);
     *p = k;
+}
+
+/* add d to the table's count of valid keys (one stripe, chosen by block and
+ * warp) */
+__device__ __forceinline__ void live_add(const TableView &t, long long d)
+{
+    if (t.live && d) {
+        const unsigned stripe = (blockIdx.x + (threadIdx.x >> 5)) & (kLiveStripes - 1);
+        atomicAdd(t.live + kLiveStride * stripe, (unsigned long long)d);
+    }
+}
+
+/* Turn the slot holding `key` into a tombstone with a compare-and-swap of
+ * the whole slot (the width of the claims' compare-and-swap), keeping its
+ * payload.  Returns true if this call erased the key; false if the slot no
+ * longer holds it (an equal key erased by another thread). */
+template <class L>
+__device__ __forceinline__ bool erase_slot(void *sp, typename L::key_t key,
+                                           typename L::key_t tomb)
+{
+    if constexpr (L::kSlotBytes == 4) {
+        return atomicCAS(reinterpret_cast<unsigned int *>(sp), key, tomb) == key;
+    } else if constexpr (L::kSlotBytes == 8 && !L::kHasValue) {
+        return atomicCAS(reinterpret_cast<unsigned long long *>(sp), (unsigned long long)key,
+                         (unsigned long long)tomb) == (unsigned long long)key;
+    } else if constexpr (L::kSlotBytes == 8) {
+        unsigned long long *p = reinterpret_cast<unsigned long long *>(sp);
+        unsigned long long cur = __ldcg(p);
+        /* a retry only follows a concurrent value update of the same key */
+        for (int tries = 0; tries < 1024; ++tries) {
+            if (uint32_t(cur) != uint32_t(key)) return false;
+            const unsigned long long old =
+                atomicCAS(p, cur, (cur & 0xffffffff00000000ull) | uint32_t(tomb));
+            if (old == cur) return true;
+            cur = old;
+        }
+        store_key<L>(sp, tomb);
+        return true;
+    } else {
+        const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(sp));
+        uint64_t lo = uint64_t(v.x) | (uint64_t(v.y) << 32);
+        uint64_t hi = uint64_t(v.z) | (uint64_t(v.w) << 32);
+        for (int tries = 0; tries < 1024; ++tries) {
+            if (lo != uint64_t(key)) return false;
+            uint64_t olo, ohi;
+            cas128(sp, lo, hi, uint64_t(tomb), hi, olo, ohi);
+            if (olo == lo && ohi == hi) return true;
+            lo = olo;
+            hi = ohi;
+        }
+        store_key<L>(sp, tomb);
+        return true;
+    }
 }
 
 /* width-generic wrappers: uint64_t is unsigned long on LP64, while the CUDA

@@ -49,9 +49,9 @@ __device__ uint32_t tile_modify(const TableView &t, const Tile &g, typename L::k
             if (hit) {
                 const unsigned leader = __ffs(hit) - 1;
                 if (op == 3) {
-                    if (r == leader) {
-                        store_key<L>(sp, tomb);
+                    if (r == leader && erase_slot<L>(sp, key, tomb)) {
                         fp_store(t, b * W + r, kFpTomb);
+                        live_add(t, -1);
                     }
                     st = kStNone;
                 } else {
@@ -80,6 +80,7 @@ __device__ uint32_t tile_modify(const TableView &t, const Tile &g, typename L::k
                     const V payload = op == 1 ? V(1) : val;
                     if (claim_slot<L>(sp, empty, key, payload, old_key)) {
                         fp_store(t, b * W + r, fingerprint(key));
+                        live_add(t, 1);
                         outcome = 1;
                     } else if (old_key == key) {
                         outcome = 2;

@@ -114,6 +114,9 @@ typedef struct wc_table_info {
     unsigned long long *num_keys; /* multi-value tables: device counter of keys
                                      holding a value (NULL for other kinds) */
     uint64_t max_values_per_key;  /* multi-value tables */
+    unsigned long long *live;     /* device: the valid-key counters, 32 of them
+                                     32 bytes apart (NULL for multi-value
+                                     tables); writers of slot keys keep them */
 } wc_table_info;
 
 typedef struct wc_table wc_table;
@@ -170,8 +173,16 @@ int wc_svht_retrieve(wc_table *t, const void *keys_in, uint64_t num_in,
 int wc_svht_erase(wc_table *t, const void *keys_in, uint64_t num_in,
                   wc_stream_t stream, uint64_t probing_length,
                   void *status_out, int status_handler, uint32_t ignore);
-/* size(stream) (single_value_hash_table.cuh:535-592); blocking */
+/* size(stream) (single_value_hash_table.cuh:535-592); blocking.  The
+ * reference counts the valid keys with a scan of the whole slot array; here
+ * single-value, set and counting tables keep a count that every claim of an
+ * empty slot and every erase maintains (bulk kernels, batches and the device
+ * per-key API alike), and size reads 256 bytes of counters.  Multi-value
+ * tables (kind 3) count by scan. */
 int wc_table_size(wc_table *t, wc_stream_t stream, uint64_t *size_out);
+/* the same count by a scan of the slot array (the reference's method, kept
+ * to check the maintained count); blocking */
+int wc_table_size_scan(wc_table *t, wc_stream_t stream, uint64_t *size_out);
 /* retrieve_all(keys_out, values_out, num_out, stream)
  * (single_value_hash_table.cuh:391-417, hash_set.cuh:367-384); blocking;
  * values_out may be NULL and is ignored for hash sets */

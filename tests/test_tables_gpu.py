@@ -432,3 +432,52 @@ def test_launch_count_counts_this_librarys_kernels():
     t.retrieve(dk, out)
     assert wc.launch_count() - c0 == 3
     assert np.array_equal(host(out), vals)
+
+
+@pytest.mark.parametrize("kind,kb,vb,cg", [
+    (o.SVHT, 4, 4, 8), (o.SVHT, 8, 8, 8), (o.SVHT, 4, 8, 4), (o.SVHT, 8, 4, 2),
+    (o.HASHSET, 4, 0, 16), (o.HASHSET, 8, 0, 1), (o.COUNTING, 4, 4, 4), (o.COUNTING, 8, 8, 32)])
+@pytest.mark.parametrize("policy", ["never", "always"])
+def test_size_counter_matches_scan(kind, kb, vb, cg, policy):
+    """size() reads the count that claims and erases maintain; after batches
+    with in-batch duplicates (inserts and erases), re-inserts of erased keys
+    and counting increments it equals the scan of the slot array and the
+    oracle's size"""
+    prev = wc.set_fingerprint_policy(policy)
+    try:
+        g, r = make_pair(kind, kb, 60000, cg, vb=None if kind == o.HASHSET else vb)
+    finally:
+        wc.set_fingerprint_policy(prev)
+    assert g.has_fingerprints == (policy == "always")
+    rng = np.random.default_rng(11)
+    keys = o.gen_unique_keys(kb, 40000, 21)
+
+    def ins(k):
+        if kind == o.SVHT:
+            v = o.gen_uniform(vb, k.size, int(k.size))
+            g.insert(dev(k), dev(v))
+            r.insert(k, v)
+        else:
+            g.insert(dev(k))
+            r.insert(k)
+
+    def check():
+        assert g.size() == g.size_scan() == r.size()
+
+    batch = np.concatenate([keys[:20000], keys[rng.integers(0, 20000, 5000)]])
+    ins(batch[rng.permutation(batch.size)])
+    check()
+    er = np.concatenate([keys[:8000:2], keys[:8000:2], keys[30000:30100]])  # dups + absent
+    er = er[rng.permutation(er.size)]
+    g.erase(dev(er))
+    r.erase(er)
+    check()
+    ins(np.concatenate([keys[:8000:4], keys[20000:40000]]))
+    check()
+    g.erase(dev(keys[::3]))
+    r.erase(keys[::3])
+    check()
+    g.init()
+    assert g.size() == g.size_scan() == 0
+    ins(keys[:100])
+    assert g.size() == 100

@@ -142,6 +142,7 @@ class TableInfo(ctypes.Structure):
         ("fingerprints", ctypes.c_void_p),
         ("num_keys", ctypes.c_void_p),
         ("max_values_per_key", ctypes.c_uint64),
+        ("live", ctypes.c_void_p),
     ]
 
 
@@ -248,6 +249,7 @@ SIGNATURES = {
     "wc_svht_retrieve": (_i, [_vp, _vp, _u64, _vp, _vp, _u64, _vp, _i, _u32]),
     "wc_svht_erase": (_i, [_vp, _vp, _u64, _vp, _u64, _vp, _i, _u32]),
     "wc_table_size": (_i, [_vp, _vp, ctypes.POINTER(_u64)]),
+    "wc_table_size_scan": (_i, [_vp, _vp, ctypes.POINTER(_u64)]),
     "wc_table_retrieve_all": (_i, [_vp, _vp, _vp, ctypes.POINTER(_u64), _vp]),
     "wc_table_peek_status": (_i, [_vp, _vp, ctypes.POINTER(_u32)]),
     "wc_table_pop_status": (_i, [_vp, _vp, ctypes.POINTER(_u32)]),
@@ -567,8 +569,15 @@ class _Table:
                                    _stream(stream)))
 
     def size(self, stream=None):
+        """valid keys: the count claims and erases maintain (one small read)"""
         out = _u64()
         _check(lib().wc_table_size(self._h, _stream(stream), ctypes.byref(out)))
+        return out.value
+
+    def size_scan(self, stream=None):
+        """valid keys counted by a scan of the slot array"""
+        out = _u64()
+        _check(lib().wc_table_size_scan(self._h, _stream(stream), ctypes.byref(out)))
         return out.value
 
     @property

@@ -245,6 +245,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs a)
                                           (bucket * W + uint64_t(s)) * SB;
                 if (cas_old == empty && cas_old_payload == claim_expect) {
                     fp_store(d.t, bucket * W + uint64_t(s), fingerprint(key));
+                    live_add(d.t, 1);
                     st = kStNone;
                     pending = false;
                 } else if (cas_old == key) {

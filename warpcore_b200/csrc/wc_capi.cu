@@ -453,6 +453,7 @@ struct wc_table {
     void *slots = nullptr;
     uint32_t *status = nullptr;            /* device Status word */
     unsigned long long *counter = nullptr; /* device scratch counter */
+    unsigned long long *live = nullptr;    /* device: kLiveStripes valid-key counters */
     int device = 0;
     uint64_t keys_inserted = 0; /* since init: an upper bound of size(), for tuning */
     L2Window l2;                /* access-policy window over the slots, if they fit */
@@ -480,12 +481,19 @@ uint64_t key_mask(uint32_t key_bytes)
     return key_bytes == 4 ? 0xffffffffull : ~0ull;
 }
 
+/* a table's small device block: Status word at 0, scratch counter at 128,
+ * multi-value key count at 192, the striped valid-key counters at 256 */
+constexpr uint64_t kLiveBytes = uint64_t(kLiveStripes) * kLiveStride * 8;
+constexpr uint64_t kAuxBytes = 256 + kLiveBytes;
+
 TableView view_of(const wc_table *t)
 {
     TableView v;
     v.slots = t->slots;
     v.status = t->status;
     v.fps = t->fps;
+    /* multi-value tables count values per key and have no live counter */
+    v.live = t->kind == 3 ? nullptr : t->live;
     v.num_buckets = t->num_buckets;
     v.seed = t->seed;
     v.empty_key = t->cfg.empty_key;
@@ -597,11 +605,12 @@ int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, ui
     if (e == cudaSuccess && fp_bytes) e = cudaMalloc(&t->fps, fp_bytes);
     if (e == cudaSuccess) {
         void *aux = nullptr;
-        e = cudaMalloc(&aux, 256);
+        e = cudaMalloc(&aux, kAuxBytes);
         if (e == cudaSuccess) {
             t->status = reinterpret_cast<uint32_t *>(aux);
             t->counter = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(aux) + 128);
             t->num_keys = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(aux) + 192);
+            t->live = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(aux) + 256);
         }
     }
     if (e != cudaSuccess) {
@@ -610,7 +619,7 @@ int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, ui
         delete t;
         return cuda_fail(e, "cudaMalloc");
     }
-    e = cudaMemset(t->status, 0, 256);
+    e = cudaMemset(t->status, 0, kAuxBytes);
     if (e != cudaSuccess) {
         wc_table_destroy(t);
         return cuda_fail(e, "cudaMemset");
@@ -810,6 +819,7 @@ int wc_table_init(wc_table *t, uint64_t seed, wc_stream_t stream)
     if (rc) return rc;
     if (t->fps) WC_CUDA(cudaMemsetAsync(t->fps, kFpEmpty, t->capacity, s));
     WC_CUDA(cudaMemsetAsync(t->status, 0, sizeof(uint32_t), s));
+    WC_CUDA(cudaMemsetAsync(t->live, 0, kLiveBytes, s));
     if (t->kind == 3) WC_CUDA(cudaMemsetAsync(t->num_keys, 0, sizeof(unsigned long long), s));
     WC_CUDA(cudaStreamSynchronize(s));
     t->initialized = true;
@@ -911,6 +921,24 @@ int wc_table_size(wc_table *t, wc_stream_t stream, uint64_t *size_out)
     *size_out = 0;
     int rc = check_table(t, 0xF); /* every table kind */
     if (rc) return rc;
+    if (t->kind == 3) return wc_table_size_scan(t, stream, size_out);
+    /* the sum of the valid-key counters that claims and erases maintain */
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    unsigned long long h[kLiveStripes * kLiveStride];
+    WC_CUDA(cudaMemcpyAsync(h, t->live, kLiveBytes, cudaMemcpyDeviceToHost, s));
+    WC_CUDA(cudaStreamSynchronize(s));
+    unsigned long long sum = 0;
+    for (int i = 0; i < kLiveStripes; ++i) sum += h[i * kLiveStride];
+    *size_out = sum;
+    return WC_OK;
+}
+
+int wc_table_size_scan(wc_table *t, wc_stream_t stream, uint64_t *size_out)
+{
+    if (!size_out) return fail(WC_ERR_INVALID_ARGUMENT, "size_out is NULL");
+    *size_out = 0;
+    int rc = check_table(t, 0xF); /* every table kind */
+    if (rc) return rc;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     CountKernel k = count_kernel(t->layout);
     WC_CUDA(cudaMemsetAsync(t->counter, 0, sizeof(unsigned long long), s));
@@ -987,13 +1015,14 @@ int wc_table_get_info(const wc_table *t, wc_table_info *info)
     info->empty_key = t->cfg.empty_key;
     info->tombstone_key = t->cfg.tombstone_key;
     info->max_count = t->max_count;
-    info->bytes_total = t->capacity * t->slot_bytes + 256 + (t->fps ? t->capacity : 0);
+    info->bytes_total = t->capacity * t->slot_bytes + kAuxBytes + (t->fps ? t->capacity : 0);
     info->slots = t->slots;
     info->status = t->status;
     info->is_initialized = t->initialized ? 1 : 0;
     info->fingerprints = t->fps;
     info->num_keys = t->kind == 3 ? t->num_keys : nullptr;
     info->max_values_per_key = t->max_values;
+    info->live = t->kind == 3 ? nullptr : t->live;
     return WC_OK;
 }
 

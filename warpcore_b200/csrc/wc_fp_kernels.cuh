@@ -222,6 +222,7 @@ __global__ void __launch_bounds__(256, (OP == kOpRetrieve || OP == kOpErase) ? W
     K key = empty;
     V val = 0;
     uint32_t st = kStNone, join = 0, cnt_add = 1;
+    int live_delta = 0; /* claims minus erases of this lane */
 
     constexpr int kCache = OP == kOpCount ? 1024 : 1;
     __shared__ K sc_key[kCache];
@@ -370,8 +371,10 @@ __global__ void __launch_bounds__(256, (OP == kOpRetrieve || OP == kOpErase) ? W
                         join |= kStDuplicateKey;
                         count_add<L>(sp, cnt_add, t.max_count, st, join);
                     } else {
-                        store_key<L>(sp, tomb);
-                        fp_store(t, base_slot + uint64_t(s), kFpTomb);
+                        if (erase_slot<L>(sp, key, tomb)) {
+                            fp_store(t, base_slot + uint64_t(s), kFpTomb);
+                            --live_delta;
+                        }
                         st = kStNone;
                     }
                     pending = false;
@@ -419,6 +422,7 @@ __global__ void __launch_bounds__(256, (OP == kOpRetrieve || OP == kOpErase) ? W
 #else
                         fp_store(t, base_slot + uint64_t(s), fp);
 #endif
+                        ++live_delta;
                         st = kStNone;
                         pending = false;
                     } else if (old == key) {
@@ -504,12 +508,17 @@ __global__ void __launch_bounds__(256, (OP == kOpRetrieve || OP == kOpErase) ? W
             __syncthreads();
             for (int c = threadIdx.x; c < kCache; c += blockDim.x) {
                 const K ck = sc_key[c];
-                if (ck != empty) count_one<L, W>(t, ck, uint32_t(sc_cnt[c]), a.max_windows, join);
+                if (ck != empty)
+                    count_one<L, W>(t, ck, uint32_t(sc_cnt[c]), a.max_windows, join, live_delta);
             }
         }
     }
     const uint32_t wjoin = __reduce_or_sync(kFull, join);
-    if (lane == 0) join_status(t.status, wjoin);
+    const int wlive = int(__reduce_add_sync(kFull, unsigned(live_delta)));
+    if (lane == 0) {
+        join_status(t.status, wjoin);
+        live_add(t, wlive);
+    }
 }
 
 /* Recompute every fingerprint from the slot array in one streaming pass.

@@ -76,7 +76,7 @@ __device__ __forceinline__ T shfl_any(T v, int src)
  * slot in slot order or add to the key's slot), as the warp kernel does */
 template <class L, int W>
 __device__ void count_one(const TableView &t, typename L::key_t key, uint32_t c,
-                          uint64_t max_windows, uint32_t &join)
+                          uint64_t max_windows, uint32_t &join, int &live_delta)
 {
     using K = typename L::key_t;
     using V = typename L::val_t;
@@ -101,6 +101,7 @@ __device__ void count_one(const TableView &t, typename L::key_t key, uint32_t c,
                 K old_key;
                 if (claim_slot<L>(sp, empty, key, V(c), old_key)) {
                     fp_store(t, b * W + s, fingerprint(key));
+                    ++live_delta;
                     resolved = true;
                 } else if (old_key == key) {
                     join |= kStDuplicateKey;
@@ -181,6 +182,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
     K key = empty;
     V val = 0;
     uint32_t st = kStNone, join = 0, cnt_add = 1;
+    int live_delta = 0; /* claims minus erases of this lane */
 
     /* Counting inserts without per-key statuses go through a per-block
      * shared-memory count cache first: equal keys of the block add up there,
@@ -394,8 +396,10 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
                         join |= kStDuplicateKey;
                         count_add<L>(sp, cnt_add, t.max_count, st, join);
                     } else {
-                        store_key<L>(sp, tomb);
-                        fp_store(t, bucket * W + uint64_t(fh), kFpTomb);
+                        if (erase_slot<L>(sp, key, tomb)) {
+                            fp_store(t, bucket * W + uint64_t(fh), kFpTomb);
+                            --live_delta;
+                        }
                         st = kStNone;
                     }
                     pending = false;
@@ -428,6 +432,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
                     unsigned char *const sp = slots + (bucket * W + uint64_t(s)) * SB;
                     if (cas_old == empty && cas_old_payload == claim_expect) {
                         fp_store(t, bucket * W + uint64_t(s), fingerprint(key));
+                        ++live_delta;
                         st = kStNone;
                         pending = false;
                     } else if (cas_old == key) {
@@ -486,12 +491,17 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
             __syncthreads();
             for (int c = threadIdx.x; c < kCache; c += blockDim.x) {
                 const K ck = sc_key[c];
-                if (ck != empty) count_one<L, W>(t, ck, uint32_t(sc_cnt[c]), a.max_windows, join);
+                if (ck != empty)
+                    count_one<L, W>(t, ck, uint32_t(sc_cnt[c]), a.max_windows, join, live_delta);
             }
         }
     }
     const uint32_t wjoin = __reduce_or_sync(kFull, join);
-    if (lane == 0) join_status(t.status, wjoin);
+    const int wlive = int(__reduce_add_sync(kFull, unsigned(live_delta)));
+    if (lane == 0) {
+        join_status(t.status, wjoin);
+        live_add(t, wlive);
+    }
 }
 
 /* fill the slot array with empty slots (key = empty, payload = 0): the
