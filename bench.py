@@ -648,6 +648,7 @@ def run_ours(args):
     value = world * ops_step * args.steps / (total_ms * 1e-3) / 1e9
 
     # end to end through the public API with host buffers
+    table_ops = table_wide_ops(wl, stream) if (world == 1 and not wl.sharded) else None
     e2e = run_e2e(wl, stream, args, world) if not args.no_e2e else None
     ref_gpu = reference_gpu(wl) if (rank == 0 and not args.no_ref_gpu) else None
 
@@ -707,6 +708,7 @@ def run_ours(args):
             },
             "cpu_baseline": cpu,
             "reference_gpu_build": ref_gpu,
+            "table_wide_ops": table_ops,
             "e2e": e2e,
             # this library's kernels launched inside the timed region, as the
             # library counts them (wc_launch_count)
@@ -724,6 +726,42 @@ def run_ours(args):
     if world > 1 or args.shard:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def table_wide_ops(wl, stream, reps=3):
+    """Erase throughput and size() on the workload's table after its insert
+    (single_value_hash_table.cuh:426-496, 535-592): erase every inserted key
+    (CUDA events on the launching stream, table re-filled untimed before
+    each repetition, best of `reps`), and the time of size() (the maintained
+    count) against size_scan() (a scan of the slot array) on the full table.
+    After the erase both sizes must be 0."""
+    import torch
+    if wl.kind not in ("svht32", "svht64", "hashset64", "counting32"):
+        return None
+    t = wl.table
+    best, sizes_ok = None, True
+    size_ms, scan_ms = [], []
+    for _ in range(reps):
+        wl.init(stream)
+        wl.insert(stream)
+        torch.cuda.synchronize()
+        for fn, acc in ((t.size, size_ms), (t.size_scan, scan_ms)):
+            t0 = time.perf_counter()
+            fn()
+            acc.append((time.perf_counter() - t0) * 1e3)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        t.erase(wl.keys, stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        best = ms if best is None else min(best, ms)
+        sizes_ok = sizes_ok and t.size() == 0 and t.size_scan() == 0
+    return {"erase_gops": round(wl.keys.numel() / (best * 1e-3) / 1e9, 4),
+            "erase_ms": round(best, 4), "erased_keys": int(wl.keys.numel()),
+            "size_ms": round(min(size_ms), 4), "size_scan_ms": round(min(scan_ms), 4),
+            "size_timing": "host wall clock of the blocking call, best of %d" % reps,
+            "sizes_zero_after_erase": sizes_ok}
 
 
 def bloom_fpr_report(wl):

@@ -563,6 +563,13 @@ int wc_fingerprint_policy(int mode, int *previous);
  * followed by a streaming rebuild of all fingerprints, which is the
  * default. */
 int wc_fingerprint_ops(uint32_t op_mask, uint32_t *previous);
+/* Which operations may probe whole windows with one key per lane (each
+ * lane reads its key's window with 32-byte loads; bit 0 insert, 2 retrieve,
+ * 3 erase, default all three) instead of with groups of lanes per window
+ * and ballots.  Applies to tables whose slot array fits in L2 and whose
+ * window is at most 128 bytes (64 bytes for inserts); counting inserts
+ * (bit 1) always use the group kernel.  Results are the same either way. */
+int wc_lane_ops(uint32_t op_mask, uint32_t *previous);
 
 /* ------------------------------------------------------------------ */
 /* Region passes (no counterpart in the reference)                       */

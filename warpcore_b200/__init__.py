@@ -280,6 +280,7 @@ SIGNATURES = {
     "wc_table_retrieve_host": (_i, [_vp, _vp, _vp, _u64, _vp, _vp, _vp, _u64]),
     "wc_l2_persistence": (_i, [_i, ctypes.POINTER(ctypes.c_int)]),
     "wc_region_bytes": (_i, [_i, _u64, ctypes.POINTER(ctypes.c_uint64)]),
+    "wc_lane_ops": (_i, [_u32, ctypes.POINTER(ctypes.c_uint32)]),
     "wc_fingerprint_policy": (_i, [_i, ctypes.POINTER(ctypes.c_int)]),
     "wc_fingerprint_ops": (_i, [_u32, ctypes.POINTER(ctypes.c_uint32)]),
     "wc_launch_count": (_i, [ctypes.POINTER(_u64)]),
@@ -390,6 +391,15 @@ def set_fingerprint_policy(mode):
     m = _FP_NAMES[mode] if isinstance(mode, str) else int(mode)
     prev = ctypes.c_int(0)
     _check(lib().wc_fingerprint_policy(m, ctypes.byref(prev)))
+    return prev.value
+
+
+def set_lane_ops(op_mask):
+    """Operations (bit 0 insert, 2 retrieve, 3 erase) whose whole-window
+    probing reads one key's window per lane (wc_lane_ops); returns the
+    previous mask"""
+    prev = ctypes.c_uint32(0)
+    _check(lib().wc_lane_ops(int(op_mask), ctypes.byref(prev)))
     return prev.value
 
 

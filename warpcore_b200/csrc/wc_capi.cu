@@ -142,6 +142,11 @@ std::atomic<int> g_fp_mode{-1}; /* -1: not yet read from the environment */
  * (11.7 G/s), so every operation reads fingerprints first. */
 std::atomic<uint32_t> g_fp_ops{0xFu};
 
+/* Operations (bit kOp*) whose whole-window probing runs the one-key-per-lane
+ * kernel (wc_lane_kernels.cuh) where a window is at most 128 bytes; the
+ * others run table_op_kernel.  Counting inserts always run table_op_kernel. */
+std::atomic<uint32_t> g_lane_ops{0xDu};
+
 /* Random-access regions of the multi-pass kernels, for inserts and for
  * queries (bytes; 0 = one pass).  Random 64-byte reads on B200 measured
  * 64 G/s over 256 MiB, 19 G/s over 320 MiB and 13.5 G/s over 512 MiB, so a
@@ -645,8 +650,33 @@ int check_table(const wc_table *t, int kind_mask)
     return WC_OK;
 }
 
+/* The one-key-per-lane window kernel reads a window with one 32-byte load
+ * per sector.  On a table that L2 holds, that beats groups of lanes per
+ * window and their ballots (B200, CUDA events: u32 pairs, 16 MB table:
+ * retrieve 60.2 vs 38.0 G keys/s, insert 21.1 vs 18.0; u64 pairs, 48 MB:
+ * retrieve 29.5 vs 16.8, insert 13.2 vs 14.8).  On a table in DRAM its
+ * sector requests cost more than one request per window (u64 pairs,
+ * 2.4 GB: insert 5.9 vs 14.5), so larger tables keep the group kernel.
+ * Inserts take the lane kernel for windows of at most 64 bytes. */
+TableKernel pick_lane_kernel(const wc_table *t, int op)
+{
+    if (!((g_lane_ops.load(std::memory_order_relaxed) >> op) & 1u)) return nullptr;
+    if (t->capacity * t->slot_bytes > uint64_t(device_props().l2_bytes)) return nullptr;
+    if (op == kOpInsert && uint64_t(t->cfg.cg_size) * t->slot_bytes > 64) return nullptr;
+    const int W = int(t->cfg.cg_size);
+    switch (t->layout) {
+    case kLayoutKV32: return lane_kernel_kv32(W, op);
+    case kLayoutKV64: return lane_kernel_kv64(W, op);
+    case kLayoutSet32: return lane_kernel_set32(W, op);
+    case kLayoutK32V64: return lane_kernel_k32v64(W, op);
+    case kLayoutK64V32: return lane_kernel_k64v32(W, op);
+    default: return lane_kernel_set64(W, op);
+    }
+}
+
 TableKernel pick_window_kernel(const wc_table *t, int op)
 {
+    if (TableKernel k = pick_lane_kernel(t, op)) return k;
     const int W = int(t->cfg.cg_size);
     switch (t->layout) {
     case kLayoutKV32: return table_kernel_kv32(W, op, false);
@@ -662,6 +692,7 @@ TableKernel pick_table_kernel(const wc_table *t, int op)
 {
     const int W = int(t->cfg.cg_size);
     const bool fp = t->fps != nullptr && ((g_fp_ops.load(std::memory_order_relaxed) >> op) & 1u);
+    if (!fp) return pick_window_kernel(t, op);
     switch (t->layout) {
     case kLayoutKV32: return table_kernel_kv32(W, op, fp);
     case kLayoutKV64: return table_kernel_kv64(W, op, fp);
@@ -1228,6 +1259,13 @@ int wc_launch_count(uint64_t *out)
 int wc_fingerprint_ops(uint32_t op_mask, uint32_t *previous)
 {
     const uint32_t prev = g_fp_ops.exchange(op_mask & 0x3Fu);
+    if (previous) *previous = prev;
+    return WC_OK;
+}
+
+int wc_lane_ops(uint32_t op_mask, uint32_t *previous)
+{
+    const uint32_t prev = g_lane_ops.exchange(op_mask & 0xDu);
     if (previous) *previous = prev;
     return WC_OK;
 }

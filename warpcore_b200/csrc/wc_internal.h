@@ -10,6 +10,7 @@
 #include "wc_bloom.cuh"
 #include "wc_batch.cuh"
 #include "wc_fp_kernels.cuh"
+#include "wc_lane_kernels.cuh"
 #include "wc_mv.cuh"
 
 namespace warpcore {
@@ -37,6 +38,13 @@ TableKernel table_kernel_set32(int W, int op, bool fingerprints);
 TableKernel table_kernel_set64(int W, int op, bool fingerprints);
 TableKernel table_kernel_k32v64(int W, int op, bool fingerprints);
 TableKernel table_kernel_k64v32(int W, int op, bool fingerprints);
+/* the one-key-per-lane window kernel of (W, op), nullptr if not built */
+TableKernel lane_kernel_kv32(int W, int op);
+TableKernel lane_kernel_kv64(int W, int op);
+TableKernel lane_kernel_set32(int W, int op);
+TableKernel lane_kernel_set64(int W, int op);
+TableKernel lane_kernel_k32v64(int W, int op);
+TableKernel lane_kernel_k64v32(int W, int op);
 
 CountKernel count_kernel(int layout);
 using RebuildKernel = void (*)(const void *, uint64_t, uint64_t, uint64_t, unsigned char *);

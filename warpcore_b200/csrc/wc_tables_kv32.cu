@@ -5,6 +5,7 @@ namespace warpcore {
 namespace b200 {
 
 TableKernel table_kernel_kv32(int W, int op, bool fp) { return pick_table_kernel_for<LayoutKV32>(W, op, fp); }
+TableKernel lane_kernel_kv32(int W, int op) { return pick_lane_kernel_for<LayoutKV32>(W, op); }
 
 } // namespace b200
 } // namespace warpcore
