@@ -47,6 +47,7 @@ typedef struct CUstream_st *wc_stream_t;
 #define WC_ERR_OUT_OF_MEMORY (-3)
 #define WC_ERR_NOT_INITIALIZED (-4)
 #define WC_ERR_UNSUPPORTED (-5)
+#define WC_ERR_TIMEOUT (-6) /* a bounded device-side wait ran out */
 
 /* ---- Status bits: identical to warpcore::Status (status.cuh:44-68) ---- */
 #define WC_STATUS_NONE 0u
@@ -669,6 +670,7 @@ int wc_batch_run(wc_batch *b, const wc_batch_request *reqs, uint32_t num_request
 
 #define WC_SERVE_PLAIN 0
 #define WC_SERVE_BATCHED 1
+#define WC_SERVE_PERSISTENT 2
 
 /* One timestamped request on a resident single-value table. */
 typedef struct wc_serve_request {
@@ -684,13 +686,14 @@ typedef struct wc_serve_request {
 } wc_serve_request;
 
 typedef struct wc_serve_options {
-    int mode;                    /* WC_SERVE_PLAIN or WC_SERVE_BATCHED */
+    int mode;                    /* WC_SERVE_PLAIN, WC_SERVE_BATCHED or WC_SERVE_PERSISTENT */
     uint32_t streams;            /* streams (0: 4); plain: tables hashed onto them,
                                     batched: batches round-robin */
     uint32_t depth;              /* batched: batches in flight per stream (0: 2) */
     uint32_t max_batch_requests; /* batched: requests per batch (0: 4096) */
-    uint64_t max_batch_keys;     /* batched: keys per batch (0: no limit) */
-    uint32_t blocks_per_sm;      /* batched: 0 = occupancy limit */
+    uint64_t max_batch_keys;     /* batched: keys per batch (0: no limit);
+                                    persistent: keys per chunk (0: 1024) */
+    uint32_t blocks_per_sm;      /* batched: 0 = occupancy limit; persistent: 0 = 3 */
     uint32_t reserved;
     uint64_t probing_length;
 } wc_serve_options;
@@ -703,13 +706,57 @@ typedef struct wc_serve_stats {
 } wc_serve_stats;
 
 /* Replays `num_requests` requests, sorted by arrival, in real time in the
- * chosen form and writes each request's completion time (device events,
- * microseconds from the start) to complete_us[] and, if not NULL, the time
- * it was issued to issue_us[].  Every table sees its requests in arrival
- * order.  Blocks until all requests are complete. */
+ * chosen form and writes each request's completion time (microseconds from
+ * the start: device events, or for the persistent form the kernel's
+ * %globaltimer stamp mapped onto the host clock) to complete_us[] and, if
+ * not NULL, the time it was issued to issue_us[].  Every table sees its
+ * requests in arrival order.  Blocks until all requests are complete. */
 int wc_serve_run(const wc_serve_request *reqs, uint64_t num_requests,
                  const wc_serve_options *opt, double *issue_us, double *complete_us,
                  wc_serve_stats *stats);
+
+/* ------------------------------------------------------------------ */
+/* Persistent server (no counterpart in the reference, whose every bulk  */
+/* call is a kernel launch, gpu_engine.cuh:203-262)                      */
+/* ------------------------------------------------------------------ */
+
+/* One resident kernel takes insert / retrieve requests on single-value
+ * tables from a ring in mapped host memory: submitting a request is a few
+ * host stores, with no kernel launch.  A dispatcher warp cuts each request
+ * into chunks of chunk_keys keys; every other warp of the grid takes chunks
+ * in order and probes them; the warp that finishes a request's last chunk
+ * stamps its completion in host memory.  Requests in flight together must
+ * commute (no insert and retrieve of one table at once); wc_serve_run with
+ * WC_SERVE_PERSISTENT keeps to that.  The kernel ends when the server is
+ * stopped, or on its own after idle_timeout_us without a request; every
+ * device-side wait is bounded.  The stream must be a non-blocking stream of
+ * its own: the kernel occupies it until the stop.  Do not free device
+ * memory (cudaFree synchronises the device) while a server runs. */
+typedef struct wc_pserver wc_pserver;
+typedef struct wc_pserver_options {
+    uint32_t key_bytes;        /* 4 (u32/u32 tables) or 8 (u64/u64) */
+    uint32_t cg_size;          /* window width of the tables served */
+    uint32_t blocks_per_sm;    /* resident blocks of 256 threads (0: 3) */
+    uint32_t reserved;
+    uint64_t chunk_keys;       /* keys per chunk (0: 1024) */
+    uint64_t idle_timeout_us;  /* 0: 2 s */
+    uint64_t probing_length;
+} wc_pserver_options;
+/* launches the kernel on `stream` and returns once it runs */
+int wc_pserver_start(const wc_pserver_options *opt, wc_stream_t stream, wc_pserver **out);
+/* queues one request (device buffers; `values` for inserts, `values_out`
+ * for retrieves, written on hits only); *ticket_out identifies it.  Waits
+ * only if the ring's 4096 slots are all in flight. */
+int wc_pserver_submit(wc_pserver *s, wc_table *table, int op, const void *keys,
+                      const void *values, void *values_out, uint64_t num,
+                      uint64_t *ticket_out);
+/* *done = 1 once the request is complete; *complete_us (if not NULL) gets
+ * its completion time on the server's host clock (wc_pserver_now_us) */
+int wc_pserver_poll(wc_pserver *s, uint64_t ticket, int *done, double *complete_us);
+int wc_pserver_now_us(const wc_pserver *s, double *now_us);
+/* stops the kernel, waits for it and frees the server; WC_ERR_TIMEOUT if
+ * the kernel had ended on a bounded wait (its idle limit) */
+int wc_pserver_stop(wc_pserver *s);
 
 /* ------------------------------------------------------------------ */
 /* Key routing for tables sharded over GPUs (no counterpart in the       */

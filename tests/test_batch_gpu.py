@@ -87,7 +87,7 @@ def test_batch_graph_reuse_many_runs():
     assert np.array_equal(host(out), vals)
 
 
-@pytest.mark.parametrize("mode", ["plain", "batched"])
+@pytest.mark.parametrize("mode", ["plain", "batched", "persistent"])
 def test_served_small_workload(mode):
     from warpcore_b200.serve import ServedWorkload, run
     w = ServedWorkload(num_tables=48, cap_lo=1 << 10, cap_hi=1 << 15, num_requests=600,
@@ -118,3 +118,85 @@ def test_served_same_answers_alone_and_in_the_mix():
     import torch
     assert torch.equal(alone, w.out)
     assert w.verify()
+    # and inside the persistent kernel, with small chunks so that requests
+    # share the resident warps chunk by chunk
+    w.reset()
+    res = run(w, "persistent", max_batch_keys=64)
+    assert res["launches"] == 1
+    assert torch.equal(alone, w.out)
+    assert w.verify()
+
+
+def _pserver(key_bytes=4, cg=8, idle_us=2000000, chunk=0):
+    import ctypes
+    import torch
+    opt = wc.PServerOptions()
+    opt.key_bytes, opt.cg_size, opt.idle_timeout_us, opt.chunk_keys = key_bytes, cg, idle_us, chunk
+    opt.probing_length = wc.DEFAULT_PROBING_LENGTH
+    stream = torch.cuda.Stream()
+    h = ctypes.c_void_p()
+    rc = wc.lib().wc_pserver_start(ctypes.byref(opt), stream.cuda_stream, ctypes.byref(h))
+    assert rc == 0, wc.lib().wc_last_error()
+    return h, stream
+
+
+def _wait(h, ticket, limit_s=10.0):
+    import ctypes
+    import time
+    done, cu = ctypes.c_int(0), ctypes.c_double(0)
+    t0 = time.time()
+    while not done.value:
+        assert wc.lib().wc_pserver_poll(h, ticket, ctypes.byref(done), ctypes.byref(cu)) == 0
+        assert time.time() - t0 < limit_s
+    return cu.value
+
+
+@pytest.mark.parametrize("kb", [4, 8])
+def test_persistent_server_requests(kb):
+    """insert, then retrieve (hits and misses), through the resident kernel;
+    answers equal the oracle's and size() counts the inserts"""
+    import ctypes
+    n = 5000
+    t = wc.SingleValueHashTable(2 * n, key_bytes=kb)
+    r = o.Table(o.SVHT, kb, kb, 2 * n)
+    allk = o.gen_unique_keys(kb, 2 * n, 61)
+    keys, absent = allk[:n], allk[n:]
+    vals = o.gen_uniform(kb, n, 62)
+    r.insert(keys, vals)
+    dk, dv = dev(keys), dev(vals)
+    q = np.concatenate([keys[::2], absent[:1000]])
+    dq = dev(q)
+    out = empty_dev(q.size, kb, 7)
+    h, _ = _pserver(key_bytes=kb, chunk=256)
+    tk = ctypes.c_uint64()
+    try:
+        assert wc.lib().wc_pserver_submit(h, t._h, wc.OP_INSERT, dk.data_ptr(), dv.data_ptr(),
+                                          None, n, ctypes.byref(tk)) == 0
+        c1 = _wait(h, tk.value)
+        assert wc.lib().wc_pserver_submit(h, t._h, wc.OP_RETRIEVE, dq.data_ptr(), None,
+                                          out.data_ptr(), q.size, ctypes.byref(tk)) == 0
+        c2 = _wait(h, tk.value)
+        assert c2 >= c1 > 0
+    finally:
+        rc = wc.lib().wc_pserver_stop(h)
+    assert rc == 0, wc.lib().wc_last_error()
+    r_out = np.full(q.size, 7, dtype=keys.dtype)
+    r_out = r.retrieve(q, r_out)
+    assert np.array_equal(host(out), r_out)
+    assert t.size() == n
+
+
+def test_persistent_server_idle_limit_ends_the_kernel():
+    """a server that gets no request ends on its idle limit (a bounded wait
+    that runs out), reports WC_ERR_TIMEOUT at the stop, and the context
+    stays usable"""
+    import time
+    h, _ = _pserver(idle_us=20000)
+    time.sleep(0.3)
+    rc = wc.lib().wc_pserver_stop(h)
+    assert rc == wc.ERR_TIMEOUT
+    assert b"idle" in wc.lib().wc_last_error()
+    t = wc.SingleValueHashTable(1000, key_bytes=4)
+    k = o.gen_unique_keys(4, 100, 3)
+    t.insert(dev(k), dev(k))
+    assert t.size() == 100

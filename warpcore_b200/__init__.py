@@ -225,8 +225,21 @@ class ServeStats(ctypes.Structure):
     ]
 
 
+class PServerOptions(ctypes.Structure):
+    _fields_ = [
+        ("key_bytes", ctypes.c_uint32),
+        ("cg_size", ctypes.c_uint32),
+        ("blocks_per_sm", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+        ("chunk_keys", ctypes.c_uint64),
+        ("idle_timeout_us", ctypes.c_uint64),
+        ("probing_length", ctypes.c_uint64),
+    ]
+
+
 OP_INSERT, OP_RETRIEVE = 0, 2
-SERVE_PLAIN, SERVE_BATCHED = 0, 1
+SERVE_PLAIN, SERVE_BATCHED, SERVE_PERSISTENT = 0, 1, 2
+ERR_TIMEOUT = -6
 
 _vp = ctypes.c_void_p
 _u64 = ctypes.c_uint64
@@ -332,6 +345,11 @@ SIGNATURES = {
     "wc_serve_run": (_i, [ctypes.POINTER(ServeRequest), _u64, ctypes.POINTER(ServeOptions),
                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                           ctypes.POINTER(ServeStats)]),
+    "wc_pserver_start": (_i, [ctypes.POINTER(PServerOptions), _vp, _pp]),
+    "wc_pserver_submit": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _u64, ctypes.POINTER(_u64)]),
+    "wc_pserver_poll": (_i, [_vp, _u64, ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_double)]),
+    "wc_pserver_now_us": (_i, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    "wc_pserver_stop": (_i, [_vp]),
 }
 
 _lib = None

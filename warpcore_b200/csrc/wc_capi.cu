@@ -768,6 +768,19 @@ int table_op(wc_table *t, int op, const void *keys, const void *values, void *ou
 
 } // namespace
 
+int warpcore::b200::host_svht_view(const wc_table *t, TableView *view, int *layout, uint32_t *cg,
+                                   uint64_t probing_length, uint64_t *max_windows_out)
+{
+    if (!t) return fail(WC_ERR_INVALID_ARGUMENT, "table is NULL");
+    if (t->kind != 0) return fail(WC_ERR_INVALID_ARGUMENT, "not a single-value table");
+    if (!t->initialized) return fail(WC_ERR_NOT_INITIALIZED, "table is not initialized");
+    *view = view_of(t);
+    *layout = t->layout;
+    *cg = t->cfg.cg_size;
+    *max_windows_out = max_windows(probing_length, t->cfg.cg_size, t->num_buckets);
+    return WC_OK;
+}
+
 /* ------------------------------------------------------------------ */
 /* C ABI                                                                 */
 /* ------------------------------------------------------------------ */

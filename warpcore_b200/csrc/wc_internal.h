@@ -106,6 +106,11 @@ int partition_by_bloom_block(const void *keys, uint64_t n, uint32_t key_bytes, u
 /* kernels this library launched (wc_launch_count) */
 void note_launches(uint32_t n);
 
+/* the device view, slot layout and window width of an initialized
+ * single-value table, and the windows a probing length allows */
+int host_svht_view(const wc_table *t, TableView *view, int *layout, uint32_t *cg,
+                   uint64_t probing_length, uint64_t *max_windows_out);
+
 } // namespace b200
 } // namespace warpcore
 

@@ -120,8 +120,20 @@ __device__ void count_one(const TableView &t, typename L::key_t key, uint32_t c,
     }
 }
 
+/* The warp-batched probing loop of table_op_kernel over the keys
+ * [wb, we) of one warp: used by table_op_kernel for its warp's range and by
+ * the persistent serving kernel for one chunk of a request.  sh_bucket,
+ * sh_key and sh_off are this warp's 32-entry rows in shared memory; sc_key /
+ * sc_cnt the block's count cache (counting inserts with use_cache).  Joins
+ * the status bits of its keys into `join` and its claims minus erases into
+ * `live_delta`. */
 template <class L, int W, int OP>
-__global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(const TableOpArgs a)
+__device__ __forceinline__ void group_range(const TableOpArgs &a, const uint64_t wb,
+                                            const uint64_t we, uint64_t *sh_bucket,
+                                            typename L::key_t *sh_key, uint32_t *sh_off,
+                                            typename L::key_t *sc_key, typename L::val_t *sc_cnt,
+                                            const bool use_cache, uint32_t &join,
+                                            int &live_delta)
 {
     using K = typename L::key_t;
     using V = typename L::val_t;
@@ -133,6 +145,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
     constexpr int G = 32 / TPK;           /* windows per warp per round */
     constexpr uint32_t kGroupMask = TPK == 32 ? kFull : ((1u << TPK) - 1u);
     constexpr bool kValueIn = OP == kOpInsert && L::kHasValue;
+    constexpr int kCache = OP == kOpCount ? 1024 : 1;
     static_assert(TPK * LB == WB && SPL * SB == LB, "window split");
 
     const TableView &t = a.t;
@@ -140,20 +153,6 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
     const int g = lane / TPK;
     const int q = lane % TPK;
     const unsigned lanemask_lt = (1u << lane) - 1u;
-    const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-    const int wib = threadIdx.x >> 5;
-    __shared__ uint64_t sh_bucket[8][32];
-    __shared__ K sh_key[8][32];
-    __shared__ uint32_t sh_off[8][32];
-
-    /* this warp's contiguous range of keys */
-    uint64_t per = (a.n + nwarps - 1) / nwarps;
-    per = (per + 31) & ~uint64_t(31);
-    const uint64_t wb = warp * per < a.n ? warp * per : a.n;
-    const uint64_t we = wb + per < a.n ? wb + per : a.n;
-    /* (a warp without keys runs the loop once and leaves it: every warp must
-     * reach the block barriers of the counting cache below) */
 
     const K empty = K(t.empty_key);
     const K tomb = K(t.tombstone_key);
@@ -181,24 +180,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
     uint64_t i = 0, bucket = 0, step = 0, wins = 0;
     K key = empty;
     V val = 0;
-    uint32_t st = kStNone, join = 0, cnt_add = 1;
-    int live_delta = 0; /* claims minus erases of this lane */
-
-    /* Counting inserts without per-key statuses go through a per-block
-     * shared-memory count cache first: equal keys of the block add up there,
-     * and each cached key reaches the table once, when the block flushes.
-     * Skewed (Zipf) streams thus stop serialising atomics on hot slots. */
-    constexpr int kCache = OP == kOpCount ? 1024 : 1;
-    __shared__ K sc_key[kCache];
-    __shared__ V sc_cnt[kCache];
-    const bool use_cache = OP == kOpCount && a.handler == kHandlerNothing;
-    if (use_cache) {
-        for (int c = threadIdx.x; c < kCache; c += blockDim.x) {
-            sc_key[c] = empty;
-            sc_cnt[c] = 0;
-        }
-        __syncthreads();
-    }
+    uint32_t st = kStNone, cnt_add = 1;
 
     for (;;) {
         /* ---- refill lanes whose key is done, in input order ---- */
@@ -318,9 +300,9 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
              * round rr then serves the owner of rank rr * G + g */
             __syncwarp();
             if (loading) {
-                sh_bucket[wib][my_rank] = bucket;
-                sh_key[wib][my_rank] = key;
-                sh_off[wib][my_rank] = uint32_t(i - wb);
+                sh_bucket[my_rank] = bucket;
+                sh_key[my_rank] = key;
+                sh_off[my_rank] = uint32_t(i - wb);
             }
             __syncwarp();
 
@@ -330,7 +312,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
                 if (rr < rounds) {
                     const int idx = rr * G + g;
                     if (idx < cnt) {
-                        const uint64_t b = sh_bucket[wib][idx];
+                        const uint64_t b = sh_bucket[idx];
                         win[rr] = load_lane<LB>(slots + (b * W + uint64_t(q) * SPL) * SB);
                     } else {
                         win[rr] = LaneWords{{0u, 0u, 0u, 0u}};
@@ -354,7 +336,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
                 if (rr < rounds) {
                     const int idx = rr * G + g;
                     const bool served = idx < cnt;
-                    const K kr = served ? sh_key[wib][idx] : empty;
+                    const K kr = served ? sh_key[idx] : empty;
 #pragma unroll
                     for (int s = 0; s < SPL; ++s) {
                         const K sk = slot_key<L>(win[rr], s);
@@ -371,7 +353,7 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
                             if (h && !a.is_set) {
                                 V v = slot_val<L>(win[rr], s);
                                 if (uint64_t(v) > t.max_count) v = V(t.max_count);
-                                st_stream(reinterpret_cast<V *>(a.out) + wb + sh_off[wib][idx], v);
+                                st_stream(reinterpret_cast<V *>(a.out) + wb + sh_off[idx], v);
                             }
                         }
                     }
@@ -485,6 +467,52 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
             has = false;
         }
     }
+}
+
+template <class L, int W, int OP>
+__global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(const TableOpArgs a)
+{
+    using K = typename L::key_t;
+    using V = typename L::val_t;
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    const int wib = threadIdx.x >> 5;
+    __shared__ uint64_t sh_bucket[8][32];
+    __shared__ K sh_key[8][32];
+    __shared__ uint32_t sh_off[8][32];
+
+    /* this warp's contiguous range of keys */
+    uint64_t per = (a.n + nwarps - 1) / nwarps;
+    per = (per + 31) & ~uint64_t(31);
+    const uint64_t wb = warp * per < a.n ? warp * per : a.n;
+    const uint64_t we = wb + per < a.n ? wb + per : a.n;
+    /* (a warp without keys runs the loop once and leaves it: every warp must
+     * reach the block barriers of the counting cache below) */
+
+    const K empty = K(a.t.empty_key);
+    uint32_t join = 0;
+    int live_delta = 0; /* claims minus erases of this warp's lanes */
+
+    /* Counting inserts without per-key statuses go through a per-block
+     * shared-memory count cache first: equal keys of the block add up there,
+     * and each cached key reaches the table once, when the block flushes.
+     * Skewed (Zipf) streams thus stop serialising atomics on hot slots. */
+    constexpr int kCache = OP == kOpCount ? 1024 : 1;
+    __shared__ K sc_key[kCache];
+    __shared__ V sc_cnt[kCache];
+    const bool use_cache = OP == kOpCount && a.handler == kHandlerNothing;
+    if (use_cache) {
+        for (int c = threadIdx.x; c < kCache; c += blockDim.x) {
+            sc_key[c] = empty;
+            sc_cnt[c] = 0;
+        }
+        __syncthreads();
+    }
+
+    group_range<L, W, OP>(a, wb, we, sh_bucket[wib], sh_key[wib], sh_off[wib], sc_key, sc_cnt,
+                          use_cache, join, live_delta);
+
     if constexpr (OP == kOpCount) {
         if (use_cache) {
             /* flush: every cached key is counted into the table once */
@@ -492,15 +520,15 @@ __global__ void __launch_bounds__(256, WC_TABLE_MIN_BLOCKS) table_op_kernel(cons
             for (int c = threadIdx.x; c < kCache; c += blockDim.x) {
                 const K ck = sc_key[c];
                 if (ck != empty)
-                    count_one<L, W>(t, ck, uint32_t(sc_cnt[c]), a.max_windows, join, live_delta);
+                    count_one<L, W>(a.t, ck, uint32_t(sc_cnt[c]), a.max_windows, join, live_delta);
             }
         }
     }
     const uint32_t wjoin = __reduce_or_sync(kFull, join);
     const int wlive = int(__reduce_add_sync(kFull, unsigned(live_delta)));
     if (lane == 0) {
-        join_status(t.status, wjoin);
-        live_add(t, wlive);
+        join_status(a.t.status, wjoin);
+        live_add(a.t, wlive);
     }
 }
 

@@ -55,6 +55,119 @@ double since(Clock::time_point t0)
     return std::chrono::duration<double, std::micro>(Clock::now() - t0).count();
 }
 
+/* WC_SERVE_PERSISTENT: one resident kernel (wc_pserve.cu); the host
+ * submits each request when it arrives, unless a request of the other kind
+ * on its table is in flight or an earlier request of its table waits, and
+ * polls completions in mapped host memory. */
+int serve_persistent(const wc_serve_request *reqs, uint64_t num_requests,
+                     const wc_serve_options *opt, double *issue_us, double *complete_us,
+                     wc_serve_stats *stats)
+{
+    uint64_t max_table = 0;
+    for (uint64_t i = 0; i < num_requests; ++i)
+        max_table = reqs[i].table_id > max_table ? reqs[i].table_id : max_table;
+    wc_table_info inf{};
+    int rc = wc_table_get_info(reqs[0].table, &inf);
+    if (rc) return rc;
+    cudaStream_t stream = nullptr;
+    SERVE_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    SERVE_CUDA(cudaDeviceSynchronize());
+    wc_pserver_options po{};
+    po.key_bytes = inf.key_bytes;
+    po.cg_size = inf.cg_size;
+    po.blocks_per_sm = opt->blocks_per_sm;
+    po.chunk_keys = opt->max_batch_keys;
+    po.probing_length = opt->probing_length;
+    wc_pserver *srv = nullptr;
+    rc = wc_pserver_start(&po, reinterpret_cast<wc_stream_t>(stream), &srv);
+    if (rc) {
+        cudaStreamDestroy(stream);
+        return rc;
+    }
+    /* per table: kind of the requests in flight (1 insert, 2 retrieve),
+     * their number, and the requests waiting behind them in arrival order */
+    std::vector<uint8_t> kind(max_table + 1, 0);
+    std::vector<uint32_t> count(max_table + 1, 0);
+    std::vector<std::deque<uint64_t>> waiting(max_table + 1);
+    std::vector<uint64_t> ticket(num_requests, 0);
+    std::vector<uint64_t> inflight;
+    inflight.reserve(4096);
+    double t0 = 0;
+    wc_pserver_now_us(srv, &t0);
+    auto now = [&]() {
+        double u = 0;
+        wc_pserver_now_us(srv, &u);
+        return u - t0;
+    };
+    auto submit = [&](uint64_t id) -> int {
+        const wc_serve_request &q = reqs[id];
+        if (issue_us) issue_us[id] = now();
+        const int r2 = wc_pserver_submit(srv, q.table, q.op, q.keys, q.values, q.values_out, q.num,
+                                         &ticket[id]);
+        if (r2) return r2;
+        kind[q.table_id] = q.op == WC_OP_INSERT ? 1 : 2;
+        ++count[q.table_id];
+        inflight.push_back(id);
+        return WC_OK;
+    };
+    uint64_t next = 0, done = 0;
+    while (done < num_requests && rc == WC_OK) {
+        const double t = now();
+        bool idle = true;
+        while (next < num_requests && reqs[next].arrival_us <= t && rc == WC_OK) {
+            const uint64_t id = next++;
+            const uint64_t tb = reqs[id].table_id;
+            const uint8_t k = reqs[id].op == WC_OP_INSERT ? 1 : 2;
+            if (waiting[tb].empty() && (count[tb] == 0 || kind[tb] == k)) rc = submit(id);
+            else waiting[tb].push_back(id);
+            idle = false;
+        }
+        for (size_t j = 0; j < inflight.size() && rc == WC_OK;) {
+            const uint64_t id = inflight[j];
+            int fin = 0;
+            double cu = 0;
+            rc = wc_pserver_poll(srv, ticket[id], &fin, &cu);
+            if (rc || !fin) {
+                ++j;
+                continue;
+            }
+            complete_us[id] = cu - t0;
+            ++done;
+            idle = false;
+            inflight[j] = inflight.back();
+            inflight.pop_back();
+            const uint64_t tb = reqs[id].table_id;
+            if (--count[tb] == 0) {
+                kind[tb] = 0;
+                /* release the waiting requests of this table that commute */
+                while (!waiting[tb].empty() && rc == WC_OK) {
+                    const uint64_t w = waiting[tb].front();
+                    const uint8_t k = reqs[w].op == WC_OP_INSERT ? 1 : 2;
+                    if (count[tb] != 0 && kind[tb] != k) break;
+                    waiting[tb].pop_front();
+                    rc = submit(w);
+                }
+            }
+        }
+        if (idle && inflight.empty() && next < num_requests) {
+            const double wait = reqs[next].arrival_us - now();
+            if (wait > 50) std::this_thread::sleep_for(std::chrono::microseconds(int64_t(wait - 40)));
+        }
+    }
+    const int rs = wc_pserver_stop(srv);
+    if (rc == WC_OK) rc = rs;
+    cudaStreamDestroy(stream);
+    if (stats) {
+        stats->launches = 1;
+        stats->batches = num_requests;
+        stats->max_keys_in_batch = po.chunk_keys ? po.chunk_keys : 1024;
+        stats->gpu_batch_us = 0;
+        stats->host_launch_us = 0;
+        stats->host_wall_us = now();
+    }
+    return rc;
+}
+
 } // namespace
 
 extern "C" int wc_serve_run(const wc_serve_request *reqs, uint64_t num_requests,
@@ -67,6 +180,8 @@ extern "C" int wc_serve_run(const wc_serve_request *reqs, uint64_t num_requests,
         if (reqs[i].arrival_us < reqs[i - 1].arrival_us)
             return serve_fail(WC_ERR_INVALID_ARGUMENT, "requests must be sorted by arrival");
 
+    if (opt->mode == WC_SERVE_PERSISTENT)
+        return serve_persistent(reqs, num_requests, opt, issue_us, complete_us, stats);
     const int nstreams = opt->streams ? int(opt->streams) : 4;
     std::vector<cudaStream_t> streams(nstreams);
     for (auto &s : streams) SERVE_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));

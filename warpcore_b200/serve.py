@@ -25,7 +25,7 @@ import math
 
 import numpy as np
 
-from . import (OP_INSERT, OP_RETRIEVE, SERVE_BATCHED, SERVE_PLAIN, ServeOptions,
+from . import (OP_INSERT, OP_RETRIEVE, SERVE_BATCHED, SERVE_PERSISTENT, SERVE_PLAIN, ServeOptions,
                ServeRequest, ServeStats, SingleValueHashTable, _check, lib,
                set_l2_persistence, valid_capacity, DEFAULT_PROBING_LENGTH)
 
@@ -235,12 +235,14 @@ class ServedWorkload:
 
 def run(workload, mode, streams=4, depth=2, max_batch_requests=4096, max_batch_keys=0,
         blocks_per_sm=0):
-    """Replays the workload in `mode` ("plain" or "batched"); returns a dict
-    with throughput, latency percentiles and launch counts."""
+    """Replays the workload in `mode` ("plain", "batched" or "persistent");
+    returns a dict with throughput, latency percentiles and launch counts.
+    For "persistent", max_batch_keys is the chunk size (0: 1024 keys)."""
     reqs, keep = workload.requests()
     n = len(keep)
     opt = ServeOptions()
-    opt.mode = SERVE_PLAIN if mode == "plain" else SERVE_BATCHED
+    opt.mode = {"plain": SERVE_PLAIN, "batched": SERVE_BATCHED,
+                "persistent": SERVE_PERSISTENT}[mode]
     opt.streams = streams
     opt.depth = depth
     opt.max_batch_requests = max_batch_requests
