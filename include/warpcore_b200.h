@@ -580,8 +580,8 @@ int wc_lane_ops(uint32_t op_mask, uint32_t *previous);
  * the GPU's address-translation reach (64-byte reads at random: 64 G/s over
  * 256 MiB, 13.5 G/s over 512 MiB).  A Bloom filter with blocks of at most
  * 128 bytes whose words exceed the region size of the operation is inserted
- * into (WC_REGION_INSERT, default 128 MiB) or queried (WC_REGION_QUERY,
- * default 256 MiB) in passes, each streaming all keys and serving those
+ * into (WC_REGION_INSERT) or queried (WC_REGION_QUERY) in passes, default
+ * 256 MiB for both, each streaming all keys and serving those
  * whose block lies in one region of the filter.  0 = always one pass;
  * otherwise 1 MiB .. 1 TiB.  Applies to later calls (*previous gets the old
  * value).  Results do not depend on it. */
@@ -693,7 +693,7 @@ typedef struct wc_serve_options {
     uint32_t max_batch_requests; /* batched: requests per batch (0: 4096) */
     uint64_t max_batch_keys;     /* batched: keys per batch (0: no limit);
                                     persistent: keys per chunk (0: 1024) */
-    uint32_t blocks_per_sm;      /* batched: 0 = occupancy limit; persistent: 0 = 3 */
+    uint32_t blocks_per_sm;      /* batched: 0 = occupancy limit; persistent: 0 = 2 */
     uint32_t reserved;
     uint64_t probing_length;
 } wc_serve_options;
@@ -736,7 +736,7 @@ typedef struct wc_pserver wc_pserver;
 typedef struct wc_pserver_options {
     uint32_t key_bytes;        /* 4 (u32/u32 tables) or 8 (u64/u64) */
     uint32_t cg_size;          /* window width of the tables served */
-    uint32_t blocks_per_sm;    /* resident blocks of 256 threads (0: 3) */
+    uint32_t blocks_per_sm;    /* resident blocks of 256 threads (0: 2) */
     uint32_t reserved;
     uint64_t chunk_keys;       /* keys per chunk (0: 1024) */
     uint64_t idle_timeout_us;  /* 0: 2 s */

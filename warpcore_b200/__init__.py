@@ -423,9 +423,9 @@ def set_lane_ops(op_mask):
 
 def set_region_bytes(nbytes, op=None):
     """Random-access region of the multi-pass kernels: a Bloom filter
-    larger than this is inserted into (op "insert", default 128 MiB) or
-    queried (op "query", default 256 MiB) in passes, one region of its blocks
-    per pass; 0 = always one pass.  `nbytes` is one value for both, or a
+    larger than this is inserted into (op "insert") or queried (op "query")
+    in passes, one region of its blocks per pass (default 256 MiB for both);
+    0 = always one pass.  `nbytes` is one value for both, or a
     pair (insert, query); op=None sets both.  Returns the previous value(s)
     in the same form."""
     ops = {"insert": 0, "query": 1}

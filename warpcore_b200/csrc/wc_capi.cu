@@ -150,10 +150,11 @@ std::atomic<uint32_t> g_lane_ops{0xDu};
 /* Random-access regions of the multi-pass kernels, for inserts and for
  * queries (bytes; 0 = one pass).  Random 64-byte reads on B200 measured
  * 64 G/s over 256 MiB, 19 G/s over 320 MiB and 13.5 G/s over 512 MiB, so a
- * query pass works on at most 256 MiB.  An insert pass also ORs words:
- * Bloom inserts into 128 MiB regions (about L2's size) ran 26.8 G keys/s
- * against 16.0 into 256 MiB regions. */
-std::atomic<uint64_t> g_region_bytes[2] = {{128ull << 20}, {256ull << 20}};
+ * pass works on at most 256 MiB.  Smaller regions cost another pass over
+ * the keys each: on the 2^32-bit filter with 2^28 keys, regions of 64 /
+ * 128 / 256 MiB ran inserts at 11.0 / 14.9 / 17.0 G keys/s and queries at
+ * 11.8 / 17.0 / 21.2. */
+std::atomic<uint64_t> g_region_bytes[2] = {{256ull << 20}, {256ull << 20}};
 
 } // namespace
 

@@ -83,7 +83,6 @@ struct PsHost {
 struct PsDev {
     unsigned long long chunk_tail; /* chunks published */
     unsigned long long chunk_head; /* tickets handed out */
-    unsigned long long consumed;   /* chunk entries read by workers */
     uint32_t stop;
     uint32_t error;
     unsigned long long remaining[kPsRing];
@@ -134,16 +133,19 @@ __device__ __forceinline__ void ps_fail(PsHost *h, PsDev *d, uint32_t bits)
  * to 32 new requests: their descriptors are copied by all lanes at once
  * (one round trip to host memory for the batch), lane j sizes request j's
  * chunks, a warp prefix sum places them in the chunk ring, and one release
- * store of chunk_tail publishes them all.  A request gets chunks of
- * max(32, n / worker warps) keys, rounded up to a multiple of 32 and capped
- * at chunk_keys, so that a large request spreads over the resident warps
- * and a small one is not cut into pieces of a few keys. */
+ * store of chunk_tail publishes them all.  Chunk sizes follow the load:
+ * while fewer than a quarter of the worker warps' worth of chunks wait
+ * unclaimed, a request gets chunks of n / (worker warps) keys (at least 32,
+ * a multiple of 32, at most chunk_keys), so that one large request spreads
+ * over all resident warps; once chunks queue up, requests get chunks of
+ * chunk_keys keys, which cost fewer claims per key.  (Measured on the
+ * served mix at 1M requests/s: chunks spread over all warps at every load
+ * gave 12.6 Gops/s, over half of them 17.7.) */
 __device__ void ps_dispatch(PsHost *h, PsDev *d, uint64_t chunk_keys, uint64_t idle_ns)
 {
     const int lane = threadIdx.x & 31;
     const unsigned lanemask_lt = (1u << lane) - 1u;
     const uint64_t workers = uint64_t(gridDim.x) * (blockDim.x >> 5) - 1;
-    const uint64_t spread = workers > 0 ? workers : 1;
     uint64_t seen = 0;
     unsigned long long ctail = 0;
     if (lane == 0) {
@@ -172,13 +174,19 @@ __device__ void ps_dispatch(PsHost *h, PsDev *d, uint64_t chunk_keys, uint64_t i
                 dst[w % kWords] = *reinterpret_cast<const volatile uint64_t *>(src + w % kWords);
             }
             __syncwarp();
+            /* chunks published and not yet claimed */
+            unsigned long long head = 0;
+            if (lane == 0) head = ld_acquire_gpu(&d->chunk_head);
+            head = __shfl_sync(kFull, head, 0);
+            const unsigned long long backlog = ctail > head ? ctail - head : 0;
+            const bool busy = backlog * 4 >= workers;
             /* lane j: request seen + j */
             const uint32_t slot = uint32_t((seen + uint64_t(lane)) % kPsRing);
             unsigned long long nch = 0;
             uint64_t chunk = 32;
             if (lane < k) {
                 const uint64_t n = d->req[slot].n;
-                chunk = (n / spread + 31) & ~uint64_t(31);
+                chunk = busy ? chunk_keys : (n / (workers ? workers : 1) + 31) & ~uint64_t(31);
                 if (chunk < 32) chunk = 32;
                 if (chunk > chunk_keys) chunk = chunk_keys;
                 nch = (n + chunk - 1) / chunk;
@@ -193,13 +201,20 @@ __device__ void ps_dispatch(PsHost *h, PsDev *d, uint64_t chunk_keys, uint64_t i
             }
             const unsigned long long total = __shfl_sync(kFull, incl, 31);
             const unsigned long long first = ctail + incl - nch;
-            /* room in the chunk ring: entries not yet read by a worker */
+            /* room in the chunk ring: entries that a worker may not have
+             * read yet; tickets are handed out in order and every warp
+             * holds at most one, so entries below chunk_head - workers are
+             * read */
             if (total) {
                 const uint64_t t_wait = global_ns();
                 bool room = false;
                 for (;;) {
                     unsigned long long used = 0;
-                    if (lane == 0) used = ctail - ld_acquire_gpu(&d->consumed);
+                    if (lane == 0) {
+                        const unsigned long long h2 = ld_acquire_gpu(&d->chunk_head);
+                        const unsigned long long read = h2 > workers ? h2 - workers : 0;
+                        used = ctail - (read < ctail ? read : ctail);
+                    }
                     used = __shfl_sync(kFull, used, 0);
                     if (used + total <= kPsChunkRing) {
                         room = true;
@@ -249,12 +264,12 @@ __device__ void ps_dispatch(PsHost *h, PsDev *d, uint64_t chunk_keys, uint64_t i
             if (lane == 0) ps_fail(h, d, kPsErrTimeout);
             return;
         }
-        __nanosleep(100);
+        /* (each poll is a round trip to host memory; no sleep between) */
     }
 }
 
 template <class L, int W>
-__global__ void __launch_bounds__(256, 3) pserve_kernel(PsHost *h, PsDev *d, uint64_t chunk_keys,
+__global__ void __launch_bounds__(256, 2) pserve_kernel(PsHost *h, PsDev *d, uint64_t chunk_keys,
                                                         uint64_t idle_ns)
 {
     using K = typename L::key_t;
@@ -296,7 +311,6 @@ __global__ void __launch_bounds__(256, 3) pserve_kernel(PsHost *h, PsDev *d, uin
         }
         if (!got) return;
         const unsigned long long e = d->chunk[ticket % kPsChunkRing];
-        if (lane == 0) atomicAdd(&d->consumed, 1ull);
         const uint32_t slot = uint32_t(e >> kPsBeginBits);
         const uint64_t begin = e & ((1ull << kPsBeginBits) - 1);
         const PsRequest &r = d->req[slot];
@@ -417,7 +431,7 @@ extern "C" int wc_pserver_start(const wc_pserver_options *opt, wc_stream_t strea
     s->opt = *opt;
     if (!s->opt.chunk_keys) s->opt.chunk_keys = 1024;
     if (!s->opt.idle_timeout_us) s->opt.idle_timeout_us = 2000000;
-    if (!s->opt.blocks_per_sm) s->opt.blocks_per_sm = 3;
+    if (!s->opt.blocks_per_sm) s->opt.blocks_per_sm = 2;
     if (s->opt.chunk_keys >= (1ull << kPsBeginBits)) {
         ps_free(s);
         return ps_fail_host(WC_ERR_INVALID_ARGUMENT, "chunk_keys too large");
