@@ -174,6 +174,22 @@ int wc_svht_retrieve(wc_table *t, const void *keys_in, uint64_t num_in,
 int wc_svht_erase(wc_table *t, const void *keys_in, uint64_t num_in,
                   wc_stream_t stream, uint64_t probing_length,
                   void *status_out, int status_handler, uint32_t ignore);
+/* No counterpart in the reference, whose tables always allocate their own
+ * memory (storage.cuh:464-516).  Device bytes a single-value table of this
+ * configuration takes when placed on caller memory: its slots, the Status
+ * word and counters, and its fingerprints if the fingerprint policy gives
+ * them to it. */
+int wc_svht_memory_bytes(const wc_table_config *cfg, uint64_t min_capacity, uint64_t *bytes_out);
+/* A single-value table placed on caller-provided device memory (256-byte
+ * aligned, at least wc_svht_memory_bytes); wc_table_destroy does not free
+ * it.  no_init 0: initialise (as wc_svht_create); 1: leave uninitialised;
+ * 2: adopt the memory's contents, a copy of the memory of a table of the
+ * same configuration (a table swapped out to the host and back).  Works on
+ * `stream` and synchronises it.  This is how a serving loop keeps tables in
+ * a memory pool of its own and moves them in and out of a device budget. */
+int wc_svht_create_on(const wc_table_config *cfg, uint64_t min_capacity, uint64_t seed,
+                      int no_init, void *memory, uint64_t memory_bytes, wc_stream_t stream,
+                      wc_table **out);
 /* size(stream) (single_value_hash_table.cuh:535-592); blocking.  The
  * reference counts the valid keys with a scan of the whole slot array; here
  * single-value, set and counting tables keep a count that every claim of an
@@ -696,6 +712,10 @@ typedef struct wc_serve_options {
     uint32_t blocks_per_sm;      /* batched: 0 = occupancy limit; persistent: 0 = 2 */
     uint32_t reserved;
     uint64_t probing_length;
+    struct wc_table_pool *pool;  /* persistent only: requests name tables of this
+                                    pool by table_id (their `table` is ignored)
+                                    and are admitted against its budget; NULL:
+                                    every request's table is resident */
 } wc_serve_options;
 
 typedef struct wc_serve_stats {
@@ -704,6 +724,41 @@ typedef struct wc_serve_stats {
     double gpu_batch_us;   /* batched: summed GPU time of the batches */
     double host_launch_us; /* batched: summed host time to launch them */
 } wc_serve_stats;
+
+/* ------------------------------------------------------------------ */
+/* Table pool: tables admitted against a device-memory budget (no        */
+/* counterpart in the reference)                                         */
+/* ------------------------------------------------------------------ */
+
+/* A set of single-value tables that share a device-memory budget.  A table
+ * is registered (wc_table_pool_add) without device memory and becomes
+ * resident when a request needs it: placed on memory of the pool's own
+ * stream-ordered memory pool (wc_svht_create_on), new and initialised, or
+ * restored from its host copy.  When the budget (resident tables plus the
+ * buffers of requests in flight) has no room, the least recently used
+ * tables with nothing in flight are copied to pinned host memory and their
+ * device memory goes back to the pool.  Stream-ordered allocation
+ * (cudaMallocAsync / cudaFreeAsync) never waits for the device, so tables
+ * move while a persistent server runs. */
+typedef struct wc_table_pool wc_table_pool;
+typedef struct wc_table_pool_stats {
+    uint64_t admissions;      /* tables placed in device memory */
+    uint64_t restores;        /* of those, restored from a host copy */
+    uint64_t evictions;       /* tables copied out to host memory */
+    uint64_t waits;           /* requests that waited for budget */
+    uint64_t peak_bytes;      /* highest resident + in-flight buffer bytes */
+    uint64_t resident_bytes;  /* now */
+    uint64_t resident_tables; /* now */
+} wc_table_pool_stats;
+int wc_table_pool_create(uint64_t budget_bytes, wc_table_pool **out);
+/* registers a table (no device memory yet); *id_out is its table_id */
+int wc_table_pool_add(wc_table_pool *p, const wc_table_config *cfg, uint64_t min_capacity,
+                      uint64_t seed, uint64_t *id_out);
+/* makes table `id` resident (evicting others if needed) and returns its
+ * handle, valid until the pool moves it again */
+int wc_table_pool_table(wc_table_pool *p, uint64_t id, wc_table **out);
+int wc_table_pool_get_stats(const wc_table_pool *p, wc_table_pool_stats *out);
+int wc_table_pool_destroy(wc_table_pool *p);
 
 /* Replays `num_requests` requests, sorted by arrival, in real time in the
  * chosen form and writes each request's completion time (microseconds from

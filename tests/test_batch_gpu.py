@@ -200,3 +200,33 @@ def test_persistent_server_idle_limit_ends_the_kernel():
     k = o.gen_unique_keys(4, 100, 3)
     t.insert(dev(k), dev(k))
     assert t.size() == 100
+
+
+def test_served_dynamic_admission_evicts_and_restores():
+    """Tables admitted against a budget of about a third of their bytes:
+    each is placed in device memory when its first request runs, evicted to
+    host memory when the budget needs room and restored when a request needs
+    it again, all while the persistent kernel runs; every answer equals the
+    run with every table resident, and the budget is never exceeded."""
+    import torch
+    from warpcore_b200.serve import ServedWorkload, run
+    # (every table takes about 8 MB under the capacity rule; at 2000
+    # requests/s a table is often idle and evicted before its next request)
+    w = ServedWorkload(num_tables=24, cap_lo=1 << 12, cap_hi=1 << 16, num_requests=300,
+                       batch_lo=1 << 4, batch_hi=1 << 11, rate=2e3, seed=13)
+    w.admit()
+    w.reset()
+    run(w, "plain", streams=1)
+    alone = w.out.clone()
+    assert w.verify()
+    budget = w.table_bytes // 3
+    w.admit(dynamic=True, budget_bytes=budget)
+    w.reset()
+    res = run(w, "persistent", max_batch_keys=64)
+    st = w.pool_stats()
+    assert res["requests"] == 300
+    assert torch.equal(alone, w.out)
+    assert w.verify()
+    assert st["admissions"] > 24 and st["evictions"] > 0 and st["restores"] > 0
+    assert st["peak_bytes"] <= budget
+    w.close()

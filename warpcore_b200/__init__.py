@@ -211,6 +211,19 @@ class ServeOptions(ctypes.Structure):
         ("blocks_per_sm", ctypes.c_uint32),
         ("reserved", ctypes.c_uint32),
         ("probing_length", ctypes.c_uint64),
+        ("pool", ctypes.c_void_p),
+    ]
+
+
+class TablePoolStats(ctypes.Structure):
+    _fields_ = [
+        ("admissions", ctypes.c_uint64),
+        ("restores", ctypes.c_uint64),
+        ("evictions", ctypes.c_uint64),
+        ("waits", ctypes.c_uint64),
+        ("peak_bytes", ctypes.c_uint64),
+        ("resident_bytes", ctypes.c_uint64),
+        ("resident_tables", ctypes.c_uint64),
     ]
 
 
@@ -350,6 +363,13 @@ SIGNATURES = {
     "wc_pserver_poll": (_i, [_vp, _u64, ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_double)]),
     "wc_pserver_now_us": (_i, [_vp, ctypes.POINTER(ctypes.c_double)]),
     "wc_pserver_stop": (_i, [_vp]),
+    "wc_table_pool_create": (_i, [_u64, _pp]),
+    "wc_table_pool_add": (_i, [_vp, ctypes.POINTER(TableConfig), _u64, _u64, ctypes.POINTER(_u64)]),
+    "wc_table_pool_table": (_i, [_vp, _u64, _pp]),
+    "wc_table_pool_get_stats": (_i, [_vp, ctypes.POINTER(TablePoolStats)]),
+    "wc_table_pool_destroy": (_i, [_vp]),
+    "wc_svht_memory_bytes": (_i, [ctypes.POINTER(TableConfig), _u64, ctypes.POINTER(_u64)]),
+    "wc_svht_create_on": (_i, [ctypes.POINTER(TableConfig), _u64, _u64, _i, _vp, _u64, _vp, _pp]),
 }
 
 _lib = None
@@ -385,6 +405,13 @@ def _load_tuning(l):
     with open(path) as f:
         for kb, op, lb, sb, block, bps in json.load(f)["entries"]:
             l.wc_tune_set(kb, op, lb, sb, block, bps)
+
+
+def wc_svht_default_config_py(key_bytes, value_bytes):
+    """wc_svht_default_config as a TableConfig"""
+    cfg = TableConfig()
+    lib().wc_svht_default_config(ctypes.byref(cfg), int(key_bytes), int(value_bytes))
+    return cfg
 
 
 def _check(rc):

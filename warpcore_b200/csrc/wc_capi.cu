@@ -460,6 +460,7 @@ struct wc_table {
     uint32_t *status = nullptr;            /* device Status word */
     unsigned long long *counter = nullptr; /* device scratch counter */
     unsigned long long *live = nullptr;    /* device: kLiveStripes valid-key counters */
+    bool owns_memory = true;               /* false: placed on caller memory */
     int device = 0;
     uint64_t keys_inserted = 0; /* since init: an upper bound of size(), for tuning */
     L2Window l2;                /* access-policy window over the slots, if they fit */
@@ -559,8 +560,27 @@ int fill_slots(wc_table *t, cudaStream_t stream)
     return WC_OK;
 }
 
+/* Memory of a table placed on caller-provided device memory: the slots at
+ * offset 0, the small device block (Status word, counters) at the next
+ * 256-byte boundary, then the fingerprints if the policy gives them. */
+struct TablePlacement {
+    uint64_t slot_bytes, fp_bytes, aux_off, fp_off, total;
+};
+
+TablePlacement placement(uint64_t cap, uint32_t slot_bytes, bool fingerprints)
+{
+    TablePlacement p;
+    p.slot_bytes = cap * slot_bytes;
+    p.fp_bytes = fingerprints ? cap : 0;
+    p.aux_off = (p.slot_bytes + 255) & ~uint64_t(255);
+    p.fp_off = p.aux_off + ((kAuxBytes + 255) & ~uint64_t(255));
+    p.total = p.fp_off + p.fp_bytes;
+    return p;
+}
+
 int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, uint64_t seed,
-                 uint64_t max_count, int no_init, wc_table **out)
+                 uint64_t max_count, int no_init, wc_table **out, void *memory = nullptr,
+                 uint64_t memory_bytes = 0, cudaStream_t stream = nullptr)
 {
     if (!out) return fail(WC_ERR_INVALID_ARGUMENT, "out is NULL");
     *out = nullptr;
@@ -594,9 +614,48 @@ int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, ui
     t->max_count = kind == 2 ? (max_count < vmax ? max_count : vmax) : ~0ull;
     cudaGetDevice(&t->device);
 
-    /* the reference checks free memory before allocating (storage.cuh:464-473) */
     const uint64_t bytes = cap * t->slot_bytes;
     const uint64_t fp_bytes = (kind != 3 && want_fingerprints(bytes)) ? cap : 0;
+    if (memory) {
+        /* caller-provided memory: carve the slots, the device block and the
+         * fingerprints out of it; the table does not free it */
+        const TablePlacement pl = placement(cap, t->slot_bytes, fp_bytes != 0);
+        if (memory_bytes < pl.total || (reinterpret_cast<uintptr_t>(memory) & 255)) {
+            delete t;
+            return fail(WC_ERR_INVALID_ARGUMENT,
+                        "memory must be 256-byte aligned and hold %llu bytes",
+                        (unsigned long long)pl.total);
+        }
+        unsigned char *base = reinterpret_cast<unsigned char *>(memory);
+        t->owns_memory = false;
+        t->slots = base;
+        t->status = reinterpret_cast<uint32_t *>(base + pl.aux_off);
+        t->counter = reinterpret_cast<unsigned long long *>(base + pl.aux_off + 128);
+        t->num_keys = reinterpret_cast<unsigned long long *>(base + pl.aux_off + 192);
+        t->live = reinterpret_cast<unsigned long long *>(base + pl.aux_off + 256);
+        t->fps = fp_bytes ? base + pl.fp_off : nullptr;
+        if (no_init == 2) {
+            /* the memory holds a table image of this configuration */
+            t->initialized = true;
+        } else {
+            cudaError_t e = cudaMemsetAsync(t->status, 0, kAuxBytes, stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+            if (e != cudaSuccess) {
+                delete t;
+                return cuda_fail(e, "cudaMemsetAsync");
+            }
+            if (!no_init) {
+                rc = wc_table_init(t, t->seed, reinterpret_cast<wc_stream_t>(stream));
+                if (rc) {
+                    delete t;
+                    return rc;
+                }
+            }
+        }
+        *out = t;
+        return WC_OK;
+    }
+    /* the reference checks free memory before allocating (storage.cuh:464-473) */
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
         delete t;
@@ -769,6 +828,44 @@ int table_op(wc_table *t, int op, const void *keys, const void *values, void *ou
 
 } // namespace
 
+/* Bytes [off, off + len) of the memory image of an empty single-value
+ * table placed on caller memory (wc_svht_create_on's layout): empty slots
+ * (the empty key, payload 0), then zeros (padding, the Status word and
+ * counters, empty fingerprints).  Copying this image in and adopting it
+ * (no_init 2) equals wc_svht_create_on with no_init 0 without a kernel. */
+int warpcore::b200::host_svht_empty_image(const wc_table_config *cfg, uint64_t min_capacity,
+                                          unsigned char *dst, uint64_t off, uint64_t len)
+{
+    int rc = check_config(cfg, 0);
+    if (rc) return rc;
+    const uint64_t cap = valid_capacity(min_capacity, cfg->cg_size);
+    const uint32_t sb = cfg->value_bytes == cfg->key_bytes ? 2 * cfg->key_bytes : 16;
+    const uint64_t slot_total = cap * sb;
+    const uint64_t e = cfg->empty_key & key_mask(cfg->key_bytes);
+    unsigned char pat[16] = {0};
+    std::memcpy(pat, &e, cfg->key_bytes); /* key first, payload (and padding) zero */
+    const uint64_t in_slots = off < slot_total ? (slot_total - off < len ? slot_total - off : len) : 0;
+    /* the slot pattern from the first slot boundary on, doubled by copies */
+    uint64_t head = (sb - off % sb) % sb;
+    if (head > in_slots) head = in_slots;
+    for (uint64_t i = 0; i < head; ++i) dst[i] = pat[(off + i) % sb];
+    uint64_t filled = 0;
+    unsigned char *body = dst + head;
+    const uint64_t body_len = in_slots - head;
+    if (body_len) {
+        const uint64_t first = body_len < sb ? body_len : sb;
+        std::memcpy(body, pat, first);
+        filled = first;
+        while (filled < body_len) {
+            const uint64_t n = filled < body_len - filled ? filled : body_len - filled;
+            std::memcpy(body + filled, body, n);
+            filled += n;
+        }
+    }
+    if (len > in_slots) std::memset(dst + in_slots, 0, len - in_slots);
+    return WC_OK;
+}
+
 int warpcore::b200::host_svht_view(const wc_table *t, TableView *view, int *layout, uint32_t *cg,
                                    uint64_t probing_length, uint64_t *max_windows_out)
 {
@@ -829,6 +926,29 @@ int wc_svht_create(const wc_table_config *cfg, uint64_t min_capacity, uint64_t s
     return table_create(0, cfg, min_capacity, seed, 0, no_init, out);
 }
 
+int wc_svht_memory_bytes(const wc_table_config *cfg, uint64_t min_capacity, uint64_t *bytes_out)
+{
+    if (!bytes_out) return fail(WC_ERR_INVALID_ARGUMENT, "bytes_out is NULL");
+    *bytes_out = 0;
+    int rc = check_config(cfg, 0);
+    if (rc) return rc;
+    const uint64_t cap = valid_capacity(min_capacity, cfg->cg_size);
+    if (cap == 0) return fail(WC_ERR_INVALID_ARGUMENT, "min_capacity exceeds the largest table capacity");
+    const uint32_t sb = cfg->value_bytes == cfg->key_bytes ? 2 * cfg->key_bytes : 16;
+    *bytes_out = placement(cap, sb, want_fingerprints(cap * sb)).total;
+    return WC_OK;
+}
+
+int wc_svht_create_on(const wc_table_config *cfg, uint64_t min_capacity, uint64_t seed,
+                      int no_init, void *memory, uint64_t memory_bytes, wc_stream_t stream,
+                      wc_table **out)
+{
+    if (!memory) return fail(WC_ERR_INVALID_ARGUMENT, "memory is NULL");
+    if (no_init < 0 || no_init > 2) return fail(WC_ERR_INVALID_ARGUMENT, "no_init must be 0, 1 or 2");
+    return table_create(0, cfg, min_capacity, seed, 0, no_init, out, memory, memory_bytes,
+                        reinterpret_cast<cudaStream_t>(stream));
+}
+
 int wc_hashset_create(const wc_table_config *cfg, uint64_t min_capacity, uint64_t seed,
                       wc_table **out)
 {
@@ -844,6 +964,10 @@ int wc_counting_create(const wc_table_config *cfg, uint64_t min_capacity, uint64
 int wc_table_destroy(wc_table *t)
 {
     if (!t) return WC_OK;
+    if (!t->owns_memory) {
+        delete t;
+        return WC_OK;
+    }
     if (t->slots) cudaFree(t->slots);
     if (t->fps) cudaFree(t->fps);
     if (t->status) cudaFree(t->status);

@@ -106,6 +106,11 @@ int partition_by_bloom_block(const void *keys, uint64_t n, uint32_t key_bytes, u
 /* kernels this library launched (wc_launch_count) */
 void note_launches(uint32_t n);
 
+/* bytes [off, off + len) of the memory image of an empty single-value
+ * table placed by wc_svht_create_on */
+int host_svht_empty_image(const wc_table_config *cfg, uint64_t min_capacity, unsigned char *dst,
+                          uint64_t off, uint64_t len);
+
 /* the device view, slot layout and window width of an initialized
  * single-value table, and the windows a probing length allows */
 int host_svht_view(const wc_table *t, TableView *view, int *layout, uint32_t *cg,

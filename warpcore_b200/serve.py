@@ -16,9 +16,17 @@ earlier requests of the same table inserted, so every request's answer is
 fixed by arrival order. The expected outputs are computed from the indices,
 without the tables.
 
-Admission: tables are created, resident for the whole run, in table order
-while the sum of their device bytes stays within `budget_bytes`. Requests
-for a table that was not admitted are rejected before the run and counted.
+Admission, two policies:
+- static (admit()): tables are created, resident for the whole run, in
+  table order while the sum of their device bytes stays within
+  `budget_bytes`; requests for a table that was not admitted are rejected
+  before the run and counted;
+- dynamic (admit(dynamic=True), persistent form only): every table is
+  registered in a table pool (wc_table_pool) with the budget and none is
+  resident; a table is placed in device memory when its first request
+  runs, and when the budget (resident tables plus the buffers of requests
+  in flight) has no room, the least recently used idle tables are copied
+  out to host memory and restored when a request needs them again.
 """
 import ctypes
 import math
@@ -161,6 +169,8 @@ class ServedWorkload:
         self.admitted = np.zeros(num_tables, dtype=bool)
         self.table_bytes = 0
         self.rejected = 0
+        self.pool = None      # table pool handle (dynamic admission)
+        self.dynamic = False
 
     def admission_plan(self):
         """tables admitted in table order while their device bytes (the
@@ -174,13 +184,22 @@ class ServedWorkload:
                 used += need
         return plan, used
 
-    def admit(self):
+    def admit(self, dynamic=False, budget_bytes=None):
         """create the admitted tables; they stay resident for the run.
+        dynamic=True instead registers every table in a table pool with the
+        budget (`budget_bytes`, default the workload's) and creates none.
         When the resident tables together exceed L2, none gets an L2
         persistence window: windows on the first few tables would only
         take L2 away from the many others (measured: -7 % aggregate at
         1M requests/s on 41 GiB of tables)."""
         import torch
+        if dynamic:
+            self.dynamic = True
+            self.pool_budget = int(self.budget_bytes if budget_bytes is None else budget_bytes)
+            self._new_pool()
+            self.admitted = np.ones(self.num_tables, dtype=bool)
+            self.rejected = 0
+            return
         plan, used = self.admission_plan()
         windows = used <= torch.cuda.get_device_properties(0).L2_cache_size
         prev = set_l2_persistence(windows)
@@ -193,7 +212,43 @@ class ServedWorkload:
         self.table_bytes = used
         self.rejected = int((~plan[self.table]).sum())
 
+    def _new_pool(self):
+        from . import TableConfig, lib as _lib, wc_svht_default_config_py
+        if self.pool is not None:
+            _lib().wc_table_pool_destroy(self.pool)
+            self.pool = None
+        h = ctypes.c_void_p()
+        _check(_lib().wc_table_pool_create(self.pool_budget, ctypes.byref(h)))
+        self.pool = h
+        cfg = wc_svht_default_config_py(4, 4)
+        tid = ctypes.c_uint64()
+        for t in range(self.num_tables):
+            _check(_lib().wc_table_pool_add(h, ctypes.byref(cfg), int(self.caps[t]),
+                                            0x5AD0DED, ctypes.byref(tid)))
+            assert tid.value == t
+        self.table_bytes = 0
+
+    def pool_stats(self):
+        from . import TablePoolStats
+        st = TablePoolStats()
+        _check(lib().wc_table_pool_get_stats(self.pool, ctypes.byref(st)))
+        return {k: int(getattr(st, k)) for k, _ in st._fields_}
+
+    def close(self):
+        if self.pool is not None:
+            lib().wc_table_pool_destroy(self.pool)
+            self.pool = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
     def reset(self):
+        """every table empty again (dynamic: a fresh pool, nothing resident)"""
+        if self.dynamic:
+            self._new_pool()
         for t in self.tables:
             if t is not None:
                 t.init()
@@ -209,7 +264,7 @@ class ServedWorkload:
         for i, r in enumerate(keep):
             q = arr[i]
             q.arrival_us = float(self.arrival_us[r])
-            q.table = self.tables[self.table[r]]._h.value
+            q.table = None if self.dynamic else self.tables[self.table[r]]._h.value
             q.table_id = int(self.table[r])
             q.op = int(self.op[r])
             off = int(self.offsets[r]) * 4
@@ -249,6 +304,10 @@ def run(workload, mode, streams=4, depth=2, max_batch_requests=4096, max_batch_k
     opt.max_batch_keys = max_batch_keys
     opt.blocks_per_sm = blocks_per_sm
     opt.probing_length = DEFAULT_PROBING_LENGTH
+    if workload.dynamic:
+        if mode != "persistent":
+            raise ValueError("dynamic admission runs with the persistent form")
+        opt.pool = workload.pool.value
     issue = (ctypes.c_double * n)()
     done = (ctypes.c_double * n)()
     stats = ServeStats()
