@@ -420,6 +420,17 @@ template <>
 struct layout_of<std::uint64_t, void> { using type = b200::LayoutSet64; };
 
 /* device-usable description of a table handle, refreshed from the C ABI */
+/* the launch geometry measured by the autotuner (tuning_b200.json next to
+ * the library, or WARPCORE_B200_TUNING), loaded once per process */
+inline void load_tuning_once()
+{
+    static const int loaded = [] {
+        std::uint64_t n = 0;
+        return wc_tune_load(nullptr, &n);
+    }();
+    (void)loaded;
+}
+
 inline b200::TableView view_from(const wc_table_info &inf)
 {
     b200::TableView v{};

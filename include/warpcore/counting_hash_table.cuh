@@ -53,6 +53,7 @@ class CountingHashTable {
     {
         const wc_table_config cfg =
             detail::make_config<ProbingScheme, Key>(sizeof(Value), EmptyKey, TombstoneKey);
+        detail::load_tuning_once();
         if (wc_counting_create(&cfg, min_capacity, std::uint64_t(seed), std::uint64_t(max_count),
                                no_init ? 1 : 0, &handle_) == WC_OK)
             refresh();

@@ -41,6 +41,7 @@ class HashSet {
     explicit HashSet(index_type min_capacity, key_type seed = defaults::seed<key_type>()) noexcept
     {
         const wc_table_config cfg = detail::make_config<ProbingScheme, Key>(0, EmptyKey, TombstoneKey);
+        detail::load_tuning_once();
         if (wc_hashset_create(&cfg, min_capacity, std::uint64_t(seed), &handle_) == WC_OK) refresh();
     }
     __host__ __device__ HashSet(const HashSet &o) noexcept

@@ -55,6 +55,7 @@ class SingleValueHashTable {
     {
         const wc_table_config cfg =
             detail::make_config<ProbingScheme, Key>(sizeof(Value), EmptyKey, TombstoneKey);
+        detail::load_tuning_once();
         if (wc_svht_create(&cfg, min_capacity, std::uint64_t(seed), no_init ? 1 : 0, &handle_) ==
             WC_OK)
             refresh();

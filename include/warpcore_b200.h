@@ -637,6 +637,12 @@ int wc_tune_set(uint32_t key_bytes, int op, uint32_t load_bucket, uint32_t size_
                 uint32_t block_threads, uint32_t blocks_per_sm);
 /* forget every tuned entry */
 int wc_tune_reset(void);
+/* Loads a tuning file written by `python -m warpcore_b200.autotune` (its
+ * "entries": one wc_tune_set each).  path NULL: the environment variable
+ * WARPCORE_B200_TUNING, else tuning_b200.json next to this library; "none"
+ * loads nothing.  *loaded (if not NULL) gets the number of entries.  The
+ * Python binding and the C++ class templates call it once. */
+int wc_tune_load(const char *path, uint64_t *loaded);
 
 /* ------------------------------------------------------------------ */
 /* Batches: many requests on many tables in one launch                  */

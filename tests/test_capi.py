@@ -107,3 +107,21 @@ def test_shipped_tuning_table_is_well_formed():
     for kb, op, lb, sb, block, bps in d["entries"]:
         assert kb in (4, 8) and op in (0, 1, 2) and 0 <= lb < 4 and 0 <= sb < 12
         assert block in (32, 64, 128, 256)
+
+
+def test_tune_load_reads_the_committed_table():
+    """wc_tune_load (used by the Python binding and the C++ headers) parses
+    the committed tuning file's entries; a missing file is an error and
+    "none" loads nothing (no GPU needed)"""
+    import ctypes
+    import json
+    import os
+    import warpcore_b200 as wc
+    path = os.path.join(os.path.dirname(wc.__file__), "tuning_b200.json")
+    n = ctypes.c_uint64(0)
+    assert wc.lib().wc_tune_load(path.encode(), ctypes.byref(n)) == 0
+    assert n.value == len(json.load(open(path))["entries"]) > 0
+    assert wc.lib().wc_tune_load(b"none", ctypes.byref(n)) == 0 and n.value == 0
+    assert wc.lib().wc_tune_load(b"/nonexistent/tuning.json", ctypes.byref(n)) != 0
+    # the library's own default location is the same file
+    assert wc.lib().wc_tune_load(None, ctypes.byref(n)) == 0 and n.value > 0

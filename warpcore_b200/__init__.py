@@ -352,6 +352,7 @@ SIGNATURES = {
     "wc_table_l2_window": (_i, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(ctypes.c_float)]),
     "wc_tune_set": (_i, [_u32, _i, _u32, _u32, _u32, _u32]),
     "wc_tune_reset": (_i, []),
+    "wc_tune_load": (_i, [ctypes.c_char_p, ctypes.POINTER(_u64)]),
     "wc_batch_create": (_i, [_u32, _u32, _pp]),
     "wc_batch_destroy": (_i, [_vp]),
     "wc_batch_run": (_i, [_vp, ctypes.POINTER(BatchRequest), _u32, _vp, _u64, _u32]),
@@ -397,14 +398,13 @@ def lib():
 
 
 def _load_tuning(l):
-    """launch geometry measured by warpcore_b200.autotune (tuning_b200.json)"""
-    import json
+    """launch geometry measured by warpcore_b200.autotune (tuning_b200.json),
+    loaded by the library itself (wc_tune_load), as the C++ headers do"""
     path = os.environ.get("WARPCORE_B200_TUNING") or os.path.join(_HERE, "tuning_b200.json")
     if path == "none" or not os.path.exists(path):
         return
-    with open(path) as f:
-        for kb, op, lb, sb, block, bps in json.load(f)["entries"]:
-            l.wc_tune_set(kb, op, lb, sb, block, bps)
+    n = ctypes.c_uint64(0)
+    l.wc_tune_load(path.encode(), ctypes.byref(n))
 
 
 def wc_svht_default_config_py(key_bytes, value_bytes):

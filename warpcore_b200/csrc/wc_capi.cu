@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <dlfcn.h>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -1458,6 +1459,72 @@ int wc_tune_set(uint32_t key_bytes, int op, uint32_t load_bucket, uint32_t size_
         return fail(WC_ERR_INVALID_ARGUMENT, "block_threads must be a multiple of 32, at most 256");
     std::lock_guard<std::mutex> lock(g_tune_mu);
     g_tune[key_bytes == 8][op][load_bucket][size_bucket] = TuneEntry{block_threads, blocks_per_sm_};
+    return WC_OK;
+}
+
+/* Reads the "entries" array of a tuning file written by
+ * warpcore_b200.autotune: [[key_bytes, op, load_bucket, size_bucket,
+ * block_threads, blocks_per_sm], ...].  Only that array is parsed: numbers
+ * in brackets after the "entries" key, six per entry. */
+int wc_tune_load(const char *path, uint64_t *loaded)
+{
+    std::string file;
+    if (path) {
+        file = path;
+    } else if (const char *env = std::getenv("WARPCORE_B200_TUNING")) {
+        file = env;
+    } else {
+        /* tuning_b200.json next to this library */
+        Dl_info info;
+        if (!dladdr(reinterpret_cast<void *>(&wc_tune_load), &info) || !info.dli_fname)
+            return fail(WC_ERR_INVALID_ARGUMENT, "cannot locate the library");
+        file = info.dli_fname;
+        const size_t slash = file.rfind('/');
+        file = (slash == std::string::npos ? std::string(".") : file.substr(0, slash)) +
+               "/tuning_b200.json";
+    }
+    if (loaded) *loaded = 0;
+    if (file == "none") return WC_OK;
+    FILE *f = std::fopen(file.c_str(), "rb");
+    if (!f) return fail(WC_ERR_INVALID_ARGUMENT, "cannot open tuning file %s", file.c_str());
+    std::string text;
+    char buf[65536];
+    size_t got;
+    while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, got);
+    std::fclose(f);
+    size_t pos = text.find("\"entries\"");
+    if (pos == std::string::npos) return fail(WC_ERR_INVALID_ARGUMENT, "no entries in %s", file.c_str());
+    pos = text.find('[', pos);
+    if (pos == std::string::npos) return fail(WC_ERR_INVALID_ARGUMENT, "malformed %s", file.c_str());
+    ++pos; /* inside the outer array */
+    uint64_t n = 0;
+    for (;;) {
+        while (pos < text.size() && (text[pos] == ' ' || text[pos] == '\n' || text[pos] == '\r' ||
+                                     text[pos] == '\t' || text[pos] == ','))
+            ++pos;
+        if (pos >= text.size()) return fail(WC_ERR_INVALID_ARGUMENT, "malformed %s", file.c_str());
+        if (text[pos] == ']') break;
+        if (text[pos] != '[') return fail(WC_ERR_INVALID_ARGUMENT, "malformed %s", file.c_str());
+        ++pos;
+        unsigned long long v[6];
+        for (int i = 0; i < 6; ++i) {
+            while (pos < text.size() && (text[pos] == ' ' || text[pos] == ',' || text[pos] == '\n'))
+                ++pos;
+            char *end = nullptr;
+            v[i] = std::strtoull(text.c_str() + pos, &end, 10);
+            if (end == text.c_str() + pos)
+                return fail(WC_ERR_INVALID_ARGUMENT, "malformed entry in %s", file.c_str());
+            pos = size_t(end - text.c_str());
+        }
+        pos = text.find(']', pos);
+        if (pos == std::string::npos) return fail(WC_ERR_INVALID_ARGUMENT, "malformed %s", file.c_str());
+        ++pos;
+        const int rc = wc_tune_set(uint32_t(v[0]), int(v[1]), uint32_t(v[2]), uint32_t(v[3]),
+                                   uint32_t(v[4]), uint32_t(v[5]));
+        if (rc) return rc;
+        ++n;
+    }
+    if (loaded) *loaded = n;
     return WC_OK;
 }
 

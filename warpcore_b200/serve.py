@@ -91,8 +91,12 @@ class ServedWorkload:
 
     def __init__(self, num_tables=4096, cap_lo=1 << 10, cap_hi=1 << 22, load=0.85,
                  num_requests=8192, batch_lo=1 << 6, batch_hi=1 << 18, insert_frac=0.3,
-                 hit_frac=0.8, rate=100000.0, seed=5, budget_bytes=64 << 30, device="cuda"):
+                 hit_frac=0.8, rate=100000.0, seed=5, budget_bytes=64 << 30, device="cuda",
+                 cg_size=None):
         import torch
+        # the window width of the tables this layer creates itself: the
+        # autotuner's choice (tuning_b200.json, "serving"), else 8
+        self.cg_size = int(cg_size or serving_tuning().get("cg_size", 8))
         rng = np.random.default_rng(seed)
         self.num_tables = num_tables
         self.caps = np.exp(rng.uniform(math.log(cap_lo), math.log(cap_hi), num_tables)).astype(np.int64)
@@ -178,7 +182,7 @@ class ServedWorkload:
         used = 0
         plan = np.zeros(self.num_tables, dtype=bool)
         for t in range(self.num_tables):
-            need = valid_capacity(int(self.caps[t]), 8) * 8 + 256
+            need = valid_capacity(int(self.caps[t]), self.cg_size) * 8 + 256
             if used + need <= self.budget_bytes:
                 plan[t] = True
                 used += need
@@ -205,7 +209,8 @@ class ServedWorkload:
         prev = set_l2_persistence(windows)
         try:
             for t in np.nonzero(plan)[0]:
-                self.tables[t] = SingleValueHashTable(int(self.caps[t]), key_bytes=4)
+                self.tables[t] = SingleValueHashTable(int(self.caps[t]), key_bytes=4,
+                                                      cg_size=self.cg_size)
         finally:
             set_l2_persistence(prev)
         self.admitted = plan
@@ -221,6 +226,7 @@ class ServedWorkload:
         _check(_lib().wc_table_pool_create(self.pool_budget, ctypes.byref(h)))
         self.pool = h
         cfg = wc_svht_default_config_py(4, 4)
+        cfg.cg_size = self.cg_size
         tid = ctypes.c_uint64()
         for t in range(self.num_tables):
             _check(_lib().wc_table_pool_add(h, ctypes.byref(cfg), int(self.caps[t]),
@@ -288,11 +294,28 @@ class ServedWorkload:
         return ok_hits and ok_miss
 
 
-def run(workload, mode, streams=4, depth=2, max_batch_requests=4096, max_batch_keys=0,
+def serving_tuning():
+    """the "serving" section of the tuning file (cg_size, chunk_keys), or {}"""
+    import json
+    import os
+    path = os.environ.get("WARPCORE_B200_TUNING") or os.path.join(
+        os.path.dirname(os.path.abspath(__file__)), "tuning_b200.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get("serving", {}) or {}
+    except (OSError, ValueError):
+        return {}
+
+
+def run(workload, mode, streams=4, depth=2, max_batch_requests=4096, max_batch_keys=None,
         blocks_per_sm=0):
     """Replays the workload in `mode` ("plain", "batched" or "persistent");
     returns a dict with throughput, latency percentiles and launch counts.
-    For "persistent", max_batch_keys is the chunk size (0: 1024 keys)."""
+    For "persistent", max_batch_keys is the largest chunk (default: the
+    autotuner's chunk_keys, else 1024 keys); for "batched" the keys per batch
+    (default no limit)."""
+    if max_batch_keys is None:
+        max_batch_keys = int(serving_tuning().get("chunk_keys", 0)) if mode == "persistent" else 0
     reqs, keep = workload.requests()
     n = len(keep)
     opt = ServeOptions()
