@@ -156,14 +156,22 @@ from warpcore_b200.datagen import (unique_keys32, unique_keys64,  # noqa: E402
 class Workload:
     """one step = init + insert(n) + retrieve(q) on resident inputs"""
 
-    def __init__(self, kind, log2n, load, rank, device, world=1, shard=False, bucket=2):
+    def __init__(self, kind, log2n, load, rank, device, world=1, shard=False, bucket=2,
+                 fill=False):
         import torch
         import warpcore_b200 as wc
         self.kind = kind
         self.n = 1 << log2n
+        # the table of min capacity 2^L / load under the capacity rule; with
+        # `fill` it is filled to a real load of `load` (n = load x capacity)
+        # instead of holding 2^L keys
+        self.table_min_cap = int(self.n / load)
+        if fill and kind in ("svht32", "svht64", "hashset64") and not shard:
+            cg = 16 if kind == "hashset64" else 8
+            self.n = int(load * wc.valid_capacity(self.table_min_cap, cg))
         # svht32 is the small configuration: every inserted key queried once
-        # plus as many absent keys; the others query 2^L keys, half of them hits
-        self.q = (2 << log2n) if kind == "svht32" else (1 << log2n)
+        # plus as many absent keys; the others query n keys, half of them hits
+        self.q = 2 * self.n if kind == "svht32" else self.n
         self.load = load
         self.device = device
         gen = torch.Generator(device=device)
@@ -190,7 +198,7 @@ class Workload:
             self.expected = exp[perm].contiguous()
             self.hit = hit[perm].contiguous()
             if kind == "hashset64":
-                self.table = wc.HashSet(int(n / load), key_bytes=8)
+                self.table = wc.HashSet(self.table_min_cap, key_bytes=8)
                 self.out = torch.empty(q, dtype=torch.uint8, device=device)
                 self.bytes_insert, self.bytes_retrieve = 8 + 32 + 32, 8 + 1 + 32
             elif shard and kind != "hashset64":
@@ -204,7 +212,7 @@ class Workload:
                 self.bytes_insert = kb + kb + 32 + 32
                 self.bytes_retrieve = kb + kb + 1 + 32
             else:
-                self.table = wc.SingleValueHashTable(int(n / load), key_bytes=kb)
+                self.table = wc.SingleValueHashTable(self.table_min_cap, key_bytes=kb)
                 self.out = torch.empty(q, dtype=self.values.dtype, device=device)
                 self.bytes_insert = kb + kb + 32 + 32
                 self.bytes_retrieve = kb + kb + 1 + 32
@@ -470,7 +478,7 @@ def reference_gpu(wl, reps=5):
     vp = ctypes.c_void_p
     torch.cuda.synchronize()
     out = torch.empty_like(wl.out)
-    min_cap = int(wl.n / wl.load) if wl.kind != "counting32" else int(wl.distinct / wl.load)
+    min_cap = wl.table_min_cap if wl.kind != "counting32" else int(wl.distinct / wl.load)
     rb = re_ = None
     st = words = None
     nslots = ctypes.c_uint64(0)
@@ -616,7 +624,7 @@ def run_ours(args):
     warpcore_b200.lib()
 
     wl = Workload(args.workload, args.log2n, args.load, rank, device, world, bucket=args.bucket,
-                  shard=args.shard or world > 1)
+                  shard=args.shard or world > 1, fill=args.fill)
     stream = torch.cuda.Stream(device=device)
     torch.cuda.synchronize()
     verified = wl.verify()
@@ -709,8 +717,14 @@ def run_ours(args):
             "data": "synthetic (seeded uniform unique keys, uniform values; inputs resident in HBM)",
             "config": {
                 "workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n, L1=args.log2n + 1, L3=args.log2n - 3,
-                                                         LF=args.load, B=args.bucket),
+                                                         LF=args.load, B=args.bucket)
+                            + ("; filled: %d keys (load x capacity) instead of 2^%d" % (wl.n, args.log2n)
+                               if wl.n != (1 << args.log2n) and args.fill else ""),
                 "capacity": int(wl.table.capacity) if hasattr(wl.table, "capacity") else None,
+                "keys_inserted": wl.n,
+                "real_load": (round(wl.n / wl.table.capacity, 4)
+                              if args.workload in ("svht32", "svht64", "hashset64") else None),
+                "filled": bool(args.fill),
                 "ops_per_step": ops_step,
                 "l2": "inputs larger than L2 (no flush)" if args.log2n >= 24 else "inputs may be L2-resident",
                 "parallelism": ("table sharded over %d GPU(s): keys routed to owners by "
@@ -1151,6 +1165,9 @@ def main():
                     help="keys per step (2^L); default 27, or 24 pairs for mv32")
     ap.add_argument("--load", type=float, default=None,
                     help="target load factor; default 0.9, or 0.8 for mv32")
+    ap.add_argument("--fill", action="store_true",
+                    help="svht32/svht64/hashset64: fill the table of min capacity 2^L/load to a "
+                         "real load of `load` (keys = load x capacity) instead of inserting 2^L")
     ap.add_argument("--cpu-log2n", type=int, default=24)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--shard", action="store_true",
