@@ -135,12 +135,37 @@ int ref_svht64_run(const uint64_t *keys, const uint64_t *vals, uint64_t n, const
         keys, vals, n, q, nq, out, min_cap, reps, ms_insert, ms_retrieve, capacity, status_out);
 }
 
+/* the same table stored as a struct of arrays (storage.cuh:218-432) */
+int ref_svht64_soa_run(const uint64_t *keys, const uint64_t *vals, uint64_t n, const uint64_t *q,
+                       uint64_t nq, uint64_t *out, uint64_t min_cap, int reps, float *ms_insert,
+                       float *ms_retrieve, uint64_t *capacity, uint32_t *status_out)
+{
+    using Soa = wc::SingleValueHashTable<uint64_t, uint64_t, wc::defaults::empty_key<uint64_t>(),
+                                         wc::defaults::tombstone_key<uint64_t>(),
+                                         wc::defaults::probing_scheme_t<uint64_t, 8>,
+                                         wc::storage::key_value::SoAStore<uint64_t, uint64_t>>;
+    return run_table<Soa>(keys, vals, n, q, nq, out, min_cap, reps, ms_insert, ms_retrieve,
+                          capacity, status_out);
+}
+
 int ref_svht32_run(const uint32_t *keys, const uint32_t *vals, uint64_t n, const uint32_t *q,
                    uint64_t nq, uint32_t *out, uint64_t min_cap, int reps, float *ms_insert,
                    float *ms_retrieve, uint64_t *capacity, uint32_t *status_out)
 {
     return run_table<wc::SingleValueHashTable<uint32_t, uint32_t>>(
         keys, vals, n, q, nq, out, min_cap, reps, ms_insert, ms_retrieve, capacity, status_out);
+}
+
+int ref_svht32_soa_run(const uint32_t *keys, const uint32_t *vals, uint64_t n, const uint32_t *q,
+                       uint64_t nq, uint32_t *out, uint64_t min_cap, int reps, float *ms_insert,
+                       float *ms_retrieve, uint64_t *capacity, uint32_t *status_out)
+{
+    using Soa = wc::SingleValueHashTable<uint32_t, uint32_t, wc::defaults::empty_key<uint32_t>(),
+                                         wc::defaults::tombstone_key<uint32_t>(),
+                                         wc::defaults::probing_scheme_t<uint32_t, 8>,
+                                         wc::storage::key_value::SoAStore<uint32_t, uint32_t>>;
+    return run_table<Soa>(keys, vals, n, q, nq, out, min_cap, reps, ms_insert, ms_retrieve,
+                          capacity, status_out);
 }
 
 /* HashSet<u64>: the host bulk retrieve does not compile (hash_set.cuh:356),

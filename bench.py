@@ -157,10 +157,13 @@ class Workload:
     """one step = init + insert(n) + retrieve(q) on resident inputs"""
 
     def __init__(self, kind, log2n, load, rank, device, world=1, shard=False, bucket=2,
-                 fill=False):
+                 fill=False, store="aos"):
         import torch
         import warpcore_b200 as wc
         self.kind = kind
+        # single-value tables: {key, value} slots ("aos") or a key array and a
+        # value array ("soa", SoAStore)
+        self.store = store if kind in ("svht32", "svht64") and not shard else "aos"
         self.n = 1 << log2n
         # the table of min capacity 2^L / load under the capacity rule; with
         # `fill` it is filled to a real load of `load` (n = load x capacity)
@@ -212,7 +215,8 @@ class Workload:
                 self.bytes_insert = kb + kb + 32 + 32
                 self.bytes_retrieve = kb + kb + 1 + 32
             else:
-                self.table = wc.SingleValueHashTable(self.table_min_cap, key_bytes=kb)
+                self.table = wc.SingleValueHashTable(self.table_min_cap, key_bytes=kb,
+                                                     store=self.store)
                 self.out = torch.empty(q, dtype=self.values.dtype, device=device)
                 self.bytes_insert = kb + kb + 32 + 32
                 self.bytes_retrieve = kb + kb + 1 + 32
@@ -486,7 +490,10 @@ def reference_gpu(wl, reps=5):
         # misses must stay untouched: the same fill as our verification run
         out.fill_(-1)
         st = torch.zeros(wl.q, dtype=torch.int32, device=out.device)
-        fn = lib.ref_svht64_run if wl.kind == "svht64" else lib.ref_svht32_run
+        if wl.store == "soa":
+            fn = lib.ref_svht64_soa_run if wl.kind == "svht64" else lib.ref_svht32_soa_run
+        else:
+            fn = lib.ref_svht64_run if wl.kind == "svht64" else lib.ref_svht32_run
         rc = fn(vp(wl.keys.data_ptr()), vp(wl.values.data_ptr()), u64(wl.n),
                 vp(wl.queries.data_ptr()), u64(wl.q), vp(out.data_ptr()), u64(min_cap),
                 ctypes.c_int(reps), ctypes.byref(ti), ctypes.byref(tr), ctypes.byref(cap),
@@ -624,7 +631,7 @@ def run_ours(args):
     warpcore_b200.lib()
 
     wl = Workload(args.workload, args.log2n, args.load, rank, device, world, bucket=args.bucket,
-                  shard=args.shard or world > 1, fill=args.fill)
+                  shard=args.shard or world > 1, fill=args.fill, store=args.store)
     stream = torch.cuda.Stream(device=device)
     torch.cuda.synchronize()
     verified = wl.verify()
@@ -719,7 +726,10 @@ def run_ours(args):
                 "workload": WORKLOAD_NAMES[args.workload].format(L=args.log2n, L1=args.log2n + 1, L3=args.log2n - 3,
                                                          LF=args.load, B=args.bucket)
                             + ("; filled: %d keys (load x capacity) instead of 2^%d" % (wl.n, args.log2n)
-                               if wl.n != (1 << args.log2n) and args.fill else ""),
+                               if wl.n != (1 << args.log2n) and args.fill else "")
+                            + ("; SoAStore (key array + value array) on both sides"
+                               if wl.store == "soa" else ""),
+                "store": wl.store,
                 "capacity": int(wl.table.capacity) if hasattr(wl.table, "capacity") else None,
                 "keys_inserted": wl.n,
                 "real_load": (round(wl.n / wl.table.capacity, 4)
@@ -1165,6 +1175,9 @@ def main():
                     help="keys per step (2^L); default 27, or 24 pairs for mv32")
     ap.add_argument("--load", type=float, default=None,
                     help="target load factor; default 0.9, or 0.8 for mv32")
+    ap.add_argument("--store", default="aos", choices=["aos", "soa"],
+                    help="svht32/svht64: slot layout of this library's table and of the "
+                         "reference build's (SoAStore for soa)")
     ap.add_argument("--fill", action="store_true",
                     help="svht32/svht64/hashset64: fill the table of min capacity 2^L/load to a "
                          "real load of `load` (keys = load x capacity) instead of inserting 2^L")

@@ -332,14 +332,14 @@ struct AoSStore {
     using value_type = Value;
     using tag = tags::key_value_storage;
 };
-/* SoAStore (storage.cuh:218-432): accepted wherever AoSStore is, as a
- * type, but it does NOT select a struct-of-arrays layout.  It names the same
- * key and value types; the tables choose their own layout in HBM whichever
- * store is named (single-value tables, sets and counters keep {key, value}
- * slots so that one compare-and-swap publishes both; the multi-bucket and
- * bucket-list tables keep keys apart from values).  Answers do not depend on
- * this parameter; code that relies on the SoA layout's memory (reading a
- * separate key array through the table's storage) is not supported. */
+/* SoAStore (storage.cuh:218-432): SingleValueHashTable<..., SoAStore<K, V>>
+ * stores its keys and values as two arrays (wc_svht_create_soa): the key
+ * array is probed like a hash set's slots, value i belongs to key slot i,
+ * and an insert writes the value after the key's compare-and-swap, as the
+ * reference's SoA store does.  The other tables accept the type and keep
+ * their own layout (counting tables {key, count} slots, so that a claim
+ * publishes both; multi-value tables their key and value arrays).  Answers
+ * do not depend on the store. */
 template <class Key, class Value>
 struct SoAStore {
     using key_type = Key;
@@ -419,6 +419,12 @@ struct layout_of<std::uint32_t, void> { using type = b200::LayoutSet32; };
 template <>
 struct layout_of<std::uint64_t, void> { using type = b200::LayoutSet64; };
 
+/* storage::key_value::SoAStore selects the struct-of-arrays layout */
+template <class Store>
+struct is_soa_store : std::false_type {};
+template <class K, class V>
+struct is_soa_store<storage::key_value::SoAStore<K, V>> : std::true_type {};
+
 /* device-usable description of a table handle, refreshed from the C ABI */
 /* the launch geometry measured by the autotuner (tuning_b200.json next to
  * the library, or WARPCORE_B200_TUNING), loaded once per process */
@@ -449,6 +455,7 @@ inline b200::TableView view_from(const wc_table_info &inf)
     v.hasher1 = inf.hasher1;
     v.hasher2 = inf.hasher2;
     v.cg_size = inf.cg_size;
+    v.values = inf.values;
     return v;
 }
 

@@ -34,6 +34,7 @@
 #define WARPCORE_B200_CORE_CUH
 
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace warpcore {
@@ -180,6 +181,8 @@ struct TableView {
     uint64_t magic_nb;   /* barrett_magic(num_buckets) */
     uint64_t magic_nb1;  /* barrett_magic(num_buckets - 1) */
     uint32_t probing, hasher1, hasher2, cg_size;
+    void *values;        /* struct-of-arrays tables: the value array, one
+                            value per slot index; NULL otherwise */
 };
 
 template <class K>
@@ -294,6 +297,24 @@ struct LayoutSet64 {
     static constexpr int kSlotBytes = 8;
     static constexpr bool kHasValue = false;
 };
+/* single-value table stored as a struct of arrays (SoAStore,
+ * storage.cuh:218-432): the slot array holds the keys only and is probed
+ * like a hash set's; the value of slot i is element i of a separate array
+ * (TableView::values).  An insert writes the value after the key's
+ * compare-and-swap, as the reference's SoA store does. */
+template <class K, class V>
+struct LayoutSoA {
+    using key_t = K;
+    using val_t = V;
+    static constexpr int kSlotBytes = int(sizeof(K));
+    static constexpr bool kHasValue = false; /* the slots carry no value */
+    static constexpr bool kSoA = true;
+};
+
+template <class L, class = void>
+struct is_soa : std::false_type {};
+template <class L>
+struct is_soa<L, std::void_t<decltype(L::kSoA)>> : std::integral_constant<bool, L::kSoA> {};
 
 /* up to 16 bytes of a probe window held by one lane */
 struct LaneWords {
@@ -448,6 +469,30 @@ __device__ __forceinline__ void store_value(void *sp, typename L::val_t v)
         volatile typename L::val_t *p = slot_value_ptr<L>(sp);
         *p = v;
     }
+}
+
+/* the value of slot index `slot` (address sp): in the slot, or in the
+ * value array of a struct-of-arrays table */
+template <class L>
+__device__ __forceinline__ void put_value(const TableView &t, void *sp, uint64_t slot,
+                                          typename L::val_t v)
+{
+    if constexpr (is_soa<L>::value) {
+        volatile typename L::val_t *p = reinterpret_cast<typename L::val_t *>(t.values) + slot;
+        *p = v;
+    } else {
+        store_value<L>(sp, v);
+    }
+}
+
+template <class L>
+__device__ __forceinline__ typename L::val_t get_soa_value(const TableView &t, uint64_t slot)
+{
+    using V = typename L::val_t;
+    if constexpr (sizeof(V) == 8)
+        return V(__ldcg(reinterpret_cast<const unsigned long long *>(t.values) + slot));
+    else
+        return V(__ldcg(reinterpret_cast<const unsigned int *>(t.values) + slot));
 }
 
 template <class L>

@@ -58,7 +58,7 @@ __device__ uint32_t tile_modify(const TableView &t, const Tile &g, typename L::k
                     st = kStDuplicateKey;
                     join = kStDuplicateKey;
                     if (r == leader) {
-                        if (op == 0) store_value<L>(sp, val);
+                        if (op == 0) put_value<L>(t, sp, b * W + r, val);
                         else if constexpr (L::kHasValue) count_add<L>(sp, 1u, t.max_count, st, join);
                     }
                     st = g.shfl(st, leader);
@@ -80,12 +80,13 @@ __device__ uint32_t tile_modify(const TableView &t, const Tile &g, typename L::k
                     const V payload = op == 1 ? V(1) : val;
                     if (claim_slot<L>(sp, empty, key, payload, old_key)) {
                         fp_store(t, b * W + r, fingerprint(key));
+                        if constexpr (is_soa<L>::value) put_value<L>(t, sp, b * W + r, val);
                         live_add(t, 1);
                         outcome = 1;
                     } else if (old_key == key) {
                         outcome = 2;
                         uint32_t s2 = kStDuplicateKey, j2 = kStDuplicateKey;
-                        if (op == 0) store_value<L>(sp, val);
+                        if (op == 0) put_value<L>(t, sp, b * W + r, val);
                         else if constexpr (L::kHasValue) count_add<L>(sp, 1u, t.max_count, s2, j2);
                         st = s2;
                         join = j2;
@@ -147,8 +148,11 @@ __device__ uint32_t tile_find(const TableView &t, const Tile &g, typename L::key
             if (hit) {
                 const unsigned leader = __ffs(hit) - 1;
                 V v = 0;
-                if (L::kHasValue && r == leader)
+                if constexpr (is_soa<L>::value) {
+                    if (r == leader) v = get_soa_value<L>(t, b * W + r);
+                } else if (L::kHasValue && r == leader) {
                     v = *slot_value_ptr<L>(const_cast<unsigned char *>(sp));
+                }
                 value_out = g.shfl(v, leader);
                 if (uint64_t(value_out) > t.max_count) value_out = V(t.max_count);
                 found = true;

@@ -36,7 +36,11 @@ class SingleValueHashTable {
 
     /* the value's bits, held in the slot as an unsigned word of its width */
     using value_word = typename std::conditional<sizeof(Value) == 4, std::uint32_t, std::uint64_t>::type;
-    using layout = typename detail::layout_of<Key, value_word>::type;
+    using key_word = typename std::conditional<sizeof(Key) == 4, std::uint32_t, std::uint64_t>::type;
+    static constexpr bool kSoA = detail::is_soa_store<TableStorage>::value;
+    /* {key, value} slots, or a key array and a value array (SoAStore) */
+    using layout = typename std::conditional<kSoA, b200::LayoutSoA<key_word, value_word>,
+                                             typename detail::layout_of<Key, value_word>::type>::type;
 
   public:
     using key_type = Key;
@@ -56,9 +60,11 @@ class SingleValueHashTable {
         const wc_table_config cfg =
             detail::make_config<ProbingScheme, Key>(sizeof(Value), EmptyKey, TombstoneKey);
         detail::load_tuning_once();
-        if (wc_svht_create(&cfg, min_capacity, std::uint64_t(seed), no_init ? 1 : 0, &handle_) ==
-            WC_OK)
-            refresh();
+        const int rc = kSoA ? wc_svht_create_soa(&cfg, min_capacity, std::uint64_t(seed),
+                                                 no_init ? 1 : 0, &handle_)
+                            : wc_svht_create(&cfg, min_capacity, std::uint64_t(seed),
+                                             no_init ? 1 : 0, &handle_);
+        if (rc == WC_OK) refresh();
     }
 
     __host__ __device__ SingleValueHashTable(const SingleValueHashTable &o) noexcept
@@ -278,7 +284,11 @@ __global__ void svht_for_each_kernel(F f, const Table table)
     const b200::TableView &t = table.device_view();
     unsigned char *const sp = reinterpret_cast<unsigned char *>(t.slots) + tid * L::kSlotBytes;
     const K key = *reinterpret_cast<const K *>(sp);
-    if (Table::is_valid_key(key)) f(key, Table::value_of(*b200::slot_value_ptr<L>(sp)));
+    if (!Table::is_valid_key(key)) return;
+    if constexpr (b200::is_soa<L>::value)
+        f(key, Table::value_of(b200::get_soa_value<L>(t, tid)));
+    else
+        f(key, Table::value_of(*b200::slot_value_ptr<L>(sp)));
 }
 } // namespace detail
 

@@ -118,6 +118,9 @@ typedef struct wc_table_info {
     unsigned long long *live;     /* device: the valid-key counters, 32 of them
                                      32 bytes apart (NULL for multi-value
                                      tables); writers of slot keys keep them */
+    void *values;                 /* struct-of-arrays single-value tables: the
+                                     value array, one value per key slot of
+                                     `slots`; NULL for every other table */
 } wc_table_info;
 
 typedef struct wc_table wc_table;
@@ -151,6 +154,18 @@ uint64_t wc_valid_capacity(uint64_t min_capacity, uint64_t cg_size);
  * (single_value_hash_table.cuh:112-128) */
 int wc_svht_create(const wc_table_config *cfg, uint64_t min_capacity,
                    uint64_t seed, int no_init, wc_table **out);
+/* SingleValueHashTable<Key, Value, ..., storage::key_value::SoAStore<Key,
+ * Value>> (storage.cuh:218-432): the same table stored as a struct of
+ * arrays.  The slot array (wc_table_info.slots) holds the keys only,
+ * capacity of them; the values sit in a separate array
+ * (wc_table_info.values), value i belonging to key slot i.  An insert
+ * claims the key slot with a compare-and-swap and then writes the value, as
+ * the reference's SoA store does; every operation, status and answer is the
+ * same as the AoS table's.  These tables keep no fingerprints, run the
+ * window kernel only, and are not accepted by the batch, served and
+ * persistent-server calls (WC_ERR_UNSUPPORTED / WC_ERR_INVALID_ARGUMENT). */
+int wc_svht_create_soa(const wc_table_config *cfg, uint64_t min_capacity,
+                       uint64_t seed, int no_init, wc_table **out);
 /* ~SingleValueHashTable (single_value_hash_table.cuh:162-169); also destroys
  * hash sets and counting tables */
 int wc_table_destroy(wc_table *t);

@@ -222,6 +222,88 @@ static void test_svht_u64_device_api()
     cudaFree(da); cudaFree(dva); cudaFree(db); cudaFree(dvb); cudaFree(dst); cudaFree(dout);
 }
 
+/* SingleValueHashTable with SoAStore: keys and values in two arrays, the
+ * same answers through the bulk and the device API */
+template <class K, class V>
+static void test_svht_soa(unsigned seed)
+{
+    using Store = wc::storage::key_value::SoAStore<K, V>;
+    using Table = wc::SingleValueHashTable<K, V, wc::defaults::empty_key<K>(),
+                                           wc::defaults::tombstone_key<K>(),
+                                           wc::defaults::probing_scheme_t<K, 8>, Store>;
+    const uint64_t n = 40000;
+    auto keys = distinct_keys<K>(2 * n, seed);
+    std::vector<K> a(keys.begin(), keys.begin() + n), b(keys.begin() + n, keys.end());
+    std::vector<V> va(n), vb(n);
+    for (uint64_t i = 0; i < n; ++i) { va[i] = V(i + 7); vb[i] = V(~i); }
+    Table t(uint64_t(2 * n / 0.9));
+    K *da = dcopy(a), *db = dcopy(b);
+    V *dva = dcopy(va), *dvb = dcopy(vb);
+    wc::Status *dst;
+    cudaMalloc(&dst, sizeof(wc::Status) * n);
+    t.insert(da, dva, n);
+    device_insert<<<blocks_for(n, Table::cg_size()), 256>>>(t, db, dvb, n, dst);
+    auto st = hcopy(reinterpret_cast<uint32_t *>(dst), n);
+    CHECK(std::all_of(st.begin(), st.end(), [](uint32_t s) { return s == 0; }));
+    CHECK(t.size() == 2 * n);
+    V *dout;
+    cudaMalloc(&dout, sizeof(V) * n);
+    t.retrieve(db, n, dout);
+    CHECK(hcopy(dout, n) == vb);
+    device_retrieve<<<blocks_for(n, Table::cg_size()), 256>>>(t, da, n, dout, dst);
+    CHECK(hcopy(dout, n) == va);
+    /* duplicates overwrite the value array's element */
+    device_insert<<<blocks_for(n, Table::cg_size()), 256>>>(t, da, dvb, n, dst);
+    st = hcopy(reinterpret_cast<uint32_t *>(dst), n);
+    CHECK(std::all_of(st.begin(), st.end(), [](uint32_t s) { return s == wc::Status::duplicate_key().base(); }));
+    t.retrieve(da, n, dout);
+    CHECK(hcopy(dout, n) == vb);
+    /* the memory is a key array and a value array: key slot i holds a key,
+     * value i its value */
+    const auto &view = t.device_view();
+    CHECK(view.values != nullptr);
+    const auto hk = hcopy(reinterpret_cast<const K *>(view.slots), t.capacity());
+    const auto hv = hcopy(reinterpret_cast<const V *>(view.values), t.capacity());
+    std::unordered_map<K, V> expect;
+    for (uint64_t i = 0; i < n; ++i) { expect[a[i]] = vb[i]; expect[b[i]] = vb[i]; }
+    uint64_t seen = 0;
+    for (uint64_t i = 0; i < t.capacity(); ++i) {
+        if (!Table::is_valid_key(hk[i])) continue;
+        ++seen;
+        CHECK(expect.count(hk[i]) == 1 && expect[hk[i]] == hv[i]);
+    }
+    CHECK(seen == 2 * n);
+    /* for_each and retrieve_all read the value array */
+    unsigned long long *dc;
+    cudaMalloc(&dc, 16);
+    cudaMemset(dc, 0, 16);
+    t.for_each([=] __device__(K k, V v) {
+        atomicAdd(dc, 1ull);
+        atomicAdd(dc + 1, (unsigned long long)v);
+    });
+    const auto c = hcopy(dc, 2);
+    unsigned long long vsum = 0;
+    for (uint64_t i = 0; i < n; ++i) vsum += 2ull * (unsigned long long)vb[i];
+    CHECK(c[0] == 2 * n && c[1] == vsum);
+    K *ak;
+    V *av;
+    cudaMalloc(&ak, sizeof(K) * t.capacity());
+    cudaMalloc(&av, sizeof(V) * t.capacity());
+    wc::index_t num = 0;
+    t.retrieve_all(ak, av, num);
+    CHECK(num == 2 * n);
+    const auto rk = hcopy(ak, num);
+    const auto rv = hcopy(av, num);
+    for (uint64_t i = 0; i < num; ++i) CHECK(expect.count(rk[i]) == 1 && expect[rk[i]] == rv[i]);
+    /* erase leaves tombstones in the key array */
+    t.erase(da, n);
+    CHECK(t.size() == n);
+    t.retrieve(db, n, dout);
+    CHECK(hcopy(dout, n) == vb);
+    cudaFree(da); cudaFree(db); cudaFree(dva); cudaFree(dvb); cudaFree(dst); cudaFree(dout);
+    cudaFree(dc); cudaFree(ak); cudaFree(av);
+}
+
 static void test_hash_set()
 {
     using Set = wc::HashSet<uint64_t>;
@@ -783,6 +865,9 @@ int main()
 {
     test_svht_u32();
     test_svht_u64_device_api();
+    test_svht_soa<uint64_t, uint64_t>(41);
+    test_svht_soa<uint32_t, uint32_t>(42);
+    test_svht_soa<uint32_t, uint64_t>(43);
     test_hash_set();
     test_counting();
     test_bloom();

@@ -22,14 +22,14 @@ ORACLE_PROBE = {wc.PROBING_DOUBLE: o.PROBE_DOUBLE, wc.PROBING_LINEAR: o.PROBE_LI
 
 def make_pair(kind, kb, n_cap, cg, probing=wc.PROBING_DOUBLE, h1=wc.HASH_MURMUR,
               h2=wc.HASH_MURMUR, seed=wc.DEFAULT_SEED, max_count=None, empty=0, tomb=None,
-              vb=None):
+              vb=None, store="aos"):
     if tomb is None:
         tomb = (1 << (8 * kb)) - 1
     vb = kb if vb is None else vb
     kw = dict(key_bytes=kb, cg_size=cg, probing=probing, hasher1=h1, hasher2=h2,
               empty_key=empty, tombstone_key=tomb)
     if kind == o.SVHT:
-        g = wc.SingleValueHashTable(n_cap, seed=seed, value_bytes=vb, **kw)
+        g = wc.SingleValueHashTable(n_cap, seed=seed, value_bytes=vb, store=store, **kw)
     elif kind == o.HASHSET:
         g = wc.HashSet(n_cap, seed=seed, **kw)
     else:
@@ -42,10 +42,10 @@ def make_pair(kind, kb, n_cap, cg, probing=wc.PROBING_DOUBLE, h1=wc.HASH_MURMUR,
 
 
 def svht_round_trip(kb, cg, probing=wc.PROBING_DOUBLE, h1=wc.HASH_MURMUR,
-                    h2=wc.HASH_MURMUR, n=20000, load=0.8, seed=7, vb=None):
+                    h2=wc.HASH_MURMUR, n=20000, load=0.8, seed=7, vb=None, store="aos"):
     vb = kb if vb is None else vb
     n_cap = int(n / load)
-    g, r = make_pair(o.SVHT, kb, n_cap, cg, probing, h1, h2, vb=vb)
+    g, r = make_pair(o.SVHT, kb, n_cap, cg, probing, h1, h2, vb=vb, store=store)
     allk = o.gen_unique_keys(kb, 2 * n, seed)
     keys, absent = allk[:n], allk[n:]
     vals = o.gen_uniform(vb, n, seed + 1)

@@ -143,6 +143,7 @@ class TableInfo(ctypes.Structure):
         ("num_keys", ctypes.c_void_p),
         ("max_values_per_key", ctypes.c_uint64),
         ("live", ctypes.c_void_p),
+        ("values", ctypes.c_void_p),
     ]
 
 
@@ -269,6 +270,7 @@ SIGNATURES = {
     "wc_counting_default_config": (None, [ctypes.POINTER(TableConfig), _u32, _u32]),
     "wc_valid_capacity": (_u64, [_u64, _u64]),
     "wc_svht_create": (_i, [ctypes.POINTER(TableConfig), _u64, _u64, _i, _pp]),
+    "wc_svht_create_soa": (_i, [ctypes.POINTER(TableConfig), _u64, _u64, _i, _pp]),
     "wc_table_destroy": (_i, [_vp]),
     "wc_table_init": (_i, [_vp, _u64, _vp]),
     "wc_svht_insert": (_i, [_vp, _vp, _vp, _u64, _vp, _u64, _vp, _i, _u32]),
@@ -694,15 +696,24 @@ def _table_config(default_fn, key_bytes, value_bytes, empty_key, tombstone_key,
 
 
 class SingleValueHashTable(_Table):
-    """warpcore::SingleValueHashTable (single_value_hash_table.cuh:29-37)."""
+    """warpcore::SingleValueHashTable (single_value_hash_table.cuh:29-37).
+
+    store="aos" (default) keeps {key, value} slots; store="soa" keeps the
+    keys in the slot array and the values in a separate array
+    (storage::key_value::SoAStore, storage.cuh:218-432), with the same
+    answers (wc_svht_create_soa)."""
 
     def __init__(self, min_capacity, seed=DEFAULT_SEED, no_init=False, key_bytes=4,
                  value_bytes=None, empty_key=None, tombstone_key=None, probing=None,
-                 hasher1=None, hasher2=None, cg_size=None):
+                 hasher1=None, hasher2=None, cg_size=None, store="aos"):
+        if store not in ("aos", "soa"):
+            raise WarpcoreError("store must be 'aos' or 'soa'")
         value_bytes = key_bytes if value_bytes is None else value_bytes
         cfg = _table_config(lib().wc_svht_default_config, key_bytes, value_bytes, empty_key,
                             tombstone_key, probing, hasher1, hasher2, cg_size)
-        self._make(lib().wc_svht_create, cfg, int(min_capacity), int(seed), int(bool(no_init)))
+        create = lib().wc_svht_create_soa if store == "soa" else lib().wc_svht_create
+        self._make(create, cfg, int(min_capacity), int(seed), int(bool(no_init)))
+        self.store = store
 
     def insert(self, keys_in, values_in, num_in=None, stream=None,
                probing_length=DEFAULT_PROBING_LENGTH, status_out=None,

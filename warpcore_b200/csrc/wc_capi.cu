@@ -471,6 +471,10 @@ struct wc_table {
     unsigned long long *num_keys = nullptr; /* device: keys holding at least one value */
     void *scratch = nullptr;                /* device: scan tile sums, grown on demand */
     uint64_t scratch_bytes = 0;
+    /* single-value tables stored as a struct of arrays: slots holds the
+     * keys (probed as a hash set's slots), values one value per slot */
+    bool soa = false;
+    void *values = nullptr;
 };
 
 struct wc_bloom {
@@ -513,6 +517,7 @@ TableView view_of(const wc_table *t)
     v.hasher1 = t->cfg.hasher1;
     v.hasher2 = t->cfg.hasher2;
     v.cg_size = t->cfg.cg_size;
+    v.values = t->values;
     return v;
 }
 
@@ -581,7 +586,7 @@ TablePlacement placement(uint64_t cap, uint32_t slot_bytes, bool fingerprints)
 
 int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, uint64_t seed,
                  uint64_t max_count, int no_init, wc_table **out, void *memory = nullptr,
-                 uint64_t memory_bytes = 0, cudaStream_t stream = nullptr)
+                 uint64_t memory_bytes = 0, cudaStream_t stream = nullptr, bool soa = false)
 {
     if (!out) return fail(WC_ERR_INVALID_ARGUMENT, "out is NULL");
     *out = nullptr;
@@ -608,6 +613,12 @@ int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, ui
         t->layout = cfg->key_bytes == 4 ? kLayoutK32V64 : kLayoutK64V32;
         t->slot_bytes = 16;
     }
+    if (soa) {
+        /* the key array is a hash set's slot array */
+        t->soa = true;
+        t->layout = cfg->key_bytes == 4 ? kLayoutSet32 : kLayoutSet64;
+        t->slot_bytes = cfg->key_bytes;
+    }
     t->capacity = cap;
     t->num_buckets = cap / cfg->cg_size;
     t->seed = seed & key_mask(cfg->key_bytes);
@@ -616,7 +627,8 @@ int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, ui
     cudaGetDevice(&t->device);
 
     const uint64_t bytes = cap * t->slot_bytes;
-    const uint64_t fp_bytes = (kind != 3 && want_fingerprints(bytes)) ? cap : 0;
+    const uint64_t fp_bytes = (kind != 3 && !soa && want_fingerprints(bytes)) ? cap : 0;
+    const uint64_t value_bytes = soa ? cap * cfg->value_bytes : 0;
     if (memory) {
         /* caller-provided memory: carve the slots, the device block and the
          * fingerprints out of it; the table does not free it */
@@ -662,13 +674,14 @@ int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, ui
         delete t;
         return cuda_fail(cudaGetLastError(), "cudaMemGetInfo");
     }
-    if (bytes + fp_bytes + 4096 > free_b) {
+    if (bytes + fp_bytes + value_bytes + 4096 > free_b) {
         delete t;
         return fail(WC_ERR_OUT_OF_MEMORY, "table needs %llu bytes, %llu free",
-                    (unsigned long long)(bytes + fp_bytes), (unsigned long long)free_b);
+                    (unsigned long long)(bytes + fp_bytes + value_bytes), (unsigned long long)free_b);
     }
     cudaError_t e = cudaMalloc(&t->slots, bytes);
     if (e == cudaSuccess && fp_bytes) e = cudaMalloc(&t->fps, fp_bytes);
+    if (e == cudaSuccess && value_bytes) e = cudaMalloc(&t->values, value_bytes);
     if (e == cudaSuccess) {
         void *aux = nullptr;
         e = cudaMalloc(&aux, kAuxBytes);
@@ -682,6 +695,7 @@ int table_create(int kind, const wc_table_config *cfg, uint64_t min_capacity, ui
     if (e != cudaSuccess) {
         if (t->slots) cudaFree(t->slots);
         if (t->fps) cudaFree(t->fps);
+        if (t->values) cudaFree(t->values);
         delete t;
         return cuda_fail(e, "cudaMalloc");
     }
@@ -737,6 +751,7 @@ TableKernel pick_lane_kernel(const wc_table *t, int op)
 
 TableKernel pick_window_kernel(const wc_table *t, int op)
 {
+    if (t->soa) return table_kernel_soa(t->cfg.key_bytes, t->cfg.value_bytes, int(t->cfg.cg_size), op);
     if (TableKernel k = pick_lane_kernel(t, op)) return k;
     const int W = int(t->cfg.cg_size);
     switch (t->layout) {
@@ -950,6 +965,12 @@ int wc_svht_create_on(const wc_table_config *cfg, uint64_t min_capacity, uint64_
                         reinterpret_cast<cudaStream_t>(stream));
 }
 
+int wc_svht_create_soa(const wc_table_config *cfg, uint64_t min_capacity, uint64_t seed,
+                       int no_init, wc_table **out)
+{
+    return table_create(0, cfg, min_capacity, seed, 0, no_init, out, nullptr, 0, nullptr, true);
+}
+
 int wc_hashset_create(const wc_table_config *cfg, uint64_t min_capacity, uint64_t seed,
                       wc_table **out)
 {
@@ -971,6 +992,7 @@ int wc_table_destroy(wc_table *t)
     }
     if (t->slots) cudaFree(t->slots);
     if (t->fps) cudaFree(t->fps);
+    if (t->values) cudaFree(t->values);
     if (t->status) cudaFree(t->status);
     if (t->scratch) cudaFree(t->scratch);
     l2_window_release(t->l2);
@@ -988,6 +1010,7 @@ int wc_table_init(wc_table *t, uint64_t seed, wc_stream_t stream)
     int rc = fill_slots(t, s);
     if (rc) return rc;
     if (t->fps) WC_CUDA(cudaMemsetAsync(t->fps, kFpEmpty, t->capacity, s));
+    if (t->values) WC_CUDA(cudaMemsetAsync(t->values, 0, t->capacity * t->cfg.value_bytes, s));
     WC_CUDA(cudaMemsetAsync(t->status, 0, sizeof(uint32_t), s));
     WC_CUDA(cudaMemsetAsync(t->live, 0, kLiveBytes, s));
     if (t->kind == 3) WC_CUDA(cudaMemsetAsync(t->num_keys, 0, sizeof(unsigned long long), s));
@@ -1133,11 +1156,18 @@ int wc_table_retrieve_all(wc_table *t, void *keys_out, void *values_out, uint64_
     int rc = check_table(t, 0xF); /* every table kind: all (key, value) pairs */
     if (rc) return rc;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    DumpKernel k = dump_kernel_ptr(t->layout);
     WC_CUDA(cudaMemsetAsync(t->counter, 0, sizeof(unsigned long long), s));
-    const unsigned grid = grid_for(reinterpret_cast<const void *>(k), kBlock, t->capacity, kBlock);
-    k<<<grid, kBlock, 0, s>>>(t->slots, t->capacity, t->cfg.empty_key, t->cfg.tombstone_key,
-                              keys_out, t->kind == 1 ? nullptr : values_out, t->counter);
+    if (t->soa) {
+        const SoaDumpKernel k = soa_dump_kernel_ptr(t->cfg.key_bytes, t->cfg.value_bytes);
+        const unsigned grid = grid_for(reinterpret_cast<const void *>(k), kBlock, t->capacity, kBlock);
+        k<<<grid, kBlock, 0, s>>>(t->slots, t->values, t->capacity, t->cfg.empty_key,
+                                  t->cfg.tombstone_key, keys_out, values_out, t->counter);
+    } else {
+        DumpKernel k = dump_kernel_ptr(t->layout);
+        const unsigned grid = grid_for(reinterpret_cast<const void *>(k), kBlock, t->capacity, kBlock);
+        k<<<grid, kBlock, 0, s>>>(t->slots, t->capacity, t->cfg.empty_key, t->cfg.tombstone_key,
+                                  keys_out, t->kind == 1 ? nullptr : values_out, t->counter);
+    }
     note_launches(1);
     WC_CUDA(cudaGetLastError());
     unsigned long long h = 0;
@@ -1185,7 +1215,8 @@ int wc_table_get_info(const wc_table *t, wc_table_info *info)
     info->empty_key = t->cfg.empty_key;
     info->tombstone_key = t->cfg.tombstone_key;
     info->max_count = t->max_count;
-    info->bytes_total = t->capacity * t->slot_bytes + kAuxBytes + (t->fps ? t->capacity : 0);
+    info->bytes_total = t->capacity * t->slot_bytes + kAuxBytes + (t->fps ? t->capacity : 0) +
+                        (t->soa ? t->capacity * t->cfg.value_bytes : 0);
     info->slots = t->slots;
     info->status = t->status;
     info->is_initialized = t->initialized ? 1 : 0;
@@ -1193,6 +1224,7 @@ int wc_table_get_info(const wc_table *t, wc_table_info *info)
     info->num_keys = t->kind == 3 ? t->num_keys : nullptr;
     info->max_values_per_key = t->max_values;
     info->live = t->kind == 3 ? nullptr : t->live;
+    info->values = t->values;
     return WC_OK;
 }
 

@@ -46,6 +46,14 @@ TableKernel lane_kernel_set64(int W, int op);
 TableKernel lane_kernel_k32v64(int W, int op);
 TableKernel lane_kernel_k64v32(int W, int op);
 
+/* struct-of-arrays single-value tables (wc_tables_soa.cu): the window
+ * kernel of (key width, value width, W, op) for insert, retrieve and erase,
+ * nullptr otherwise; and the dump of (key array, value array) */
+TableKernel table_kernel_soa(uint32_t key_bytes, uint32_t value_bytes, int W, int op);
+using SoaDumpKernel = void (*)(const void *, const void *, uint64_t, uint64_t, uint64_t, void *,
+                               void *, unsigned long long *);
+SoaDumpKernel soa_dump_kernel_ptr(uint32_t key_bytes, uint32_t value_bytes);
+
 CountKernel count_kernel(int layout);
 using RebuildKernel = void (*)(const void *, uint64_t, uint64_t, uint64_t, unsigned char *);
 RebuildKernel fp_rebuild_kernel_ptr(int layout);

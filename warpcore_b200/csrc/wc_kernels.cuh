@@ -144,7 +144,8 @@ __device__ __forceinline__ void group_range(const TableOpArgs &a, const uint64_t
     constexpr int SPL = LB / SB;          /* slots per lane */
     constexpr int G = 32 / TPK;           /* windows per warp per round */
     constexpr uint32_t kGroupMask = TPK == 32 ? kFull : ((1u << TPK) - 1u);
-    constexpr bool kValueIn = OP == kOpInsert && L::kHasValue;
+    constexpr bool kSoA = is_soa<L>::value;
+    constexpr bool kValueIn = OP == kOpInsert && (L::kHasValue || kSoA);
     constexpr int kCache = OP == kOpCount ? 1024 : 1;
     static_assert(TPK * LB == WB && SPL * SB == LB, "window split");
 
@@ -369,10 +370,13 @@ __device__ __forceinline__ void group_range(const TableOpArgs &a, const uint64_t
                     if constexpr (OP == kOpRetrieve) {
                         st = kStNone;
                         flag = true;
+                        if constexpr (kSoA)
+                            st_stream(reinterpret_cast<V *>(a.out) + i,
+                                      get_soa_value<L>(t, bucket * W + uint64_t(fh)));
                     } else if constexpr (OP == kOpInsert) {
                         st = kStDuplicateKey;
                         join |= kStDuplicateKey;
-                        store_value<L>(sp, val);
+                        put_value<L>(t, sp, bucket * W + uint64_t(fh), val);
                     } else if constexpr (OP == kOpCount) {
                         st = kStDuplicateKey;
                         join |= kStDuplicateKey;
@@ -414,13 +418,14 @@ __device__ __forceinline__ void group_range(const TableOpArgs &a, const uint64_t
                     unsigned char *const sp = slots + (bucket * W + uint64_t(s)) * SB;
                     if (cas_old == empty && cas_old_payload == claim_expect) {
                         fp_store(t, bucket * W + uint64_t(s), fingerprint(key));
+                        if constexpr (kSoA) put_value<L>(t, sp, bucket * W + uint64_t(s), val);
                         ++live_delta;
                         st = kStNone;
                         pending = false;
                     } else if (cas_old == key) {
                         st = kStDuplicateKey;
                         join |= kStDuplicateKey;
-                        if constexpr (OP == kOpInsert) store_value<L>(sp, val);
+                        if constexpr (OP == kOpInsert) put_value<L>(t, sp, bucket * W + uint64_t(s), val);
                         else count_add<L>(sp, cnt_add, t.max_count, st, join);
                         pending = false;
                     } else if (cas_old == empty) {
