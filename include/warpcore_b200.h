@@ -876,8 +876,9 @@ int wc_partition_restore(const void *values, const uint32_t *status, const uint6
  * (key_bytes 4 or 8; value_bytes 0 for a hash set, else equal to key_bytes)
  * and writes the count to *size_out, a DEVICE pointer to one uint64, on
  * `stream`, without allocating any device memory.  A key-only array (a hash
- * set's slots, or the separate key array of a multi-bucket or bucket-list
- * table, whose wc_table_info reports value_bytes equal to key_bytes) must be
+ * set's slots, the key array of a struct-of-arrays single-value table, or
+ * the separate key array of a multi-bucket or bucket-list table, whose
+ * wc_table_info reports value_bytes equal to key_bytes) must be
  * passed with value_bytes 0: the 8- or 16-byte key+value layout would count
  * it wrongly.  It is meant for callers
  * that hold a table's slots without a handle of this library and may not

@@ -134,3 +134,21 @@ def test_multi_bucket_key_array_counted_as_keys_only():
     got = noalloc_count(inf.keys, inf.capacity, inf.key_bytes, 0, inf.empty_key,
                         inf.tombstone_key)
     assert got == t.num_keys() == n
+
+
+def test_soa_key_array_counted_as_keys_only():
+    # a struct-of-arrays single-value table: its slot array holds keys only
+    # and is counted with value_bytes 0
+    import torch
+    n = 200000
+    t = wc.SingleValueHashTable(n, key_bytes=8, store="soa")
+    keys = o.gen_unique_keys(8, n, 97)
+    t.insert(dev(keys), dev(o.gen_uniform(8, n, 96)))
+    t.erase(dev(keys[::5]))
+    inf = t.info()
+    out = torch.full((1,), -1, dtype=torch.int64, device="cuda")
+    rc = wc.lib().wc_slots_size_noalloc(inf.slots, inf.capacity, inf.key_bytes, 0,
+                                        inf.empty_key, inf.tombstone_key,
+                                        torch.cuda.current_stream().cuda_stream, out.data_ptr())
+    assert rc == 0, wc.lib().wc_last_error()
+    assert int(out.item()) == t.size() == n - keys[::5].size
