@@ -75,6 +75,35 @@ def measure_l2_copy_gbs(device, mib=32, reps=200):
     return 2 * (mib << 20) * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9
 
 
+def measure_random_atomic_gops(device, array_bytes, n, reps=3):
+    """Random 64-bit atomic adds per second (G/s) into an array of
+    `array_bytes`, n per launch with indices streamed from memory
+    (torch index_add_, one atomicAdd per element), median of `reps` CUDA-event
+    timings: an insert claims at least one random slot by an atomic, so this
+    rate bounds inserts into a table of that size whatever their bytes."""
+    import statistics as st
+    import torch
+    m = max(int(array_bytes) // 8, 1 << 20)
+    g = torch.Generator(device=device)
+    g.manual_seed(5)
+    buf = torch.zeros(m, dtype=torch.int64, device=device)
+    idx = torch.randint(0, m, (n,), device=device, generator=g)
+    ones = torch.ones(n, dtype=torch.int64, device=device)
+    buf.index_add_(0, idx, ones)
+    ms = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        buf.index_add_(0, idx, ones)
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    del buf, idx, ones
+    torch.cuda.empty_cache()
+    return n / (st.median(ms) * 1e-3) / 1e9
+
+
 def profile_traffic(name):
     """dram bytes per launch recorded by the ncu capture summarised under
     profiles/ (line 'dram_bytes_per_launch <kernel-tag> <bytes>')."""
@@ -709,6 +738,17 @@ def run_ours(args):
         if l2_resident:
             peak, peak_src = round(measure_l2_copy_gbs(device), 1), "measured L2-resident copy (2 x 32 MiB)"
         cpu = cpu_baseline(args) if not args.no_cpu else None
+        # inserts into a table in DRAM: the rate of random atomics into an
+        # array of the table's size bounds them too (one claim per key)
+        atomic = None
+        if dom == "insert" and table_bytes and not l2_resident:
+            rate = measure_random_atomic_gops(device, table_bytes, dom_ops)
+            ins_rate = dom_ops / (dom_ms * 1e-3) / 1e9
+            atomic = {"random_atomic_gops": round(rate, 3),
+                      "insert_gops": round(ins_rate, 3),
+                      "frac": round(ins_rate / rate, 4),
+                      "measured": "torch index_add_ of %d int64 ones at random indices into "
+                                  "%d bytes (one atomicAdd each), median of 3" % (dom_ops, table_bytes)}
         line = {
             "metric": "insert+retrieve Gops/s (keys processed per second, whole job)",
             "value": round(value, 4),
@@ -759,6 +799,7 @@ def run_ours(args):
                 "traffic": traffic,
                 "frac_of_hbm": round(achieved / hbm_peak, 4),
                 "table_bytes": table_bytes or None,
+                "atomic_ceiling": atomic,
             },
             "cpu_baseline": cpu,
             "reference_gpu_build": ref_gpu,
