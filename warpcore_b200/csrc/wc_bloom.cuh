@@ -279,15 +279,20 @@ __global__ void __launch_bounds__(256) bloom_lane_kernel(const BloomArgs a)
  * in shared memory (ballot + prefix count, input order kept).  The lanes
  * then take the list densely, kRegionU entries per lane at a time, issue
  * all their block reads before testing any, and write flags / OR words as
- * the one-key-per-lane kernel does.  Each key is served by exactly one
+ * the one-key-per-lane kernel does.  One entry per lane with four resident
+ * blocks per SM (64-byte blocks; two for 128-byte blocks, whose words take
+ * twice the registers) keeps more warps issuing than four entries per lane
+ * with two blocks: on the 2^32-bit filter of 64-byte blocks, 2^28 keys,
+ * 20.3 / 27.2 G keys/s (insert / query) against 16.9 / 21.3; two entries
+ * with three blocks 19.7 / 25.5.  Each key is served by exactly one
  * pass; a query's flag is written there (a key of another shard's block
  * gets 0 in the first pass). */
 constexpr int kRegionKpl = 8;   /* keys per lane per warp tile */
-constexpr int kRegionU = 4;     /* compacted keys per lane in flight */
+constexpr int kRegionU = 1;     /* compacted keys per lane in flight */
 constexpr int kRegionWarps = 8; /* 256 threads */
 
 template <class K, class S, int CG, bool INSERT>
-__global__ void __launch_bounds__(256) bloom_region_kernel(const BloomArgs a)
+__global__ void __launch_bounds__(256, CG * sizeof(S) <= 64 ? 4 : 2) bloom_region_kernel(const BloomArgs a)
 {
     constexpr int SB = sizeof(S);
     constexpr int BB = CG * SB;
