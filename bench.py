@@ -741,7 +741,8 @@ def run_ours(args):
         # inserts into a table in DRAM: the rate of random atomics into an
         # array of the table's size bounds them too (one claim per key)
         atomic = None
-        if dom == "insert" and table_bytes and not l2_resident:
+        if (dom == "insert" and table_bytes and not l2_resident
+                and args.workload in ("svht32", "svht64", "hashset64")):
             rate = measure_random_atomic_gops(device, table_bytes, dom_ops)
             ins_rate = dom_ops / (dom_ms * 1e-3) / 1e9
             atomic = {"random_atomic_gops": round(rate, 3),

@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(256, (OP == kOpRetrieve || OP == kOpErase) ? W
     uint32_t st = kStNone, join = 0, cnt_add = 1;
     int live_delta = 0; /* claims minus erases of this lane */
 
-    constexpr int kCache = OP == kOpCount ? 1024 : 1;
+    constexpr int kCache = OP == kOpCount ? (1 << count_cache_bits<L>()) : 1;
     __shared__ K sc_key[kCache];
     __shared__ V sc_cnt[kCache];
     const bool use_cache = OP == kOpCount && a.handler == kHandlerNothing;
@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(256, (OP == kOpRetrieve || OP == kOpErase) ? W
             if (use_cache && refill && pending) {
                 using CW = typename std::conditional<sizeof(K) == 8, unsigned long long,
                                                      unsigned int>::type;
-                const uint32_t h = uint32_t((uint64_t(key) * 0x9E3779B97F4A7C15ull) >> 54);
+                const uint32_t h = uint32_t((uint64_t(key) * 0x9E3779B97F4A7C15ull) >> (64 - count_cache_bits<L>()));
 #pragma unroll
                 for (int p = 0; p < 4; ++p) {
                     const int c = int((h + p) & (kCache - 1));
