@@ -32,9 +32,16 @@
 namespace warpcore {
 namespace b200 {
 
-#ifndef WC_LANE_MIN_BLOCKS
-#define WC_LANE_MIN_BLOCKS 3
-#endif
+/* resident 256-thread blocks per SM the lane kernels are built for: 4 for
+ * u32 pairs with windows of at most 64 bytes (64 registers, no spills; the
+ * u32/u32 insert of 2^20 keys into 2 097 496 slots ran 21.2-21.4 against
+ * 20.2 G keys/s with 3, the retrieve unchanged, and 5 spilled and lost),
+ * 3 elsewhere, where 4 spills */
+template <class L, int W>
+constexpr int lane_min_blocks()
+{
+    return (L::kSlotBytes == 8 && L::kHasValue && W * L::kSlotBytes <= 64) ? 4 : 3;
+}
 
 /* a bucket's window of WB bytes, read by one lane from L2 (.cg: a claim by
  * another lane is seen): 32-byte vector loads for windows of 32 bytes or
@@ -108,7 +115,7 @@ __device__ __forceinline__ typename L::val_t window_val_at(const uint32_t *w, in
 }
 
 template <class L, int W, int OP>
-__global__ void __launch_bounds__(256, WC_LANE_MIN_BLOCKS) lane_op_kernel(const TableOpArgs a)
+__global__ void __launch_bounds__(256, lane_min_blocks<L, W>()) lane_op_kernel(const TableOpArgs a)
 {
     using K = typename L::key_t;
     using V = typename L::val_t;
