@@ -86,3 +86,59 @@ def test_soa_tables_are_not_batched():
         b.run([(g, "insert", keys, vals)])
     with pytest.raises(wc.WarpcoreError):
         wc.SingleValueHashTable(1000, store="columnar")
+
+
+def test_soa_custom_sentinels():
+    # the empty and tombstone keys of the key array are the table's own
+    kb, n = 4, 5000
+    g, r = make_pair(o.SVHT, kb, 8000, 8, empty=7, tomb=9, store="soa")
+    keys = o.gen_unique_keys(kb, n, 3)
+    keys = keys[(keys != 7) & (keys != 9)]
+    keys = np.concatenate([keys, np.array([0, 0xFFFFFFFF, 7, 9], dtype=np.uint32)])
+    vals = o.gen_uniform(kb, keys.size, 4)
+    st = empty_dev(keys.size, 4)
+    g.insert(dev(keys), dev(vals), status_out=st)
+    assert np.array_equal(host(st), r.insert(keys, vals, want_status=True))
+    out = empty_dev(keys.size, kb, 0xA5A5A5A5)
+    g.retrieve(dev(keys), out)
+    r_out = r.retrieve(keys, np.full(keys.size, 0xA5A5A5A5, dtype=np.uint32))
+    assert np.array_equal(host(out), r_out)
+    assert g.peek_status() == r.peek_status()
+    assert g.size() == g.size_scan() == r.size()
+
+
+def test_soa_full_table_reports_probing_length_exceeded():
+    # every key slot taken: further inserts and misses end after every bucket
+    g = wc.SingleValueHashTable(1, key_bytes=4, cg_size=32, probing=wc.PROBING_LINEAR,
+                                store="soa")
+    cap = g.capacity
+    keys = o.gen_unique_keys(4, cap + 64, 12)
+    vals = o.gen_uniform(4, keys.size, 13)
+    st = empty_dev(cap, 4)
+    g.insert(dev(keys[:cap]), dev(vals[:cap]), status_out=st)
+    assert (host(st) == 0).all()
+    assert g.size() == cap
+    st2 = empty_dev(64, 4)
+    g.insert(dev(keys[cap:]), dev(vals[cap:]), status_out=st2)
+    assert (host(st2) == wc.Status.probing_length_exceeded().base()).all()
+    out = empty_dev(cap, 4)
+    g.retrieve(dev(keys[:cap]), out)
+    assert np.array_equal(host(out), vals[:cap])
+    assert g.pop_status().has_probing_length_exceeded()
+
+
+def test_soa_boolean_handler_matches_oracle():
+    n = 4000
+    g, r = make_pair(o.SVHT, 4, 8000, 8, store="soa")
+    keys = o.gen_unique_keys(4, 2 * n, 5)
+    vals = o.gen_uniform(4, n, 6)
+    g.insert(dev(keys[:n]), dev(vals))
+    r.insert(keys[:n], vals)
+    q = np.concatenate([keys, np.array([0, 0xFFFFFFFF], dtype=np.uint32)])
+    for ignore in (0, wc.Status.key_not_found().base()):
+        b = empty_dev(q.size, 1, 9)
+        out = empty_dev(q.size, 4)
+        g.retrieve(dev(q), out, status_out=b, status_handler=wc.HANDLER_BOOLEAN, ignore=ignore)
+        _, r_st = r.retrieve(q, want_status=True)
+        exp = np.array([o.status_to_bool(int(s), ignore) for s in r_st], dtype=np.uint8)
+        assert np.array_equal(host(b), exp)
