@@ -774,7 +774,8 @@ def run_ours(args):
                 "capacity": int(wl.table.capacity) if hasattr(wl.table, "capacity") else None,
                 "keys_inserted": wl.n,
                 "real_load": (round(wl.n / wl.table.capacity, 4)
-                              if args.workload in ("svht32", "svht64", "hashset64") else None),
+                              if args.workload in ("svht32", "svht64", "hashset64")
+                              and hasattr(wl.table, "capacity") else None),
                 "filled": bool(args.fill),
                 "ops_per_step": ops_step,
                 "l2": "inputs larger than L2 (no flush)" if args.log2n >= 24 else "inputs may be L2-resident",
