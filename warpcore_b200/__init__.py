@@ -1241,8 +1241,8 @@ class BloomFilter:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib().wc_bloom_destroy(h)
+        if h is not None and h.value and _lib is not None:
+            _lib.wc_bloom_destroy(h)
             self._h = None
 
     def info(self):
@@ -1312,8 +1312,8 @@ class HostPipe:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib().wc_host_pipe_destroy(h)
+        if h is not None and h.value and _lib is not None:
+            _lib.wc_host_pipe_destroy(h)
             self._h = None
 
 
@@ -1329,8 +1329,8 @@ class Batch:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib().wc_batch_destroy(h)
+        if h is not None and h.value and _lib is not None:
+            _lib.wc_batch_destroy(h)
             self._h = None
 
     def run(self, requests, stream=None, probing_length=DEFAULT_PROBING_LENGTH, blocks_per_sm=0):
