@@ -737,7 +737,8 @@ def run_ours(args):
         hbm_peak = peak
         if l2_resident:
             peak, peak_src = round(measure_l2_copy_gbs(device), 1), "measured L2-resident copy (2 x 32 MiB)"
-        cpu = cpu_baseline(args) if not args.no_cpu else None
+        # the host baseline is timed on rank 0 of a one-GPU run only
+        cpu = cpu_baseline(args) if not args.no_cpu and world == 1 else None
         # inserts into a table in DRAM: the rate of random atomics into an
         # array of the table's size bounds them too (one claim per key)
         atomic = None
