@@ -97,6 +97,58 @@ __device__ __forceinline__ void block_masks(K key, K seed, uint32_t hasher, uint
     }
 }
 
+/* word i of a block held in registers, by a select tree (no dynamic
+ * register indexing) */
+template <class S, int CG>
+__device__ __forceinline__ S pick_word(const S (&w)[CG], int i)
+{
+    if constexpr (CG == 1) {
+        return w[0];
+    } else if constexpr (CG == 2) {
+        return (i & 1) ? w[1] : w[0];
+    } else if constexpr (CG == 4) {
+        const S a = (i & 1) ? w[1] : w[0], b = (i & 1) ? w[3] : w[2];
+        return (i & 2) ? b : a;
+    } else if constexpr (CG == 8) {
+        const S a = (i & 1) ? w[1] : w[0], b = (i & 1) ? w[3] : w[2];
+        const S c = (i & 1) ? w[5] : w[4], d = (i & 1) ? w[7] : w[6];
+        const S e = (i & 2) ? b : a, f = (i & 2) ? d : c;
+        return (i & 4) ? f : e;
+    } else {
+        S v = 0;
+#pragma unroll
+        for (int s = 0; s < CG; ++s)
+            if (s == i) v = w[s];
+        return v;
+    }
+}
+
+/* Whether every one of the key's k bits is set in the block w, each bit
+ * tested in the word it falls in (the query needs no masks).  Against
+ * building the k masks (a compare and select per word and bit) and testing
+ * them, 36.4 against 27.9 G queries/s on the 2^32-bit filter of 64-byte
+ * blocks. */
+template <class K, class S, int CG>
+__device__ __forceinline__ bool block_has_all(K key, K seed, uint32_t hasher, uint64_t k,
+                                              const S (&w)[CG])
+{
+    constexpr uint64_t kSlotBits = sizeof(S) * 8;
+    constexpr uint64_t kBlockBits = kSlotBits * CG;
+    bool ok = true;
+    if (hasher == kHashMurmur) {
+        for (uint64_t j = 0; j < k; ++j) {
+            const uint64_t h = hash_key<K>(kHashMurmur, K(key + seed + K(j))) & (kBlockBits - 1);
+            ok &= ((pick_word<S, CG>(w, int(h / kSlotBits)) >> (h % kSlotBits)) & S(1)) != 0;
+        }
+        return ok;
+    }
+    for (uint64_t j = 0; j < k; ++j) {
+        const uint64_t h = hash_key<K>(hasher, K(key + seed + K(j))) & (kBlockBits - 1);
+        ok &= ((pick_word<S, CG>(w, int(h / kSlotBits)) >> (h % kSlotBits)) & S(1)) != 0;
+    }
+    return ok;
+}
+
 template <class K, class S, int CG, bool INSERT>
 __global__ void __launch_bounds__(256) bloom_kernel(const BloomArgs a)
 {
@@ -240,8 +292,6 @@ __global__ void __launch_bounds__(256) bloom_lane_kernel(const BloomArgs a)
             continue;
         }
         if (blk < a.region_lo || blk >= a.region_hi) continue;
-        S m[CG];
-        block_masks<K, S, CG>(key, seed, a.hasher, a.k, m);
         const uint64_t w0 = blk * CG;
         S w[CG];
         constexpr bool kRead = !INSERT || WC_BLOOM_INSERT_READS_BLOCK;
@@ -262,18 +312,21 @@ __global__ void __launch_bounds__(256) bloom_lane_kernel(const BloomArgs a)
 #pragma unroll
             for (int s = 0; s < CG; ++s) w[s] = 0;
         }
-        bool ok = true;
+        if constexpr (!INSERT) {
+            a.flags_out[i] = (unsigned char)block_has_all<K, S, CG>(key, seed, a.hasher, a.k, w);
+        } else {
+            S m[CG];
+            block_masks<K, S, CG>(key, seed, a.hasher, a.k, m);
 #pragma unroll
-        for (int s = 0; s < CG; ++s) {
-            const bool missing = (w[s] & m[s]) != m[s];
-            ok &= !missing;
-            if (INSERT && m[s] && (!kRead || missing)) {
-                uint64_t wi = w0 + uint64_t(s);
-                if (wi >= a.num_slots) wi -= a.num_slots;
-                atomic_or_any(words + wi, m[s]);
+            for (int s = 0; s < CG; ++s) {
+                const bool missing = (w[s] & m[s]) != m[s];
+                if (m[s] && (!kRead || missing)) {
+                    uint64_t wi = w0 + uint64_t(s);
+                    if (wi >= a.num_slots) wi -= a.num_slots;
+                    atomic_or_any(words + wi, m[s]);
+                }
             }
         }
-        if constexpr (!INSERT) a.flags_out[i] = (unsigned char)ok;
     }
 }
 
@@ -389,20 +442,22 @@ __global__ void __launch_bounds__(256, CG * sizeof(S) <= 64 ? 4 : 2) bloom_regio
                 if (e >= cnt) continue;
                 const K key = s_key[wib][e];
                 const uint64_t w0 = (a.region_lo + s_rel[wib][e]) * CG;
-                S m[CG];
-                block_masks<K, S, CG>(key, seed, a.hasher, a.k, m);
-                bool ok = true;
+                if constexpr (!INSERT) {
+                    a.flags_out[base + s_off[wib][e]] =
+                        (unsigned char)block_has_all<K, S, CG>(key, seed, a.hasher, a.k, w[u]);
+                } else {
+                    S m[CG];
+                    block_masks<K, S, CG>(key, seed, a.hasher, a.k, m);
 #pragma unroll
-                for (int s = 0; s < CG; ++s) {
-                    const bool missing = (w[u][s] & m[s]) != m[s];
-                    ok &= !missing;
-                    if (INSERT && m[s] && (!kRead || missing)) {
-                        uint64_t wi = w0 + uint64_t(s);
-                        if (wi >= a.num_slots) wi -= a.num_slots;
-                        atomic_or_any(words + wi, m[s]);
+                    for (int s = 0; s < CG; ++s) {
+                        const bool missing = (w[u][s] & m[s]) != m[s];
+                        if (m[s] && (!kRead || missing)) {
+                            uint64_t wi = w0 + uint64_t(s);
+                            if (wi >= a.num_slots) wi -= a.num_slots;
+                            atomic_or_any(words + wi, m[s]);
+                        }
                     }
                 }
-                if constexpr (!INSERT) a.flags_out[base + s_off[wib][e]] = (unsigned char)ok;
             }
         }
         __syncwarp();
