@@ -739,18 +739,22 @@ def run_ours(args):
             peak, peak_src = round(measure_l2_copy_gbs(device), 1), "measured L2-resident copy (2 x 32 MiB)"
         # the host baseline is timed on rank 0 of a one-GPU run only
         cpu = cpu_baseline(args) if not args.no_cpu and world == 1 else None
-        # inserts into a table in DRAM: the rate of random atomics into an
-        # array of the table's size bounds them too (one claim per key)
+        # inserts: the rate of random atomics into an array of the table's
+        # size (in DRAM, or in L2 for a table that L2 holds) bounds them too
+        # (one claim per key); at least 2^24 atomics, so that the rate is the
+        # throughput and not the ramp of a short launch
         atomic = None
-        if (dom == "insert" and table_bytes and not l2_resident
+        if (dom == "insert" and table_bytes
                 and args.workload in ("svht32", "svht64", "hashset64")):
-            rate = measure_random_atomic_gops(device, table_bytes, dom_ops)
+            n_atomic = max(dom_ops, 1 << 24)
+            rate = measure_random_atomic_gops(device, table_bytes, n_atomic)
             ins_rate = dom_ops / (dom_ms * 1e-3) / 1e9
             atomic = {"random_atomic_gops": round(rate, 3),
                       "insert_gops": round(ins_rate, 3),
                       "frac": round(ins_rate / rate, 4),
                       "measured": "torch index_add_ of %d int64 ones at random indices into "
-                                  "%d bytes (one atomicAdd each), median of 3" % (dom_ops, table_bytes)}
+                                  "%d bytes%s (one atomicAdd each), median of 3"
+                                  % (n_atomic, table_bytes, " (L2-resident)" if l2_resident else "")}
         line = {
             "metric": "insert+retrieve Gops/s (keys processed per second, whole job)",
             "value": round(value, 4),
