@@ -13,8 +13,10 @@
  *     pair table) mostly stays in L2;
  *   - a hit costs the fingerprint words plus one slot, read with an
  *     evict-first hint so that slot lines do not push fingerprints out
- *     (retrieve, erase), or from L2 without an L1 copy (inserts: a claim's
- *     compare-and-swap lands in L2, and an equal key's lane must see it).
+ *     (retrieve), or from L2 without an L1 copy (inserts: a claim's
+ *     compare-and-swap lands in L2, and an equal key's lane must see it;
+ *     erase: its compare-and-swap on the slot follows, with the words read
+ *     as the expected value).
  *
  * Each lane owns one key and issues one memory operation per wave: a
  * fingerprint load, a candidate slot load, or a compare-and-swap claim.
@@ -43,8 +45,8 @@ namespace b200 {
 #endif
 
 /* L2 eviction priorities: fingerprint lines are loaded and stored with
- * evict_last and slot lines read by retrieve and erase with evict_first
- * (ld.cs), so that the
+ * evict_last and slot lines read by retrieve with evict_first (ld.cs),
+ * so that the
  * random slot traffic of a table larger than L2 evicts slot lines before
  * fingerprint lines (a fingerprint byte written into an evicted sector
  * costs a DRAM read to merge). */
@@ -171,6 +173,43 @@ __device__ __forceinline__ LaneWords load_slot_once(const unsigned char *sp)
         r.w[0] = __ldcs(reinterpret_cast<const unsigned int *>(sp));
     }
     return r;
+}
+
+/* erase of a slot whose words this lane has just read from L2: the words
+ * read are the compare-and-swap's first expected value, so no second read
+ * precedes it */
+template <class L>
+__device__ __forceinline__ bool erase_slot_seen(void *sp, typename L::key_t key,
+                                                typename L::key_t tomb, const LaneWords &sw)
+{
+    if constexpr (L::kSlotBytes == 16) {
+        uint64_t lo = uint64_t(sw.w[0]) | (uint64_t(sw.w[1]) << 32);
+        uint64_t hi = uint64_t(sw.w[2]) | (uint64_t(sw.w[3]) << 32);
+        for (int tries = 0; tries < 1024; ++tries) {
+            if (lo != uint64_t(key)) return false;
+            uint64_t olo, ohi;
+            cas128(sp, lo, hi, uint64_t(tomb), hi, olo, ohi);
+            if (olo == lo && ohi == hi) return true;
+            lo = olo;
+            hi = ohi;
+        }
+        store_key<L>(sp, tomb);
+        return true;
+    } else if constexpr (L::kSlotBytes == 8 && L::kHasValue) {
+        unsigned long long *p = reinterpret_cast<unsigned long long *>(sp);
+        unsigned long long cur = uint64_t(sw.w[0]) | (uint64_t(sw.w[1]) << 32);
+        for (int tries = 0; tries < 1024; ++tries) {
+            if (uint32_t(cur) != uint32_t(key)) return false;
+            const unsigned long long old =
+                atomicCAS(p, cur, (cur & 0xffffffff00000000ull) | uint32_t(tomb));
+            if (old == cur) return true;
+            cur = old;
+        }
+        store_key<L>(sp, tomb);
+        return true;
+    } else {
+        return erase_slot<L>(sp, key, tomb);
+    }
 }
 
 template <class L, int W, int OP>
@@ -347,9 +386,13 @@ __global__ void __launch_bounds__(256, (OP == kOpRetrieve || OP == kOpErase) ? W
                 unsigned char *const sp = slots + (base_slot + uint64_t(s)) * SB;
                 /* inserts read the slot where the claims' atomics land (L2):
                  * an L1 copy may predate the claim of an equal key by
-                 * another lane, which would then be inserted twice */
-                const LaneWords sw = (OP == kOpInsert || OP == kOpCount) ? load_lane<SB>(sp)
-                                                                         : load_slot_once<L>(sp);
+                 * another lane, which would then be inserted twice.  Erase
+                 * reads it the same way, since its compare-and-swap follows
+                 * on the same line: with the evict-first read and a second
+                 * read before the compare-and-swap, erasing 2^27 keys of a
+                 * 2.4 GB table ran at 7.0 G keys/s, against 9.2 now */
+                const LaneWords sw = (OP != kOpRetrieve) ? load_lane<SB>(sp)
+                                                         : load_slot_once<L>(sp);
                 const K sk = slot_key<L>(sw, 0);
                 if (sk == key) {
                     if constexpr (OP == kOpRetrieve) {
@@ -371,7 +414,7 @@ __global__ void __launch_bounds__(256, (OP == kOpRetrieve || OP == kOpErase) ? W
                         join |= kStDuplicateKey;
                         count_add<L>(sp, cnt_add, t.max_count, st, join);
                     } else {
-                        if (erase_slot<L>(sp, key, tomb)) {
+                        if (erase_slot_seen<L>(sp, key, tomb, sw)) {
                             fp_store(t, base_slot + uint64_t(s), kFpTomb);
                             --live_delta;
                         }
