@@ -514,11 +514,14 @@ __device__ __forceinline__ void live_add(const TableView &t, long long d)
 
 /* Turn the slot holding `key` into a tombstone with a compare-and-swap of
  * the whole slot (the width of the claims' compare-and-swap), keeping its
- * payload.  Returns true if this call erased the key; false if the slot no
- * longer holds it (an equal key erased by another thread). */
+ * payload.  `seen` is the slot as this thread last read it from L2: the
+ * first expected value of the compare-and-swap of a slot with a payload (a
+ * key-only slot needs none).  Returns true if this call erased the key;
+ * false if the slot no longer holds it (an equal key erased by another
+ * thread). */
 template <class L>
-__device__ __forceinline__ bool erase_slot(void *sp, typename L::key_t key,
-                                           typename L::key_t tomb)
+__device__ __forceinline__ bool erase_slot_seen(void *sp, typename L::key_t key,
+                                                typename L::key_t tomb, const LaneWords &seen)
 {
     if constexpr (L::kSlotBytes == 4) {
         return atomicCAS(reinterpret_cast<unsigned int *>(sp), key, tomb) == key;
@@ -527,7 +530,7 @@ __device__ __forceinline__ bool erase_slot(void *sp, typename L::key_t key,
                          (unsigned long long)tomb) == (unsigned long long)key;
     } else if constexpr (L::kSlotBytes == 8) {
         unsigned long long *p = reinterpret_cast<unsigned long long *>(sp);
-        unsigned long long cur = __ldcg(p);
+        unsigned long long cur = uint64_t(seen.w[0]) | (uint64_t(seen.w[1]) << 32);
         /* a retry only follows a concurrent value update of the same key */
         for (int tries = 0; tries < 1024; ++tries) {
             if (uint32_t(cur) != uint32_t(key)) return false;
@@ -539,9 +542,8 @@ __device__ __forceinline__ bool erase_slot(void *sp, typename L::key_t key,
         store_key<L>(sp, tomb);
         return true;
     } else {
-        const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(sp));
-        uint64_t lo = uint64_t(v.x) | (uint64_t(v.y) << 32);
-        uint64_t hi = uint64_t(v.z) | (uint64_t(v.w) << 32);
+        uint64_t lo = uint64_t(seen.w[0]) | (uint64_t(seen.w[1]) << 32);
+        uint64_t hi = uint64_t(seen.w[2]) | (uint64_t(seen.w[3]) << 32);
         for (int tries = 0; tries < 1024; ++tries) {
             if (lo != uint64_t(key)) return false;
             uint64_t olo, ohi;
@@ -553,6 +555,17 @@ __device__ __forceinline__ bool erase_slot(void *sp, typename L::key_t key,
         store_key<L>(sp, tomb);
         return true;
     }
+}
+
+/* the same, reading the slot first (from L2) where it has a payload */
+template <class L>
+__device__ __forceinline__ bool erase_slot(void *sp, typename L::key_t key,
+                                           typename L::key_t tomb)
+{
+    if constexpr (L::kSlotBytes == 4 || !L::kHasValue)
+        return erase_slot_seen<L>(sp, key, tomb, LaneWords{{0u, 0u, 0u, 0u}});
+    else
+        return erase_slot_seen<L>(sp, key, tomb, load_lane<L::kSlotBytes>(sp));
 }
 
 /* width-generic wrappers: uint64_t is unsigned long on LP64, while the CUDA

@@ -175,43 +175,6 @@ __device__ __forceinline__ LaneWords load_slot_once(const unsigned char *sp)
     return r;
 }
 
-/* erase of a slot whose words this lane has just read from L2: the words
- * read are the compare-and-swap's first expected value, so no second read
- * precedes it */
-template <class L>
-__device__ __forceinline__ bool erase_slot_seen(void *sp, typename L::key_t key,
-                                                typename L::key_t tomb, const LaneWords &sw)
-{
-    if constexpr (L::kSlotBytes == 16) {
-        uint64_t lo = uint64_t(sw.w[0]) | (uint64_t(sw.w[1]) << 32);
-        uint64_t hi = uint64_t(sw.w[2]) | (uint64_t(sw.w[3]) << 32);
-        for (int tries = 0; tries < 1024; ++tries) {
-            if (lo != uint64_t(key)) return false;
-            uint64_t olo, ohi;
-            cas128(sp, lo, hi, uint64_t(tomb), hi, olo, ohi);
-            if (olo == lo && ohi == hi) return true;
-            lo = olo;
-            hi = ohi;
-        }
-        store_key<L>(sp, tomb);
-        return true;
-    } else if constexpr (L::kSlotBytes == 8 && L::kHasValue) {
-        unsigned long long *p = reinterpret_cast<unsigned long long *>(sp);
-        unsigned long long cur = uint64_t(sw.w[0]) | (uint64_t(sw.w[1]) << 32);
-        for (int tries = 0; tries < 1024; ++tries) {
-            if (uint32_t(cur) != uint32_t(key)) return false;
-            const unsigned long long old =
-                atomicCAS(p, cur, (cur & 0xffffffff00000000ull) | uint32_t(tomb));
-            if (old == cur) return true;
-            cur = old;
-        }
-        store_key<L>(sp, tomb);
-        return true;
-    } else {
-        return erase_slot<L>(sp, key, tomb);
-    }
-}
-
 template <class L, int W, int OP>
 __global__ void __launch_bounds__(256, (OP == kOpRetrieve || OP == kOpErase) ? WC_FP_MIN_BLOCKS_READ
                                                                             : WC_FP_MIN_BLOCKS)
