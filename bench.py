@@ -830,19 +830,35 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def _wrapping_sum(x):
+    """sum of a key or value tensor as unsigned 64-bit words, modulo 2^64"""
+    import torch
+    if x.dtype == torch.int32:
+        x = x.to(torch.int64) & 0xFFFFFFFF
+    return int(x.sum().item()) & ((1 << 64) - 1)
+
+
 def table_wide_ops(wl, stream, reps=3):
-    """Erase throughput and size() on the workload's table after its insert
-    (single_value_hash_table.cuh:426-496, 535-592): erase every inserted key
-    (CUDA events on the launching stream, table re-filled untimed before
-    each repetition, best of `reps`), and the time of size() (the maintained
-    count) against size_scan() (a scan of the slot array) on the full table.
-    After the erase both sizes must be 0."""
+    """Table-wide operations on the workload's table after its insert
+    (single_value_hash_table.cuh:426-496, 535-592, 606-651): retrieve_all of
+    every stored pair and the erase of every inserted key (CUDA events on
+    the launching stream, table re-filled untimed before each repetition,
+    best of `reps`), and the time of size() (the maintained count) against
+    size_scan() (a scan of the slot array) on the full table.  The dump must
+    hold as many entries as the table and, for the single-value tables and
+    the set, the inserted keys and values (equal sums modulo 2^64; the
+    counting table: counts summing to the keys inserted).  After the erase
+    both sizes must be 0."""
     import torch
     if wl.kind not in ("svht32", "svht64", "hashset64", "counting32"):
         return None
     t = wl.table
     best, sizes_ok = None, True
-    size_ms, scan_ms = [], []
+    size_ms, scan_ms, dump_ms = [], [], []
+    dump_ok = True
+    kdt = torch.int64 if t.key_bytes == 8 else torch.int32
+    has_val = wl.kind != "hashset64"
+    vdt = wl.values.dtype if wl.values is not None else torch.int32
     for _ in range(reps):
         wl.init(stream)
         wl.insert(stream)
@@ -851,6 +867,24 @@ def table_wide_ops(wl, stream, reps=3):
             t0 = time.perf_counter()
             fn()
             acc.append((time.perf_counter() - t0) * 1e3)
+        live = int(t.size())
+        kout = torch.empty(live, dtype=kdt, device=wl.keys.device)
+        vout = torch.empty(live, dtype=vdt, device=wl.keys.device) if has_val else None
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        got = t.retrieve_all(kout, vout, stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        dump_ms.append(a.elapsed_time(b))
+        ok = got == live
+        if wl.kind == "counting32":
+            ok = ok and _wrapping_sum(vout) == wl.keys.numel()
+        else:
+            ok = ok and got == wl.keys.numel() and _wrapping_sum(kout) == _wrapping_sum(wl.keys)
+            if has_val:
+                ok = ok and _wrapping_sum(vout) == _wrapping_sum(wl.values)
+        dump_ok = dump_ok and ok
+        del kout, vout
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         t.erase(wl.keys, stream=stream)
@@ -859,7 +893,11 @@ def table_wide_ops(wl, stream, reps=3):
         ms = a.elapsed_time(b)
         best = ms if best is None else min(best, ms)
         sizes_ok = sizes_ok and t.size() == 0 and t.size_scan() == 0
-    return {"erase_gops": round(wl.keys.numel() / (best * 1e-3) / 1e9, 4),
+    return {"retrieve_all_ms": round(min(dump_ms), 4), "retrieved_all": int(got),
+            "retrieve_all_gops": round(got / (min(dump_ms) * 1e-3) / 1e9, 4),
+            "retrieve_all_verified": dump_ok,
+            "retrieve_all_timing": "CUDA events around the blocking call, best of %d" % reps,
+            "erase_gops": round(wl.keys.numel() / (best * 1e-3) / 1e9, 4),
             "erase_ms": round(best, 4), "erased_keys": int(wl.keys.numel()),
             "size_ms": round(min(size_ms), 4), "size_scan_ms": round(min(scan_ms), 4),
             "size_timing": "host wall clock of the blocking call, best of %d" % reps,

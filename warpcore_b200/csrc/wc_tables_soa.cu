@@ -36,7 +36,7 @@ TableKernel pick_soa_for(int W, int op)
 }
 
 /* every valid (key, value) of the key array and the value array, compacted
- * per warp as dump_kernel does */
+ * by block tiles as dump_kernel does (dump_tiles); both arrays are streamed */
 template <class K, class V>
 __global__ void __launch_bounds__(256) soa_dump_kernel(const void *keys, const void *values,
                                                        uint64_t capacity, uint64_t empty,
@@ -44,25 +44,14 @@ __global__ void __launch_bounds__(256) soa_dump_kernel(const void *keys, const v
                                                        void *values_out,
                                                        unsigned long long *count)
 {
-    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-    const int lane = threadIdx.x & 31;
-    const uint64_t start = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    const uint64_t rounds = (capacity + stride - 1) / stride;
-    for (uint64_t r = 0; r < rounds; ++r) {
-        const uint64_t s = start + r * stride;
-        K k = K(empty);
-        if (s < capacity) k = reinterpret_cast<const K *>(keys)[s];
-        const bool valid = s < capacity && k != K(empty) && k != K(tomb);
-        const unsigned m = __ballot_sync(kFull, valid);
-        unsigned long long base = 0;
-        if (lane == 0 && m) base = atomicAdd(count, (unsigned long long)__popc(m));
-        base = __shfl_sync(kFull, base, 0);
-        if (valid) {
-            const uint64_t o = base + __popc(m & ((1u << lane) - 1u));
-            reinterpret_cast<K *>(keys_out)[o] = k;
-            if (values_out) reinterpret_cast<V *>(values_out)[o] = reinterpret_cast<const V *>(values)[s];
-        }
-    }
+    const K *const kin = reinterpret_cast<const K *>(keys);
+    const V *const vin = reinterpret_cast<const V *>(values);
+    const bool want_values = values_out != nullptr;
+    dump_tiles<K, V>(capacity, K(empty), K(tomb), reinterpret_cast<K *>(keys_out),
+                     reinterpret_cast<V *>(values_out), count, [&](uint64_t s, K &k, V &v) {
+                         k = kin[s];
+                         if (want_values) v = vin[s];
+                     });
 }
 
 } // namespace
