@@ -838,6 +838,33 @@ def _wrapping_sum(x):
     return int(x.sum().item()) & ((1 << 64) - 1)
 
 
+def multi_value_keys_op(wl, stream, reps=3):
+    """retrieve_all_keys of a multi-value table after the timed steps
+    (multi_value_hash_table.cuh:561-598; bucket_list_hash_table.cuh and
+    multi_bucket_hash_table.cuh through gpu_engine.cuh:51-93): each stored
+    key once, CUDA events around the blocking call, best of `reps`.  The
+    keys must be the distinct inserted keys (count and sum modulo 2^64)."""
+    import torch
+    t = wl.table
+    nk = int(t.num_keys())
+    kout = torch.empty(nk, dtype=wl.keys.dtype, device=wl.keys.device)
+    expect = _wrapping_sum(torch.unique(wl.keys))
+    ms, ok = [], nk == wl.distinct
+    for _ in range(reps):
+        kout.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        got = t.retrieve_all_keys(kout, stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+        ok = ok and got == nk and _wrapping_sum(kout) == expect
+    return {"retrieve_all_keys_ms": round(min(ms), 4), "keys": nk,
+            "retrieve_all_keys_gkeys": round(nk / (min(ms) * 1e-3) / 1e9, 4),
+            "retrieve_all_keys_verified": ok,
+            "timing": "CUDA events around the blocking call, best of %d" % reps}
+
+
 def table_wide_ops(wl, stream, reps=3):
     """Table-wide operations on the workload's table after its insert
     (single_value_hash_table.cuh:426-496, 535-592, 606-651): retrieve_all of
@@ -850,6 +877,8 @@ def table_wide_ops(wl, stream, reps=3):
     counting table: counts summing to the keys inserted).  After the erase
     both sizes must be 0."""
     import torch
+    if wl.kind in ("mv32", "mb32", "bl32"):
+        return multi_value_keys_op(wl, stream, reps)
     if wl.kind not in ("svht32", "svht64", "hashset64", "counting32"):
         return None
     t = wl.table

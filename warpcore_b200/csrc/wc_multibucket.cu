@@ -12,6 +12,7 @@
 #include <warpcore_b200.h>
 
 #include "wc_internal.h"
+#include "wc_compact.cuh"
 #include <warpcore/detail/mb_ops.cuh>
 
 #include <cstdio>
@@ -149,7 +150,8 @@ __global__ void __launch_bounds__(256, WC_MULTI_MIN_BLOCKS) mb_find_kernel(const
 }
 
 /* retrieve_all_keys (gpu_engine.cuh:51-93): slot `gid` emits its key when
- * it is the lowest slot of the first window holding the key */
+ * it is the lowest slot of the first window holding the key; compacted by
+ * block tiles (wc_compact.cuh) */
 template <class K>
 __global__ void __launch_bounds__(256) mb_unique_keys_kernel(const MbView m, uint64_t capacity,
                                                              void *keys_out,
@@ -158,35 +160,21 @@ __global__ void __launch_bounds__(256) mb_unique_keys_kernel(const MbView m, uin
     const TableView &t = m.t;
     const K empty = K(t.empty_key), tomb = K(t.tombstone_key);
     const K *const keys = reinterpret_cast<const K *>(t.slots);
-    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-    const int lane = threadIdx.x & 31;
-    const uint64_t rounds = (capacity + stride - 1) / stride;
-    for (uint64_t r = 0; r < rounds; ++r) {
-        const uint64_t gid = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x + r * stride;
-        bool emit = false;
-        K key = empty;
-        if (gid < capacity) {
-            key = keys[gid];
-            if (key != empty && key != tomb) {
-                uint64_t b = probe_begin<K>(t, key), step = 0;
-                for (uint64_t w = 0; w < t.num_buckets; ++w) {
-                    uint32_t hits, emp;
-                    mb_window<K, 0>(keys + b * t.cg_size, t.cg_size, key, empty, hits, emp);
-                    if (hits) {
-                        emit = b * t.cg_size + uint64_t(__ffs(hits) - 1) == gid;
-                        break;
-                    }
-                    if (w == 0) step = probe_step<K>(t, key);
-                    b = probe_next(t, b, step);
-                }
-            }
-        }
-        const unsigned msk = __ballot_sync(0xffffffffu, emit);
-        unsigned long long base = 0;
-        if (lane == 0 && msk) base = atomicAdd(count, (unsigned long long)__popc(msk));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (emit) reinterpret_cast<K *>(keys_out)[base + __popc(msk & ((1u << lane) - 1u))] = key;
-    }
+    compact_tiles<K, K>(capacity, reinterpret_cast<K *>(keys_out), nullptr, count,
+                        [&](uint64_t gid, K &key, K &) {
+                            key = keys[gid];
+                            if (key == empty || key == tomb) return false;
+                            uint64_t b = probe_begin<K>(t, key), step = 0;
+                            for (uint64_t w = 0; w < t.num_buckets; ++w) {
+                                uint32_t hits, emp;
+                                mb_window<K, 0>(keys + b * t.cg_size, t.cg_size, key, empty,
+                                                hits, emp);
+                                if (hits) return b * t.cg_size + uint64_t(__ffs(hits) - 1) == gid;
+                                if (w == 0) step = probe_step<K>(t, key);
+                                b = probe_next(t, b, step);
+                            }
+                            return false;
+                        });
 }
 
 /* size (gpu_engine.cuh:419-464): non-empty values of slots with a valid key */

@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(256, WC_MULTI_MIN_BLOCKS) mv_find_kernel(const
 
 /* retrieve_all_keys: slot `gid` emits its key when it is the key's first
  * entry along its bucket sequence (lowest slot of the first bucket holding
- * the key) */
+ * the key), compacted by block tiles (wc_compact.cuh) */
 template <class L, int W>
 __global__ void __launch_bounds__(256) mv_unique_keys_kernel(TableView t, uint64_t capacity,
                                                              void *keys_out,
@@ -145,36 +145,22 @@ __global__ void __launch_bounds__(256) mv_unique_keys_kernel(TableView t, uint64
     using K = typename L::key_t;
     constexpr int SB = L::kSlotBytes;
     const K empty = K(t.empty_key), tomb = K(t.tombstone_key);
-    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-    const int lane = threadIdx.x & 31;
-    const uint64_t rounds = (capacity + stride - 1) / stride;
-    for (uint64_t r = 0; r < rounds; ++r) {
-        const uint64_t gid = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x + r * stride;
-        bool emit = false;
-        K key = empty;
-        if (gid < capacity) {
-            key = *reinterpret_cast<const K *>(reinterpret_cast<const unsigned char *>(t.slots) +
-                                               gid * SB);
-            if (key != empty && key != tomb) {
-                uint64_t b = probe_begin<K>(t, key), step = 0;
-                for (uint64_t w = 0; w < t.num_buckets; ++w) {
-                    uint32_t hits, emp;
-                    mv_bucket<L, W>(t, b, key, hits, emp, [](int, const LaneWords &, int) {});
-                    if (hits) {
-                        emit = b * W + uint64_t(__ffs(hits) - 1) == gid;
-                        break;
-                    }
-                    if (w == 0) step = probe_step<K>(t, key);
-                    b = probe_next(t, b, step);
-                }
-            }
-        }
-        const unsigned m = __ballot_sync(kFull, emit);
-        unsigned long long base = 0;
-        if (lane == 0 && m) base = atomicAdd(count, (unsigned long long)__popc(m));
-        base = __shfl_sync(kFull, base, 0);
-        if (emit) reinterpret_cast<K *>(keys_out)[base + __popc(m & ((1u << lane) - 1u))] = key;
-    }
+    const unsigned char *const slots = reinterpret_cast<const unsigned char *>(t.slots);
+    compact_tiles<K, K>(capacity, reinterpret_cast<K *>(keys_out), nullptr, count,
+                        [&](uint64_t gid, K &key, K &) {
+                            key = *reinterpret_cast<const K *>(slots + gid * SB);
+                            if (key == empty || key == tomb) return false;
+                            uint64_t b = probe_begin<K>(t, key), step = 0;
+                            for (uint64_t w = 0; w < t.num_buckets; ++w) {
+                                uint32_t hits, emp;
+                                mv_bucket<L, W>(t, b, key, hits, emp,
+                                                [](int, const LaneWords &, int) {});
+                                if (hits) return b * W + uint64_t(__ffs(hits) - 1) == gid;
+                                if (w == 0) step = probe_step<K>(t, key);
+                                b = probe_next(t, b, step);
+                            }
+                            return false;
+                        });
 }
 
 /* ---- inclusive scan of per-key counts into end offsets, begin offsets

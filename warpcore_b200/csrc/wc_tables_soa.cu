@@ -36,7 +36,7 @@ TableKernel pick_soa_for(int W, int op)
 }
 
 /* every valid (key, value) of the key array and the value array, compacted
- * by block tiles as dump_kernel does (dump_tiles); both arrays are streamed */
+ * by block tiles as dump_kernel does (compact_tiles); both arrays are streamed */
 template <class K, class V>
 __global__ void __launch_bounds__(256) soa_dump_kernel(const void *keys, const void *values,
                                                        uint64_t capacity, uint64_t empty,
@@ -47,11 +47,12 @@ __global__ void __launch_bounds__(256) soa_dump_kernel(const void *keys, const v
     const K *const kin = reinterpret_cast<const K *>(keys);
     const V *const vin = reinterpret_cast<const V *>(values);
     const bool want_values = values_out != nullptr;
-    dump_tiles<K, V>(capacity, K(empty), K(tomb), reinterpret_cast<K *>(keys_out),
-                     reinterpret_cast<V *>(values_out), count, [&](uint64_t s, K &k, V &v) {
-                         k = kin[s];
-                         if (want_values) v = vin[s];
-                     });
+    compact_tiles<K, V>(capacity, reinterpret_cast<K *>(keys_out),
+                        reinterpret_cast<V *>(values_out), count, [&](uint64_t s, K &k, V &v) {
+                            k = kin[s];
+                            if (want_values) v = vin[s];
+                            return k != K(empty) && k != K(tomb);
+                        });
 }
 
 } // namespace
