@@ -123,10 +123,8 @@ __global__ void __launch_bounds__(256, WC_MULTI_MIN_BLOCKS) bl_find_kernel(const
         }
     }
     const uint32_t wj = __reduce_or_sync(0xffffffffu, join);
-    const unsigned lo = __reduce_add_sync(0xffffffffu, unsigned(total & 0xffffffffu));
-    const unsigned hi = __reduce_add_sync(0xffffffffu, unsigned(total >> 32));
+    const unsigned long long sum = warp_sum_u64(total);
     if ((threadIdx.x & 31) == 0) {
-        const unsigned long long sum = (unsigned long long)lo + ((unsigned long long)hi << 32);
         if (a.total && sum) atomicAdd(a.total, sum);
         join_status(a.v.t.status, wj);
     }
@@ -166,10 +164,7 @@ __global__ void __launch_bounds__(256) bl_scan_keys_kernel(const BlView v, uint6
                             vals += bl_unpack(v, v.handles[i]).count;
                             return true;
                         });
-    /* 64-bit warp sum (a sum of 32-bit halves would drop the low halves'
-     * carries) */
-#pragma unroll
-    for (int o = 16; o; o >>= 1) vals += __shfl_down_sync(0xffffffffu, vals, o);
+    vals = warp_sum_u64(vals);
     if ((threadIdx.x & 31) == 0 && vals) atomicAdd(num_values, vals);
 }
 

@@ -2,7 +2,8 @@
  * wc_compact.cuh -- stream compaction of a slot array into an output array,
  * for the table-wide dumps: retrieve_all (single_value_hash_table.cuh:391-417)
  * and retrieve_all_keys (gpu_engine.cuh:51-93; bucket_list_hash_table.cuh,
- * multi_bucket_hash_table.cuh).
+ * multi_bucket_hash_table.cuh), and the warp sum of 64-bit counts that the
+ * counting kernels beside them use.
  *
  * A block takes tiles of kCompactPerThread x 256 consecutive slots.  Every
  * thread fetches its kCompactPerThread slots before any is placed, so their
@@ -21,6 +22,15 @@ namespace warpcore {
 namespace b200 {
 
 constexpr int kCompactPerThread = 8;
+
+/* sum of a 64-bit count over the 32 lanes of a full warp, in every lane (a
+ * sum of two 32-bit halves would drop the carries of the low halves) */
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
 
 /* fetch(s, k, v) reads slot s (< capacity) into k and v and returns whether
  * the slot emits an entry.  Entries go to keys_out (if not NULL) and

@@ -140,10 +140,8 @@ __global__ void __launch_bounds__(256, WC_MULTI_MIN_BLOCKS) mb_find_kernel(const
         }
     }
     const uint32_t wj = __reduce_or_sync(0xffffffffu, join);
-    const unsigned lo = __reduce_add_sync(0xffffffffu, unsigned(total & 0xffffffffu));
-    const unsigned hi = __reduce_add_sync(0xffffffffu, unsigned(total >> 32));
+    const unsigned long long sum = warp_sum_u64(total);
     if ((threadIdx.x & 31) == 0) {
-        const unsigned long long sum = (unsigned long long)lo + ((unsigned long long)hi << 32);
         if (a.total && sum) atomicAdd(a.total, sum);
         join_status(a.m.t.status, wj);
     }

@@ -122,13 +122,10 @@ __global__ void __launch_bounds__(256, WC_MULTI_MIN_BLOCKS) mv_find_kernel(const
             mv_write_status(a, i, st);
         }
     }
-    /* every lane of the warp arrives here (no early exits); 64-bit sum as
-     * two 32-bit halves */
+    /* every lane of the warp arrives here (no early exits) */
     const uint32_t wj = __reduce_or_sync(kFull, join);
-    const unsigned lo = __reduce_add_sync(kFull, unsigned(total & 0xffffffffu));
-    const unsigned hi = __reduce_add_sync(kFull, unsigned(total >> 32));
+    const unsigned long long sum = warp_sum_u64(total);
     if ((threadIdx.x & 31) == 0) {
-        const unsigned long long sum = (unsigned long long)lo + ((unsigned long long)hi << 32);
         if (a.total && sum) atomicAdd(a.total, sum);
         join_status(a.t.status, wj);
     }
