@@ -217,7 +217,9 @@ int wc_table_size(wc_table *t, wc_stream_t stream, uint64_t *size_out);
 int wc_table_size_scan(wc_table *t, wc_stream_t stream, uint64_t *size_out);
 /* retrieve_all(keys_out, values_out, num_out, stream)
  * (single_value_hash_table.cuh:391-417, hash_set.cuh:367-384); blocking;
- * values_out may be NULL and is ignored for hash sets */
+ * values_out may be NULL and is ignored for hash sets.  The outputs must
+ * hold size() entries; the order of the pairs is unspecified, as in the
+ * reference. */
 int wc_table_retrieve_all(wc_table *t, void *keys_out, void *values_out,
                           uint64_t *num_out, wc_stream_t stream);
 /* peek_status(stream) / pop_status(stream)
